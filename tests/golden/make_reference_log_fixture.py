@@ -1,0 +1,54 @@
+"""Extract the reference's logged solver/vmult results into tests/golden/reference_logs.json.
+
+Run once in a container that has the reference checkout (REFERENCE_ROOT, default
+/root/reference); the JSON it writes is committed and is what the tests read.  Each row
+keeps the file and line of the log it came from.
+"""
+import json
+import os
+import re
+import sys
+
+ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+LOGS = {
+    "fp64": "tests/poisson_cube_bk3_fp64/results/single-gpu-batched.out",
+    "mixed": "tests/poisson_cube_bk3/results/signle-gpu-batched-mixed-precision.out",
+}
+
+
+def parse(rel):
+    rows = []
+    with open(os.path.join(ROOT, rel)) as f:
+        lines = f.readlines()
+    start = None
+    for i, line in enumerate(lines):
+        if re.match(r"^\s*cells\s+dofs\s+mv_outer\s+mv_inner\s+cg_time\s+cg_its\s+cg_reduction", line):
+            start = i
+    if start is None:
+        raise SystemExit("table not found in " + rel)
+    for j in range(start + 1, len(lines)):
+        parts = lines[j].split()
+        if len(parts) != 7:
+            break
+        cells, dofs, mv_o, mv_i, cg_t, its, red = parts
+        rows.append({"cells": int(cells), "dofs": int(dofs), "mv_outer_s": float(mv_o),
+                     "mv_inner_s": float(mv_i), "cg_time_s": float(cg_t), "cg_its": int(its),
+                     "cg_reduction": float(red), "source": f"{rel}:{j + 1}"})
+    return rows
+
+
+def main():
+    out = {
+        "what": "Q4 ph-multigrid CG on the doubling mesh, f=1, Chebyshev degree 5, range 15, "
+                "10 eigenvalue iterations, ReductionControl(100,1e-16,1e-9); logged by the "
+                "reference (1 GPU).",
+        "tables": {k: parse(v) for k, v in LOGS.items()},
+    }
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_logs.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", dst, {k: len(v) for k, v in out["tables"].items()})
+
+
+if __name__ == "__main__":
+    sys.exit(main())
