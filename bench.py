@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark: continuous Q4 Laplace vmult (GDoF/s) on the deformed unit cube.
+
+Workload (one step = one operator application dst = A src over the whole mesh): 128^3
+hexahedra of [0,1]^3 mapped by x' = x + 0.1 sin(pi x) sin(pi y) sin(pi z) (per component,
+Q4 isoparametric, non-affine Jacobians at 5^3 Gauss points), FE_Q(4), 135,005,697 DoFs, src
+uniform[-1,1] from seed 1234, FP64.  Inputs (12.6 GB of geometry) are far larger than L2,
+so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--cells 128]
+
+--impl b200 (default): the CUDA library through its C ABI.  `value` is device-timed with
+the inputs resident in HBM; `e2e` repeats the measurement through the same C-ABI call with
+the input in pinned host memory, the host->device copy of src and the device->host copy of
+dst inside the timed region.  Under torchrun (N > 1) every rank runs an independent replica
+(the operator is not partitioned across GPUs); value sums the ranks' DoFs over the slowest
+rank's time.
+--impl reference: the CPU restatement of the reference's operator (oracle/pmg_oracle.c;
+the reference itself needs deal.II + Kokkos + MPI + p4est, none of which exist here) on all
+host cores, on a bounded sample of the same workload (the same deformed-cube mesh family
+at 32^3 cells).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "portable-multigrid_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "Q4 vmult GDoF/s"
+WORKLOAD = "Q4 Laplace vmult, deformed unit cube x'=x+0.1 sin(pi x)sin(pi y)sin(pi z)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cells", type=int, default=128, help="cells per direction (power of 2)")
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    ap.add_argument("--extra", action="store_true", help="also time the FP32 operator")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def box_for(cells):
+    refine = int(round(np.log2(cells)))
+    assert 1 << refine == cells, "--cells must be a power of two"
+    return refine
+
+
+# ----------------------------------------------------------------------------------------
+# CPU leg: the oracle's OpenMP vmult on a bounded sample (same mesh family, 32^3 cells)
+# ----------------------------------------------------------------------------------------
+def cpu_vmult_rate(steps=None, seconds=12.0, sample_cells=32):
+    from oracle import oracle as O
+    refine = box_for(sample_cells)
+    box = O.Box.make(refine=refine, deform=1, amp=0.1)
+    plain, cons, idx = O.dofs(box, 4)
+    G = O.geometry_G(box, 4)
+    color = O.colors(box)
+    src = np.random.default_rng(1234).uniform(-1.0, 1.0, cons.shape[0])
+    O.vmult(4, idx, G, cons, src, color=color)  # warm
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        O.vmult(4, idx, G, cons, src, color=color)
+        n += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and n >= steps) or (steps is None and el >= seconds):
+            break
+    rate = cons.shape[0] * n / el / 1e9
+    return rate, {"n_dofs": int(cons.shape[0]), "vmults": n, "seconds": el,
+                  "cores": O.num_threads()}
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    # each step is one vmult of the 32^3 sample
+    rate_w, info_w = cpu_vmult_rate(steps=max(1, args.warmup))
+    rate, info = cpu_vmult_rate(steps=max(1, args.steps))
+    sample = (f"oracle CPU restatement, OpenMP over {info['cores']} threads, {info['vmults']} "
+              f"vmults of the 32^3-cell deformed cube (Q4, {info['n_dofs']} DoFs)")
+    line = {
+        "metric": METRIC, "value": rate, "unit": "GDoF/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": info["seconds"] / info["vmults"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD + " (32^3-cell sample on the host CPU)",
+                   "cells": 32 ** 3, "n_dofs": info["n_dofs"], "degree": 4},
+        "cpu_baseline": {"value": rate, "unit": "GDoF/s", "cores": info["cores"], "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(key):
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(key)
+
+
+def time_vmults(op, dst, src, steps, torch, stream):
+    import pmg
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pmg.profile_reset()
+    pmg.profile_enable(True)
+    start.record(stream)
+    for _ in range(steps):
+        op.vmult(dst, src)
+    stop.record(stream)
+    stop.synchronize()
+    pmg.profile_enable(False)
+    total_ms = start.elapsed_time(stop)
+    cell_ms, cell_n = pmg.profile_query("vmult_cell")
+    cons_ms, cons_n = pmg.profile_query("vmult_constrained")
+    return total_ms, cell_ms, cell_n, cons_n
+
+
+def gpu_arm(args):
+    import torch
+    import pmg
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    dt = pmg.F64 if args.dtype == "f64" else pmg.F32
+    tdt = torch.float64 if dt == pmg.F64 else torch.float32
+    refine = box_for(args.cells)
+    box = pmg.Box.make(refine=refine, deform=1, amp=0.1)
+    t_setup = time.perf_counter()
+    mesh = pmg.Mesh(box)
+    op = pmg.LaplaceOperator(mesh, 4, dt, pmg.GEOMETRY_FULL, device=dev)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t_setup
+    N = op.m()
+    src_host = torch.from_numpy(np.random.default_rng(1234).uniform(-1.0, 1.0, N)).to(tdt)
+    src = src_host.to(f"cuda:{dev}")
+    dst = torch.empty_like(src)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        op.vmult(dst, src)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    total_ms, cell_ms, cell_n, cons_n = time_vmults(op, dst, src, args.steps, torch, stream)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    barrier()
+    # slowest rank
+    t_local = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        torch.distributed.all_reduce(t_local, op=torch.distributed.ReduceOp.MAX)
+    t_max = float(t_local.item())
+    ms_per_step = t_max / args.steps
+    value = N * world * args.steps / (t_max * 1e-3) / 1e9
+
+    # end to end through the same C-ABI call, host buffers, copies inside the timed region
+    src_pinned = src_host.pin_memory()
+    dst_pinned = torch.empty_like(src_pinned).pin_memory()
+    e2e_steps = max(3, min(args.steps // 10, 20))
+    for _ in range(2):
+        src.copy_(src_pinned, non_blocking=True)
+        op.vmult(dst, src)
+        dst_pinned.copy_(dst, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        src.copy_(src_pinned, non_blocking=True)
+        op.vmult(dst, src)
+        dst_pinned.copy_(dst, non_blocking=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    e2e_ms = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = N * world * e2e_steps / (float(e2e_ms.item()) * 1e-3) / 1e9
+    bytes_elem = 8 if dt == pmg.F64 else 4
+
+    # roofline of the cell kernel: algorithmic bytes per launch over its event-timed duration
+    alg_bytes = op.bytes_per_vmult()
+    cell_avg_s = (cell_ms / max(cell_n, 1)) * 1e-3
+    achieved = alg_bytes / cell_avg_s / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic_per_dof = ncu_traffic(f"vmult_q4_{args.dtype}_bytes_per_dof")
+    traffic = traffic_per_dof * N if traffic_per_dof else None
+
+    extra = {}
+    if args.extra and rank == 0:
+        op32 = pmg.LaplaceOperator(mesh, 4, pmg.F32, pmg.GEOMETRY_FULL, device=dev)
+        s32, d32 = src.float(), torch.empty(N, dtype=torch.float32, device=f"cuda:{dev}")
+        for _ in range(3):
+            op32.vmult(d32, s32)
+        t32, c32, n32, _ = time_vmults(op32, d32, s32, args.steps, torch, stream)
+        extra["fp32_vmult_gdofs"] = N * args.steps / (t32 * 1e-3) / 1e9
+        extra["fp32_cell_kernel_frac_of_hbm"] = op32.bytes_per_vmult() / (c32 / n32 * 1e-3) / 1e9 / peak
+        del op32
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        rate, info = cpu_vmult_rate(seconds=12.0)
+        cpu = {"value": rate, "unit": "GDoF/s", "cores": info["cores"], "kind": "port",
+               "sample": (f"oracle CPU restatement, {info['vmults']} vmults of the 32^3-cell "
+                          f"deformed cube (Q4, {info['n_dofs']} DoFs), OpenMP over "
+                          f"{info['cores']} threads, {info['seconds']:.1f} s")}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": args.cells ** 3, "n_dofs": N, "degree": 4,
+                       "geometry": "full G per quadrature point (6 x 125 per cell)",
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "inputs > L2 (geometry 12.6 GB at 128^3), no flush",
+                       "setup_s": t_setup},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
+                         "kernel": "vmult_slab_kernel<5,double,0>",
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "kernel_ms_avg": cell_avg_s * 1e3},
+            "e2e": {"value": e2e_value, "unit": "GDoF/s",
+                    "h2d_bytes_per_step": N * bytes_elem, "d2h_bytes_per_step": N * bytes_elem,
+                    "steps": e2e_steps},
+            "gpu_launches": int(cell_n + cons_n),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,250 @@
+/*
+ * pmg.h -- C ABI of the B200 matrix-free multigrid library (libpmg_b200.so).
+ *
+ * Every entry point is plain C: opaque handles, plain pointers and sizes, a pmg_status
+ * return code (0 = success, negative = error, message via pmg_last_error).  Vectors are
+ * device pointers owned by the caller; a `stream` argument is a cudaStream_t passed as
+ * void* (NULL = the legacy default stream).  All work is ordered on that stream; only the
+ * create functions, pmg_cg_solve and the Chebyshev eigenvalue estimate synchronise the host.
+ * Handles are not thread safe; distinct handles may be used from distinct threads.
+ *
+ * The entry points replace the C++ virtual interfaces of the reference
+ * (gshubhamk/portable-multigrid) for the matrix-free Laplace hot path; each declaration
+ * names the interface member it stands in for.
+ */
+#ifndef PMG_PMG_H
+#define PMG_PMG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t pmg_status;
+#define PMG_OK 0
+#define PMG_EINVAL (-1)     /* bad argument or unsupported combination                 */
+#define PMG_ENOMEM (-2)     /* device or host allocation failed                         */
+#define PMG_ECUDA (-3)      /* a CUDA call failed                                       */
+#define PMG_ENONFINITE (-4) /* a NaN or Inf appeared in a residual or a dot product     */
+#define PMG_ENOCONV (-5)    /* iteration limit reached before the tolerance             */
+#define PMG_EBOUNDS (-6)    /* an index map entry is out of range                       */
+#define PMG_ESTATE (-7)     /* call made on an object in the wrong state                */
+#define PMG_ENODEV (-8)     /* no CUDA device, or the library was built without one      */
+
+typedef enum { PMG_F64 = 0, PMG_F32 = 1 } pmg_dtype;
+
+typedef struct pmg_mesh pmg_mesh;
+typedef struct pmg_operator pmg_operator;
+typedef struct pmg_transfer pmg_transfer;
+typedef struct pmg_chebyshev pmg_chebyshev;
+typedef struct pmg_mg pmg_mg;
+
+/* ---------------------------------------------------------------------------------- */
+/* Errors and version                                                                 */
+/* ---------------------------------------------------------------------------------- */
+
+/* Copies the message of the last failed call on this host thread into buf (NUL
+ * terminated, truncated to n bytes); returns the message length. */
+size_t pmg_last_error(char *buf, size_t n);
+/* Static name of a status code. */
+const char *pmg_status_string(pmg_status status);
+pmg_status pmg_version(int32_t *major, int32_t *minor);
+
+/* ---------------------------------------------------------------------------------- */
+/* Meshes                                                                             */
+/* ---------------------------------------------------------------------------------- */
+
+/* A box [lo,hi] of coarse[0]*coarse[1]*coarse[2] coarse hexahedra, each refined globally
+ * `refine` times: GridGenerator::subdivided_hyper_rectangle + Triangulation::refine_global
+ * as driven in tests/poisson_cube_bk3/program.cc:937-957.  Cells are ordered coarse cell by
+ * coarse cell, Morton order inside each.  deform = 1 maps every Q_p mapping node by
+ * x' = x + amp*sin(pi x)sin(pi y)sin(pi z) in each component.  dirichlet_mask bit f marks
+ * face f (x-, x+, y-, y+, z-, z+) homogeneous Dirichlet (0x3F: all faces). */
+typedef struct {
+  int32_t coarse[3];
+  int32_t refine;
+  double lo[3];
+  double hi[3];
+  int32_t deform;
+  double amp;
+  int32_t dirichlet_mask;
+} pmg_box;
+
+pmg_status pmg_mesh_create_box(const pmg_box *box, pmg_mesh **mesh);
+pmg_status pmg_mesh_destroy(pmg_mesh *mesh);
+pmg_status pmg_mesh_n_cells(const pmg_mesh *mesh, int64_t *n_cells);
+
+/* ---------------------------------------------------------------------------------- */
+/* Level operators: Portable::LaplaceOperatorBase<3,Number>                           */
+/* (include/base/portable_laplace_operator_base.h:17-61)                              */
+/* ---------------------------------------------------------------------------------- */
+
+#define PMG_GEOMETRY_AUTO 0   /* per-cell constants on undeformed boxes, else per point */
+#define PMG_GEOMETRY_FULL 1   /* symmetric tensor G per quadrature point, 6*nq^3/cell   */
+#define PMG_GEOMETRY_AFFINE 2 /* 6 constants per cell, times w_q and the coefficient   */
+
+#define PMG_COEFF_NONE 0   /* -lap u                                                   */
+#define PMG_COEFF_KAPPA 1  /* kappa = 1 + 0.9 sin(2 pi x) sin(2 pi y) sin(2 pi z)      */
+#define PMG_COEFF_VALUES 2 /* caller-supplied values per quadrature point [C][nq^3]     */
+
+typedef struct {
+  int32_t degree;          /* FE_Q degree 1..6 (OperatorDispatchFactory::max_degree)    */
+  int32_t dtype;           /* pmg_dtype: arithmetic and vector type                     */
+  int32_t geometry;        /* PMG_GEOMETRY_*                                            */
+  int32_t coeff_kind;      /* PMG_COEFF_*                                               */
+  const double *coeff_qp;  /* host array [C][(degree+1)^3] for PMG_COEFF_VALUES         */
+  int32_t device;          /* CUDA device ordinal                                       */
+} pmg_operator_params;
+
+/* LaplaceOperatorBK3 constructor + setup_dof_indices_per_color + compute_G_tensors
+ * (include/operators/portable_laplace_operator_bk3.h:104-126, :360-437, :456-515). */
+pmg_status pmg_operator_create(const pmg_mesh *mesh, const pmg_operator_params *params,
+                               pmg_operator **op);
+pmg_status pmg_operator_destroy(pmg_operator *op);
+/* m() / n() (bk3.h:570-582). */
+pmg_status pmg_operator_m(const pmg_operator *op, int64_t *m);
+pmg_status pmg_operator_n(const pmg_operator *op, int64_t *n);
+pmg_status pmg_operator_n_cells(const pmg_operator *op, int64_t *n_cells);
+pmg_status pmg_operator_degree(const pmg_operator *op, int32_t *degree, int32_t *dtype);
+/* vmult(dst, src): dst = A src with identity rows on constrained DoFs (bk3.h:128-231).
+ * dst is overwritten; dst and src must not overlap. */
+pmg_status pmg_operator_vmult(const pmg_operator *op, void *dst, const void *src, void *stream);
+/* Tvmult == vmult (bk3.h:440-453). */
+pmg_status pmg_operator_tvmult(const pmg_operator *op, void *dst, const void *src, void *stream);
+/* vmult_dummy(dst, src, ghost_exchange_on, computation_on) (bk3.h:233-357): with one GPU
+ * there is no ghost exchange; computation_on = 0 only zeroes dst and copies the
+ * constrained values. */
+pmg_status pmg_operator_vmult_dummy(const pmg_operator *op, void *dst, const void *src,
+                                    int32_t ghost_exchange_on, int32_t computation_on,
+                                    void *stream);
+/* compute_diagonal() (bk3.h:533-561): inverse of diag(A), 1 on constrained rows. */
+pmg_status pmg_operator_compute_diagonal(pmg_operator *op, void *stream);
+/* get_matrix_diagonal_inverse() (bk3.h:563-568): device pointer owned by the operator,
+ * valid until the operator is destroyed; PMG_ESTATE before compute_diagonal. */
+pmg_status pmg_operator_get_inverse_diagonal(const pmg_operator *op, const void **inv_diag);
+/* Copies the inverse diagonal into a caller-owned device vector (ordered on stream). */
+pmg_status pmg_operator_copy_inverse_diagonal(const pmg_operator *op, void *dst, void *stream);
+/* el(row, col) (bk3.h:584-595): 1/inv_diag(row); only row == col is defined. */
+pmg_status pmg_operator_el(const pmg_operator *op, int64_t row, int64_t col, double *value);
+/* Algorithmic bytes of one vmult: 2*s*N + 4*nm^3*C + geometry bytes. */
+pmg_status pmg_operator_bytes_per_vmult(const pmg_operator *op, int64_t *bytes);
+/* Right-hand side b_i = (phi_i, f) with an nq-point Gauss rule, zero on constrained DoFs
+ * (tests/poisson_cube_bk3/program.cc:517-566): f_kind 0: f = 1;
+ * f_kind 1: f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z).  b has the operator's dtype. */
+pmg_status pmg_operator_assemble_rhs(const pmg_operator *op, int32_t f_kind, int32_t nq,
+                                     void *b, void *stream);
+/* Inspection, host copies in the reference layouts: the dof index map with the
+ * 0xFFFFFFFF sentinel [C][nm^3] (bk3.h:397-433), the constrained flags [N], and the
+ * geometry tensor [C][6][nq^3] in the order rr,rs,rt,ss,st,tt (bk3.h:477-510; full
+ * geometry only). */
+pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host);
+pmg_status pmg_operator_copy_constrained(const pmg_operator *op, uint8_t *host);
+pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host);
+
+/* ---------------------------------------------------------------------------------- */
+/* Transfers: Portable::MGTransferBase<3,number>                                      */
+/* (include/base/portable_mg_transfer_base.h:16-37)                                   */
+/* ---------------------------------------------------------------------------------- */
+
+/* reinit(mf_coarse, mf_fine, constraints_coarse, constraints_fine): a polynomial transfer
+ * (PolynomialTransfer, include/multigrid/portable_polynomial_transfer.h:1044-1361) when
+ * both operators live on the same mesh with degree_coarse < degree_fine, a geometric one
+ * (GeometricTransfer, include/multigrid/portable_geometric_transfer.h:944-1486) when the
+ * degrees agree and the fine mesh is the coarse box refined once more.  Both operators
+ * must have the same dtype. */
+pmg_status pmg_transfer_create(const pmg_operator *coarse, const pmg_operator *fine,
+                               pmg_transfer **transfer);
+pmg_status pmg_transfer_destroy(pmg_transfer *transfer);
+/* prolongate_and_add(dst_fine, src_coarse) */
+pmg_status pmg_transfer_prolongate_and_add(const pmg_transfer *transfer, void *dst_fine,
+                                           const void *src_coarse, void *stream);
+/* restrict_and_add(dst_coarse, src_fine) */
+pmg_status pmg_transfer_restrict_and_add(const pmg_transfer *transfer, void *dst_coarse,
+                                         const void *src_fine, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Smoother: deal.II PreconditionChebyshev<LaplaceOperatorBase, Vector> as configured at */
+/* tests/poisson_cube_bk3/program.cc:474-515                                          */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct {
+  int32_t degree;              /* <= 0: chosen so the Chebyshev bound reaches range   */
+  double smoothing_range;      /* > 1: lambda_max/range; < 1: target reduction        */
+  int32_t eig_cg_n_iterations; /* CG steps of the eigenvalue estimate                 */
+} pmg_chebyshev_params;
+
+/* initialize(matrix, data) with the operator's inverse diagonal as preconditioner
+ * (computed here if needed); the eigenvalue estimate runs on the first use or in
+ * pmg_chebyshev_estimate. */
+pmg_status pmg_chebyshev_create(pmg_operator *op, const pmg_chebyshev_params *params,
+                                pmg_chebyshev **smoother);
+pmg_status pmg_chebyshev_destroy(pmg_chebyshev *smoother);
+pmg_status pmg_chebyshev_estimate(pmg_chebyshev *smoother, void *stream);
+/* vmult(dst, src): degree-1 matrix-vector products from a zero initial guess. */
+pmg_status pmg_chebyshev_vmult(pmg_chebyshev *smoother, void *dst, const void *src,
+                               void *stream);
+/* step(dst, src): degree products starting from dst. */
+pmg_status pmg_chebyshev_step(pmg_chebyshev *smoother, void *dst, const void *src,
+                              void *stream);
+pmg_status pmg_chebyshev_info(const pmg_chebyshev *smoother, double *min_eigenvalue,
+                              double *max_eigenvalue, int32_t *degree, int32_t *cg_iterations);
+
+/* ---------------------------------------------------------------------------------- */
+/* V-cycle: VCycleMultigridBase::vmult (include/base/portable_v_cycle_multigrid_base.h:   */
+/* 18-27), MultigridSolver::vmult / v_cycle (tests/common/portable_multigrid_solver.h:    */
+/* 171-271)                                                                           */
+/* ---------------------------------------------------------------------------------- */
+
+/* levels[0] is the coarsest; transfers[l] connects levels l-1 and l (transfers[0] is
+ * ignored); smoothers[l] smooths level l (smoothers[0] is the coarse solver).  The
+ * objects are borrowed and must outlive the multigrid handle. */
+pmg_status pmg_mg_create(int32_t n_levels, pmg_operator *const *levels,
+                         pmg_transfer *const *transfers, pmg_chebyshev *const *smoothers,
+                         pmg_mg **mg);
+pmg_status pmg_mg_destroy(pmg_mg *mg);
+/* dst = V-cycle(src); src and dst have dtype vec_dtype, converted on entry and exit when
+ * it differs from the finest level's dtype. */
+pmg_status pmg_mg_vmult(pmg_mg *mg, void *dst, const void *src, int32_t vec_dtype,
+                        void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Conjugate gradients: MultigridSolver::solve_cg (portable_multigrid_solver.h:147-169)  */
+/* with deal.II SolverCG + ReductionControl                                           */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct {
+  int32_t iterations;
+  int32_t converged;
+  double initial_residual;
+  double final_residual;
+  double reduction_per_step; /* (final/initial)^(1/iterations), as the reference reports */
+} pmg_cg_info;
+
+/* Solves A x = b (A FP64) by preconditioned CG from the given x, stopping when
+ * ||r|| <= max(abs_tol, reduce*||r_0||) or after max_iterations (PMG_ENOCONV).
+ * precond: NULL = the operator's Jacobi preconditioner (computed if needed), else a
+ * multigrid V-cycle. */
+pmg_status pmg_cg_solve(pmg_operator *A, pmg_mg *precond, void *x, const void *b,
+                        double reduce, double abs_tol, int32_t max_iterations,
+                        pmg_cg_info *info, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Kernel timing (no reference counterpart; the reference times with deal.II Timer)   */
+/* ---------------------------------------------------------------------------------- */
+
+/* While enabled, every instrumented kernel launch records a CUDA event pair on its own
+ * stream.  Labels: "vmult_cell", "vmult_constrained", "diag_cell", "transfer_prolongate",
+ * "transfer_restrict". */
+pmg_status pmg_profile_enable(int32_t on);
+pmg_status pmg_profile_reset(void);
+/* Waits for the recorded events of `kernel` and returns their summed device time and the
+ * number of launches since the last reset. */
+pmg_status pmg_profile_query(const char *kernel, double *total_ms, int64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMG_PMG_H */

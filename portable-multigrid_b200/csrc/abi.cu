@@ -1,0 +1,432 @@
+// extern "C" entry points of libpmg_b200.so (declared in include/pmg/pmg.h): argument
+// checks, exception-to-status translation, per-thread error messages.
+#include <cstdio>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "pmg_internal.hpp"
+#include "solver.hpp"
+#include "transfer.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F> pmg_status guarded(const char *fn, F &&f) {
+  try {
+    f();
+    return PMG_OK;
+  } catch (const pmg::Error &e) {
+    g_last_error = std::string(fn) + ": " + e.what();
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    g_last_error = std::string(fn) + ": host allocation failed";
+    return PMG_ENOMEM;
+  } catch (const std::exception &e) {
+    g_last_error = std::string(fn) + ": " + e.what();
+    return PMG_EINVAL;
+  } catch (...) {
+    g_last_error = std::string(fn) + ": unknown error";
+    return PMG_EINVAL;
+  }
+}
+
+#define NEED(ptr) PMG_REQUIRE((ptr) != nullptr, #ptr " is NULL")
+
+inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+} // namespace
+
+extern "C" {
+
+size_t pmg_last_error(char *buf, size_t n) {
+  if (buf && n > 0) {
+    const size_t m = std::min(n - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), m);
+    buf[m] = '\0';
+  }
+  return g_last_error.size();
+}
+
+const char *pmg_status_string(pmg_status s) {
+  switch (s) {
+  case PMG_OK: return "PMG_OK";
+  case PMG_EINVAL: return "PMG_EINVAL";
+  case PMG_ENOMEM: return "PMG_ENOMEM";
+  case PMG_ECUDA: return "PMG_ECUDA";
+  case PMG_ENONFINITE: return "PMG_ENONFINITE";
+  case PMG_ENOCONV: return "PMG_ENOCONV";
+  case PMG_EBOUNDS: return "PMG_EBOUNDS";
+  case PMG_ESTATE: return "PMG_ESTATE";
+  case PMG_ENODEV: return "PMG_ENODEV";
+  default: return "PMG_UNKNOWN";
+  }
+}
+
+pmg_status pmg_version(int32_t *major, int32_t *minor) {
+  return guarded(__func__, [&] {
+    NEED(major);
+    NEED(minor);
+    *major = 0;
+    *minor = 1;
+  });
+}
+
+// ---------------------------------------------------------------------------------------
+pmg_status pmg_mesh_create_box(const pmg_box *box, pmg_mesh **mesh) {
+  return guarded(__func__, [&] {
+    NEED(box);
+    NEED(mesh);
+    auto m = std::make_unique<pmg_mesh>();
+    m->m = pmg::make_box(*box);
+    *mesh = m.release();
+  });
+}
+
+pmg_status pmg_mesh_destroy(pmg_mesh *mesh) {
+  delete mesh;
+  return PMG_OK;
+}
+
+pmg_status pmg_mesh_n_cells(const pmg_mesh *mesh, int64_t *n) {
+  return guarded(__func__, [&] {
+    NEED(mesh);
+    NEED(n);
+    *n = mesh->m.n_cells;
+  });
+}
+
+// ---------------------------------------------------------------------------------------
+pmg_status pmg_operator_create(const pmg_mesh *mesh, const pmg_operator_params *params,
+                               pmg_operator **op) {
+  return guarded(__func__, [&] {
+    NEED(mesh);
+    NEED(params);
+    NEED(op);
+    auto o = std::make_unique<pmg_operator>();
+    pmg::operator_setup(*o, *mesh, *params);
+    *op = o.release();
+  });
+}
+
+pmg_status pmg_operator_destroy(pmg_operator *op) {
+  if (op) {
+    cudaSetDevice(op->device);
+    delete op;
+  }
+  return PMG_OK;
+}
+
+pmg_status pmg_operator_m(const pmg_operator *op, int64_t *m) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(m);
+    *m = op->n_dofs;
+  });
+}
+
+pmg_status pmg_operator_n(const pmg_operator *op, int64_t *n) { return pmg_operator_m(op, n); }
+
+pmg_status pmg_operator_n_cells(const pmg_operator *op, int64_t *n) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(n);
+    *n = op->n_cells;
+  });
+}
+
+pmg_status pmg_operator_degree(const pmg_operator *op, int32_t *degree, int32_t *dtype) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    if (degree) *degree = op->degree;
+    if (dtype) *dtype = op->dtype;
+  });
+}
+
+pmg_status pmg_operator_vmult(const pmg_operator *op, void *dst, const void *src, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    PMG_CUDA(cudaSetDevice(op->device));
+    pmg::operator_vmult(*op, dst, src, as_stream(stream));
+  });
+}
+
+pmg_status pmg_operator_tvmult(const pmg_operator *op, void *dst, const void *src, void *stream) {
+  return pmg_operator_vmult(op, dst, src, stream);
+}
+
+pmg_status pmg_operator_vmult_dummy(const pmg_operator *op, void *dst, const void *src,
+                                    int32_t ghost_exchange_on, int32_t computation_on,
+                                    void *stream) {
+  (void)ghost_exchange_on; // a single device has no ghost DoFs
+  return guarded(__func__, [&] {
+    NEED(op);
+    PMG_CUDA(cudaSetDevice(op->device));
+    pmg::operator_vmult(*op, dst, src, as_stream(stream), computation_on != 0);
+  });
+}
+
+pmg_status pmg_operator_compute_diagonal(pmg_operator *op, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    pmg::operator_compute_inverse_diagonal(*op, as_stream(stream));
+  });
+}
+
+pmg_status pmg_operator_get_inverse_diagonal(const pmg_operator *op, const void **inv_diag) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(inv_diag);
+    if (!op->has_diag) pmg::fail(PMG_ESTATE, "compute_diagonal has not been called");
+    *inv_diag = op->inv_diag.get();
+  });
+}
+
+pmg_status pmg_operator_copy_inverse_diagonal(const pmg_operator *op, void *dst, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(dst);
+    if (!op->has_diag) pmg::fail(PMG_ESTATE, "compute_diagonal has not been called");
+    PMG_CUDA(cudaSetDevice(op->device));
+    PMG_CUDA(cudaMemcpyAsync(dst, op->inv_diag.get(), op->inv_diag.bytes(), cudaMemcpyDeviceToDevice,
+                             as_stream(stream)));
+  });
+}
+
+pmg_status pmg_operator_el(const pmg_operator *op, int64_t row, int64_t col, double *value) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(value);
+    PMG_REQUIRE(row == col, "el() is only defined on the diagonal");
+    if (row < 0 || row >= op->n_dofs) pmg::fail(PMG_EBOUNDS, "row out of range");
+    if (!op->has_diag) pmg::fail(PMG_ESTATE, "compute_diagonal has not been called");
+    PMG_CUDA(cudaSetDevice(op->device));
+    PMG_CUDA(cudaDeviceSynchronize());
+    double inv = 0;
+    if (op->dtype == PMG_F64) {
+      PMG_CUDA(cudaMemcpy(&inv, op->inv_diag.as<double>() + row, 8, cudaMemcpyDeviceToHost));
+    } else {
+      float f = 0;
+      PMG_CUDA(cudaMemcpy(&f, op->inv_diag.as<float>() + row, 4, cudaMemcpyDeviceToHost));
+      inv = f;
+    }
+    *value = 1.0 / inv;
+  });
+}
+
+pmg_status pmg_operator_bytes_per_vmult(const pmg_operator *op, int64_t *bytes) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(bytes);
+    *bytes = pmg::operator_bytes(*op);
+  });
+}
+
+pmg_status pmg_operator_assemble_rhs(const pmg_operator *op, int32_t f_kind, int32_t nq, void *b,
+                                     void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(b);
+    pmg::operator_assemble_rhs(*op, f_kind, nq, b, as_stream(stream));
+  });
+}
+
+pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(host);
+    for (size_t e = 0; e < op->num.plain.size(); ++e) {
+      const uint32_t d = op->num.plain[e];
+      host[e] = op->num.constrained[d] ? pmg::kInvalid : d;
+    }
+  });
+}
+
+pmg_status pmg_operator_copy_constrained(const pmg_operator *op, uint8_t *host) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(host);
+    std::memcpy(host, op->num.constrained.data(), op->num.constrained.size());
+  });
+}
+
+pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(host);
+    PMG_CUDA(cudaSetDevice(op->device));
+    pmg::operator_copy_geometry(*op, host);
+  });
+}
+
+// ---------------------------------------------------------------------------------------
+pmg_status pmg_transfer_create(const pmg_operator *coarse, const pmg_operator *fine,
+                               pmg_transfer **transfer) {
+  return guarded(__func__, [&] {
+    NEED(coarse);
+    NEED(fine);
+    NEED(transfer);
+    auto t = std::make_unique<pmg_transfer>();
+    pmg::transfer_setup(*t, *coarse, *fine);
+    *transfer = t.release();
+  });
+}
+
+pmg_status pmg_transfer_destroy(pmg_transfer *t) {
+  if (t) {
+    cudaSetDevice(t->device);
+    delete t;
+  }
+  return PMG_OK;
+}
+
+pmg_status pmg_transfer_prolongate_and_add(const pmg_transfer *t, void *dst_fine,
+                                           const void *src_coarse, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(t);
+    PMG_CUDA(cudaSetDevice(t->device));
+    pmg::transfer_apply(*t, 0, dst_fine, src_coarse, as_stream(stream));
+  });
+}
+
+pmg_status pmg_transfer_restrict_and_add(const pmg_transfer *t, void *dst_coarse,
+                                         const void *src_fine, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(t);
+    PMG_CUDA(cudaSetDevice(t->device));
+    pmg::transfer_apply(*t, 1, dst_coarse, src_fine, as_stream(stream));
+  });
+}
+
+// ---------------------------------------------------------------------------------------
+pmg_status pmg_chebyshev_create(pmg_operator *op, const pmg_chebyshev_params *params,
+                                pmg_chebyshev **smoother) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(params);
+    NEED(smoother);
+    auto c = std::make_unique<pmg_chebyshev>();
+    pmg::chebyshev_setup(*c, *op, *params);
+    *smoother = c.release();
+  });
+}
+
+pmg_status pmg_chebyshev_destroy(pmg_chebyshev *c) {
+  if (c) {
+    if (c->op) cudaSetDevice(c->op->device);
+    delete c;
+  }
+  return PMG_OK;
+}
+
+pmg_status pmg_chebyshev_estimate(pmg_chebyshev *c, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(c);
+    PMG_CUDA(cudaSetDevice(c->op->device));
+    pmg::chebyshev_estimate(*c, as_stream(stream));
+  });
+}
+
+pmg_status pmg_chebyshev_vmult(pmg_chebyshev *c, void *dst, const void *src, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(c);
+    NEED(dst);
+    NEED(src);
+    PMG_CUDA(cudaSetDevice(c->op->device));
+    pmg::chebyshev_apply(*c, dst, src, true, as_stream(stream));
+  });
+}
+
+pmg_status pmg_chebyshev_step(pmg_chebyshev *c, void *dst, const void *src, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(c);
+    NEED(dst);
+    NEED(src);
+    PMG_CUDA(cudaSetDevice(c->op->device));
+    pmg::chebyshev_apply(*c, dst, src, false, as_stream(stream));
+  });
+}
+
+pmg_status pmg_chebyshev_info(const pmg_chebyshev *c, double *min_ev, double *max_ev,
+                              int32_t *degree, int32_t *cg_its) {
+  return guarded(__func__, [&] {
+    NEED(c);
+    if (!c->estimated) pmg::fail(PMG_ESTATE, "eigenvalues not estimated yet");
+    if (min_ev) *min_ev = c->min_ev;
+    if (max_ev) *max_ev = c->max_ev;
+    if (degree) *degree = c->degree;
+    if (cg_its) *cg_its = c->cg_its;
+  });
+}
+
+// ---------------------------------------------------------------------------------------
+pmg_status pmg_mg_create(int32_t n_levels, pmg_operator *const *levels,
+                         pmg_transfer *const *transfers, pmg_chebyshev *const *smoothers,
+                         pmg_mg **mg) {
+  return guarded(__func__, [&] {
+    NEED(levels);
+    NEED(smoothers);
+    NEED(mg);
+    PMG_REQUIRE(n_levels == 1 || transfers, "transfers is NULL");
+    auto m = std::make_unique<pmg_mg>();
+    std::vector<pmg_transfer *> tr(n_levels, nullptr);
+    for (int l = 1; l < n_levels; ++l) tr[l] = transfers[l];
+    pmg::mg_setup(*m, n_levels, levels, tr.data(), smoothers);
+    *mg = m.release();
+  });
+}
+
+pmg_status pmg_mg_destroy(pmg_mg *mg) {
+  if (mg) {
+    if (!mg->levels.empty()) cudaSetDevice(mg->levels.back()->device);
+    delete mg;
+  }
+  return PMG_OK;
+}
+
+pmg_status pmg_mg_vmult(pmg_mg *mg, void *dst, const void *src, int32_t vec_dtype, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(mg);
+    NEED(dst);
+    NEED(src);
+    PMG_REQUIRE(vec_dtype == PMG_F64 || vec_dtype == PMG_F32, "bad vec_dtype");
+    PMG_CUDA(cudaSetDevice(mg->levels.back()->device));
+    pmg::mg_vmult(*mg, dst, src, vec_dtype, as_stream(stream));
+  });
+}
+
+pmg_status pmg_cg_solve(pmg_operator *A, pmg_mg *precond, void *x, const void *b, double reduce,
+                        double abs_tol, int32_t max_iterations, pmg_cg_info *info, void *stream) {
+  pmg_cg_info local{};
+  pmg_status st = guarded(__func__, [&] {
+    NEED(A);
+    pmg::cg_solve(*A, precond, x, b, reduce, abs_tol, max_iterations, local, as_stream(stream));
+  });
+  if (info) *info = local;
+  if (st == PMG_OK && !local.converged) {
+    g_last_error = "pmg_cg_solve: iteration limit reached";
+    return PMG_ENOCONV;
+  }
+  return st;
+}
+
+// ---------------------------------------------------------------------------------------
+pmg_status pmg_profile_enable(int32_t on) {
+  return guarded(__func__, [&] { pmg::prof::set_enabled(on != 0); });
+}
+
+pmg_status pmg_profile_reset(void) {
+  return guarded(__func__, [&] { pmg::prof::reset(); });
+}
+
+pmg_status pmg_profile_query(const char *kernel, double *total_ms, int64_t *launches) {
+  return guarded(__func__, [&] {
+    NEED(kernel);
+    NEED(total_ms);
+    NEED(launches);
+    pmg::prof::query(kernel, total_ms, launches);
+  });
+}
+
+} // extern "C"

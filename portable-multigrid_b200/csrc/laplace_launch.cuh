@@ -1,0 +1,130 @@
+// Launchers of the slab kernels for one polynomial degree.  Included by laplace_p<d>.cu
+// with PMG_DEGREE defined, so each degree compiles as its own translation unit.
+#pragma once
+
+#include "laplace_kernels.cuh"
+#include "pmg_internal.hpp"
+
+#ifndef PMG_DEGREE
+#error "define PMG_DEGREE before including laplace_launch.cuh"
+#endif
+
+#define PMG_CAT2(a, b) a##b
+#define PMG_CAT(a, b) PMG_CAT2(a, b)
+
+namespace pmg {
+namespace {
+
+constexpr int kN = PMG_DEGREE + 1;
+constexpr int kWarpsPerBlock = 4;
+
+template <typename T> kern::Tab<kN, T> make_tab(const SlabLaunch &L) {
+  kern::Tab<kN, T> t;
+  for (int a = 0; a < kN * kN; ++a) {
+    t.S[a] = (T)L.S[a];
+    t.SD[a] = (T)L.SD[a];
+    t.D[a] = (T)L.D[a];
+  }
+  for (int a = 0; a < kN; ++a) t.W[a] = (T)L.W[a];
+  return t;
+}
+
+template <typename T> kern::Tab2<kN, T> make_tab2(const SlabLaunch &L) {
+  kern::Tab2<kN, T> t;
+  for (int a = 0; a < kN * kN; ++a) {
+    t.S2[a] = (T)(L.S[a] * L.S[a]);
+    t.SS[a] = (T)(L.S[a] * L.SD[a]);
+    t.D2[a] = (T)(L.SD[a] * L.SD[a]);
+  }
+  for (int a = 0; a < kN; ++a) t.W[a] = (T)L.W[a];
+  return t;
+}
+
+template <typename T> constexpr size_t vmult_smem() {
+  return size_t(kWarpsPerBlock) * 2 * kern::Layout<kN>::CPW * kern::Layout<kN>::N3 * sizeof(T);
+}
+template <typename T> constexpr size_t diag_smem() {
+  return size_t(kWarpsPerBlock) * 3 * kern::Layout<kN>::CPW * kern::Layout<kN>::N3 * sizeof(T);
+}
+
+// cudaFuncSetAttribute for the dynamic shared memory once per device and kernel
+template <typename K> void allow_smem(K kernel, size_t bytes) {
+  static bool done[64] = {false};
+  int dev = 0;
+  PMG_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && !done[dev]) {
+    PMG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done[dev] = true;
+  }
+}
+
+template <typename T, int GEOM> void vmult_geom(const SlabLaunch &L) {
+  auto k = kern::vmult_slab_kernel<kN, T, GEOM>;
+  allow_smem(k, vmult_smem<T>());
+  k<<<L.grid, 32 * kWarpsPerBlock, vmult_smem<T>(), L.stream>>>(
+      make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
+      static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups);
+  PMG_LAUNCH_CHECK();
+}
+
+template <typename T, int GEOM> void diag_geom(const SlabLaunch &L) {
+  auto k = kern::diag_slab_kernel<kN, T, GEOM>;
+  allow_smem(k, diag_smem<T>());
+  k<<<L.grid, 32 * kWarpsPerBlock, diag_smem<T>(), L.stream>>>(
+      make_tab2<T>(L), static_cast<T *>(L.dst), L.idx, static_cast<const T *>(L.geo),
+      static_cast<const T *>(L.coef), L.n_groups);
+  PMG_LAUNCH_CHECK();
+}
+
+template <typename T> void vmult_type(const SlabLaunch &L) {
+  if (L.geom == 0) vmult_geom<T, 0>(L);
+  else if (L.geom == 1) vmult_geom<T, 1>(L);
+  else vmult_geom<T, 2>(L);
+}
+
+template <typename T> void diag_type(const SlabLaunch &L) {
+  if (L.geom == 0) diag_geom<T, 0>(L);
+  else if (L.geom == 1) diag_geom<T, 1>(L);
+  else diag_geom<T, 2>(L);
+}
+
+template <typename T, int GEOM> int occ_vmult() {
+  auto k = kern::vmult_slab_kernel<kN, T, GEOM>;
+  allow_smem(k, vmult_smem<T>());
+  int nb = 0;
+  PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kWarpsPerBlock, vmult_smem<T>()));
+  return nb;
+}
+template <typename T, int GEOM> int occ_diag() {
+  auto k = kern::diag_slab_kernel<kN, T, GEOM>;
+  allow_smem(k, diag_smem<T>());
+  int nb = 0;
+  PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kWarpsPerBlock, diag_smem<T>()));
+  return nb;
+}
+
+} // namespace
+
+void PMG_CAT(launch_vmult_p, PMG_DEGREE)(const SlabLaunch &L) {
+  if (L.dtype == PMG_F64) vmult_type<double>(L);
+  else vmult_type<float>(L);
+}
+
+void PMG_CAT(launch_diag_p, PMG_DEGREE)(const SlabLaunch &L) {
+  if (L.dtype == PMG_F64) diag_type<double>(L);
+  else diag_type<float>(L);
+}
+
+int PMG_CAT(occupancy_vmult_p, PMG_DEGREE)(int dtype, int geom) {
+  if (dtype == PMG_F64)
+    return geom == 0 ? occ_vmult<double, 0>() : geom == 1 ? occ_vmult<double, 1>() : occ_vmult<double, 2>();
+  return geom == 0 ? occ_vmult<float, 0>() : geom == 1 ? occ_vmult<float, 1>() : occ_vmult<float, 2>();
+}
+
+int PMG_CAT(occupancy_diag_p, PMG_DEGREE)(int dtype, int geom) {
+  if (dtype == PMG_F64)
+    return geom == 0 ? occ_diag<double, 0>() : geom == 1 ? occ_diag<double, 1>() : occ_diag<double, 2>();
+  return geom == 0 ? occ_diag<float, 0>() : geom == 1 ? occ_diag<float, 1>() : occ_diag<float, 2>();
+}
+
+} // namespace pmg

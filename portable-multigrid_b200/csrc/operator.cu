@@ -1,0 +1,483 @@
+// Level operator: setup of the index map and geometry on the device, vmult, diagonal,
+// right-hand side assembly (LaplaceOperatorBK3, include/operators/portable_laplace_operator_bk3.h).
+#include <algorithm>
+#include <cmath>
+
+#include "laplace_kernels.cuh"
+#include "pmg_internal.hpp"
+
+namespace pmg {
+namespace {
+
+constexpr int kMaxNm = 8;   // nodes per direction (degree <= 6, +1 for nq = p+2 rules)
+constexpr int kMaxNq = 8;
+
+// Everything the per-cell geometry kernels need, passed by value (constant bank).
+struct GeoParams {
+  double lo[3], h[3];
+  int deform;
+  double amp;
+  int nm, nq;
+  int N, cpw, lanes; // slab layout of the owning operator (nm == nq == N for G output)
+  double xl[kMaxNm];
+  double S[kMaxNm * kMaxNq], SD[kMaxNm * kMaxNq], W[kMaxNq];
+};
+
+__device__ __forceinline__ void map_point(const GeoParams &g, const double xr[3], double xp[3]) {
+  xp[0] = xr[0];
+  xp[1] = xr[1];
+  xp[2] = xr[2];
+  if (g.deform == 1) {
+    const double s = g.amp * sin(M_PI * xr[0]) * sin(M_PI * xr[1]) * sin(M_PI * xr[2]);
+    xp[0] += s;
+    xp[1] += s;
+    xp[2] += s;
+  }
+}
+
+__device__ __forceinline__ double coefficient(int kind, const double x[3]) {
+  if (kind == PMG_COEFF_KAPPA)
+    return 1.0 + 0.9 * sin(2 * M_PI * x[0]) * sin(2 * M_PI * x[1]) * sin(2 * M_PI * x[2]);
+  return 1.0;
+}
+
+// One block per cell (grid-stride): mapping nodes in shared memory, then per quadrature
+// point the Jacobian of the isoparametric Q_p map, its inverse and determinant.
+// mode 0: write G = coef * |det J| w_q J^{-1} J^{-T} into the slab layout (full geometry);
+// mode 1: write coef * (per-point factor) into the affine coefficient layout;
+// mode 2: right-hand side, b_i += sum_q phi_i(x_q) f(x_q) |det J| w_q (atomic).
+template <typename T>
+__global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restrict__ cell_xyz,
+                                     int64_t n_cells, int mode, int coeff_kind,
+                                     const double *__restrict__ coef_values,
+                                     T *__restrict__ out, const uint32_t *__restrict__ idx_perm,
+                                     int f_kind) {
+  __shared__ double X[3][kMaxNm * kMaxNm * kMaxNm];
+  __shared__ double fq[kMaxNq * kMaxNq * kMaxNq];
+  const int nm = g.nm, nq = g.nq, nm3 = nm * nm * nm, nq3 = nq * nq * nq;
+  for (int64_t c = blockIdx.x; c < n_cells; c += gridDim.x) {
+    const int cx = cell_xyz[3 * c], cy = cell_xyz[3 * c + 1], cz = cell_xyz[3 * c + 2];
+    for (int l = threadIdx.x; l < nm3; l += blockDim.x) {
+      const int i = l % nm, j = (l / nm) % nm, k = l / (nm * nm);
+      const double xr[3] = {g.lo[0] + (cx + g.xl[i]) * g.h[0], g.lo[1] + (cy + g.xl[j]) * g.h[1],
+                            g.lo[2] + (cz + g.xl[k]) * g.h[2]};
+      double xp[3];
+      map_point(g, xr, xp);
+      X[0][l] = xp[0];
+      X[1][l] = xp[1];
+      X[2][l] = xp[2];
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nq3; q += blockDim.x) {
+      const int q0 = q % nq, q1 = (q / nq) % nq, q2 = q / (nq * nq);
+      double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, xq[3] = {0, 0, 0};
+      for (int k = 0; k < nm; ++k)
+        for (int j = 0; j < nm; ++j) {
+          const double sj = g.S[j * nq + q1], dj = g.SD[j * nq + q1];
+          const double sk = g.S[k * nq + q2], dk = g.SD[k * nq + q2];
+          for (int i = 0; i < nm; ++i) {
+            const int l = (k * nm + j) * nm + i;
+            const double si = g.S[i * nq + q0], di = g.SD[i * nq + q0];
+            const double v = si * sj * sk, g0 = di * sj * sk, g1 = si * dj * sk, g2 = si * sj * dk;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const double xv = X[d][l];
+              xq[d] += xv * v;
+              J[3 * d + 0] += xv * g0;
+              J[3 * d + 1] += xv * g1;
+              J[3 * d + 2] += xv * g2;
+            }
+          }
+        }
+      const double A = J[4] * J[8] - J[5] * J[7], B = -(J[3] * J[8] - J[5] * J[6]),
+                   C = J[3] * J[7] - J[4] * J[6];
+      const double det = J[0] * A + J[1] * B + J[2] * C;
+      const double r = 1.0 / det;
+      const double inv[9] = {A * r,
+                             -(J[1] * J[8] - J[2] * J[7]) * r,
+                             (J[1] * J[5] - J[2] * J[4]) * r,
+                             B * r,
+                             (J[0] * J[8] - J[2] * J[6]) * r,
+                             -(J[0] * J[5] - J[2] * J[3]) * r,
+                             C * r,
+                             -(J[0] * J[7] - J[1] * J[6]) * r,
+                             (J[0] * J[4] - J[1] * J[3]) * r};
+      const double wq = g.W[q0] * g.W[q1] * g.W[q2];
+      double kap = coefficient(coeff_kind, xq);
+      if (coef_values) kap *= coef_values[c * nq3 + q];
+      const int64_t grp = c / g.cpw;
+      const int e = (int)(c % g.cpw);
+      const int m = q1 * g.N + q0, lane = e * g.N + q2;
+      if (mode == 0) {
+        const double f = fabs(det) * wq * kap;
+        int comp = 0;
+        for (int d1 = 0; d1 < 3; ++d1)
+          for (int d2 = d1; d2 < 3; ++d2) {
+            const double s = inv[3 * d1] * inv[3 * d2] + inv[3 * d1 + 1] * inv[3 * d2 + 1] +
+                             inv[3 * d1 + 2] * inv[3 * d2 + 2];
+            out[((grp * (g.N * g.N) + m) * 6 + comp) * g.lanes + lane] = (T)(f * s);
+            ++comp;
+          }
+      } else if (mode == 1) {
+        out[(grp * (g.N * g.N) + m) * g.lanes + lane] = (T)kap;
+      } else {
+        double f = 1.0;
+        if (f_kind == 1) f = 3.0 * M_PI * M_PI * sin(M_PI * xq[0]) * sin(M_PI * xq[1]) * sin(M_PI * xq[2]);
+        fq[q] = f * fabs(det) * wq;
+      }
+    }
+    __syncthreads();
+    if (mode == 2) {
+      for (int l = threadIdx.x; l < nm3; l += blockDim.x) {
+        const int i = l % nm, j = (l / nm) % nm, k = l / (nm * nm);
+        double s = 0;
+        for (int q2 = 0; q2 < nq; ++q2)
+          for (int q1 = 0; q1 < nq; ++q1) {
+            const double sjk = g.S[j * nq + q1] * g.S[k * nq + q2];
+            for (int q0 = 0; q0 < nq; ++q0)
+              s += g.S[i * nq + q0] * sjk * fq[(q2 * nq + q1) * nq + q0];
+          }
+        const int64_t grp = c / g.cpw;
+        const int e = (int)(c % g.cpw);
+        // Y-slab layout of the index map: [group][k*N + i][lane = e*N + j]
+        const uint32_t id = idx_perm[(grp * (g.N * g.N) + k * g.N + i) * g.lanes + e * g.N + j];
+        if (id != kInvalid) atomicAdd(out + id, (T)s);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <typename T>
+__global__ void invert_diagonal_kernel(T *__restrict__ d, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = (d[i] != T(0)) ? T(1) / d[i] : T(1);
+}
+
+template <typename T>
+__global__ void set_constrained_kernel(T *__restrict__ dst, const T *__restrict__ src,
+                                       const uint32_t *__restrict__ list, int64_t n, T value) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[list[i]] = src ? src[list[i]] : value;
+}
+
+GeoParams make_geo_params(const pmg_operator &op, int nq) {
+  GeoParams g{};
+  const auto &b = op.mesh.box;
+  for (int d = 0; d < 3; ++d) {
+    g.lo[d] = b.lo[d];
+    g.h[d] = (b.hi[d] - b.lo[d]) / double(op.mesh.n[d]);
+  }
+  g.deform = b.deform;
+  g.amp = b.amp;
+  g.nm = op.nm;
+  g.nq = nq;
+  g.N = op.nm;
+  g.cpw = op.cpw;
+  g.lanes = op.lanes;
+  const Tables1D t = make_tables(op.degree, nq);
+  for (int i = 0; i < op.nm; ++i) g.xl[i] = t.xl[i];
+  for (size_t a = 0; a < t.S.size(); ++a) {
+    g.S[a] = t.S[a];
+    g.SD[a] = t.SD[a];
+  }
+  for (int q = 0; q < nq; ++q) g.W[q] = t.W[q];
+  return g;
+}
+
+int num_sms(int device) {
+  int n = 0;
+  PMG_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device));
+  return n;
+}
+
+typedef void (*slab_fn)(const SlabLaunch &);
+slab_fn vmult_fn(int degree) {
+  static const slab_fn f[] = {nullptr,         launch_vmult_p1, launch_vmult_p2, launch_vmult_p3,
+                              launch_vmult_p4, launch_vmult_p5, launch_vmult_p6};
+  return f[degree];
+}
+slab_fn diag_fn(int degree) {
+  static const slab_fn f[] = {nullptr,        launch_diag_p1, launch_diag_p2, launch_diag_p3,
+                              launch_diag_p4, launch_diag_p5, launch_diag_p6};
+  return f[degree];
+}
+int occupancy(bool diag, int degree, int dtype, int geom) {
+  typedef int (*occ_fn)(int, int);
+  static const occ_fn fv[] = {nullptr,           occupancy_vmult_p1, occupancy_vmult_p2,
+                              occupancy_vmult_p3, occupancy_vmult_p4, occupancy_vmult_p5,
+                              occupancy_vmult_p6};
+  static const occ_fn fd[] = {nullptr,          occupancy_diag_p1, occupancy_diag_p2,
+                              occupancy_diag_p3, occupancy_diag_p4, occupancy_diag_p5,
+                              occupancy_diag_p6};
+  return (diag ? fd : fv)[degree](dtype, geom);
+}
+
+int geom_code(const pmg_operator &op) {
+  if (op.geometry == PMG_GEOMETRY_FULL) return 0;
+  return op.has_coeff_values ? 2 : 1;
+}
+
+SlabLaunch slab_launch(const pmg_operator &op, const Tables1D &t, cudaStream_t s) {
+  SlabLaunch L{};
+  L.idx = op.idx.as<uint32_t>();
+  L.geo = op.geo.get();
+  L.coef = op.coef.get();
+  L.n_groups = op.n_groups;
+  L.geom = geom_code(op);
+  L.dtype = op.dtype;
+  L.stream = s;
+  L.S = t.S.data();
+  L.SD = t.SD.data();
+  L.D = t.D.data();
+  L.W = t.W.data();
+  return L;
+}
+
+const Tables1D &cached_tables(int degree) {
+  static Tables1D tabs[kMaxDegree + 1];
+  static bool ready[kMaxDegree + 1] = {false};
+  if (!ready[degree]) {
+    tabs[degree] = make_tables(degree, degree + 1);
+    ready[degree] = true;
+  }
+  return tabs[degree];
+}
+
+} // namespace
+
+void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_params &prm) {
+  PMG_REQUIRE(prm.degree >= 1 && prm.degree <= kMaxDegree, "degree must be in [1,6]");
+  PMG_REQUIRE(prm.dtype == PMG_F64 || prm.dtype == PMG_F32, "dtype must be PMG_F64 or PMG_F32");
+  PMG_REQUIRE(prm.coeff_kind >= 0 && prm.coeff_kind <= 2, "bad coeff_kind");
+  PMG_REQUIRE(prm.coeff_kind != PMG_COEFF_VALUES || prm.coeff_qp, "coeff_qp is required");
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
+    (void)cudaGetLastError();
+    fail(PMG_ENODEV, "no CUDA device available");
+  }
+  PMG_REQUIRE(prm.device >= 0 && prm.device < n_dev, "bad device ordinal");
+  PMG_CUDA(cudaSetDevice(prm.device));
+  op.device = prm.device;
+  op.degree = prm.degree;
+  op.nm = op.nq = prm.degree + 1;
+  op.dtype = prm.dtype;
+  op.coeff_kind = prm.coeff_kind;
+  op.mesh = mesh.m;
+  op.n_cells = mesh.m.n_cells;
+  int geometry = prm.geometry;
+  if (geometry == PMG_GEOMETRY_AUTO) geometry = mesh.m.box.deform ? PMG_GEOMETRY_FULL : PMG_GEOMETRY_AFFINE;
+  PMG_REQUIRE(geometry == PMG_GEOMETRY_FULL || geometry == PMG_GEOMETRY_AFFINE, "bad geometry");
+  PMG_REQUIRE(!(geometry == PMG_GEOMETRY_AFFINE && mesh.m.box.deform), "affine geometry needs an undeformed box");
+  op.geometry = geometry;
+  op.has_coeff_values = (geometry == PMG_GEOMETRY_AFFINE && prm.coeff_kind != PMG_COEFF_NONE);
+
+  const int N = op.nm, N2 = N * N, N3 = N2 * N;
+  op.cpw = 32 / N;
+  op.lanes = op.cpw * N;
+  op.n_groups = (op.n_cells + op.cpw - 1) / op.cpw;
+
+  // numbering (setup_dof_indices_per_color, bk3.h:360-437)
+  op.num = make_numbering(mesh.m, op.degree, true);
+  op.n_dofs = op.num.n_dofs;
+
+  // index map with the sentinel, permuted into the Y-slab layout [group][k*N+i][e*N+j]
+  {
+    std::vector<uint32_t> perm((size_t)op.n_groups * N2 * op.lanes, kInvalid);
+    const uint32_t *plain = op.num.plain.data();
+    const uint8_t *cons = op.num.constrained.data();
+    const int64_t C = op.n_cells, lanes = op.lanes, cpw = op.cpw;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < C; ++c) {
+      const int64_t grp = c / cpw, e = c % cpw;
+      for (int k = 0; k < N; ++k)
+        for (int j = 0; j < N; ++j)
+          for (int i = 0; i < N; ++i) {
+            const uint32_t d = plain[c * N3 + (k * N + j) * N + i];
+            perm[(grp * N2 + k * N + i) * lanes + e * N + j] = cons[d] ? kInvalid : d;
+          }
+    }
+    op.idx = upload(perm);
+  }
+  // constrained list (copy_constrained_values, bk3.h:230)
+  {
+    std::vector<uint32_t> list;
+    for (int64_t i = 0; i < op.n_dofs; ++i)
+      if (op.num.constrained[i]) list.push_back((uint32_t)i);
+    op.n_constrained = (int64_t)list.size();
+    op.constrained_list = upload(list);
+  }
+  // geometry (compute_G_tensors, bk3.h:456-515), computed on the device
+  const size_t s = dtype_size(op.dtype);
+  DeviceBuffer xyz = upload(mesh.m.cell_xyz);
+  DeviceBuffer coef_in;
+  if (prm.coeff_kind == PMG_COEFF_VALUES) {
+    coef_in.allocate(sizeof(double) * op.n_cells * N3);
+    PMG_CUDA(cudaMemcpy(coef_in.get(), prm.coeff_qp, sizeof(double) * op.n_cells * N3,
+                        cudaMemcpyHostToDevice));
+  }
+  const GeoParams gp = make_geo_params(op, op.nq);
+  const int sms = num_sms(op.device);
+  const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)sms * 16);
+  if (geometry == PMG_GEOMETRY_FULL) {
+    op.geo.allocate(s * op.n_groups * N2 * 6 * op.lanes);
+    PMG_CUDA(cudaMemset(op.geo.get(), 0, op.geo.bytes()));
+    if (op.dtype == PMG_F64)
+      cell_geometry_kernel<double><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 0, prm.coeff_kind,
+                                                  coef_in.as<double>(), op.geo.as<double>(), nullptr, 0);
+    else
+      cell_geometry_kernel<float><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 0, prm.coeff_kind,
+                                                 coef_in.as<double>(), op.geo.as<float>(), nullptr, 0);
+    PMG_LAUNCH_CHECK();
+  } else {
+    // affine: C = |det J| J^{-1} J^{-T} / (w-independent) per cell; axis-aligned boxes give
+    // J = diag(h) for every cell
+    std::vector<double> c8(8, 0.0);
+    double h[3];
+    for (int d = 0; d < 3; ++d) h[d] = (mesh.m.box.hi[d] - mesh.m.box.lo[d]) / double(mesh.m.n[d]);
+    const double vol = h[0] * h[1] * h[2];
+    c8[0] = vol / (h[0] * h[0]);
+    c8[3] = vol / (h[1] * h[1]);
+    c8[5] = vol / (h[2] * h[2]);
+    const int64_t n_slots = op.n_groups * op.cpw;
+    if (op.dtype == PMG_F64) {
+      std::vector<double> v(n_slots * 8, 0.0);
+      for (int64_t c = 0; c < op.n_cells; ++c) std::copy(c8.begin(), c8.end(), v.begin() + 8 * c);
+      op.geo = upload(v);
+    } else {
+      std::vector<float> v(n_slots * 8, 0.0f);
+      for (int64_t c = 0; c < op.n_cells; ++c)
+        for (int a = 0; a < 8; ++a) v[8 * c + a] = (float)c8[a];
+      op.geo = upload(v);
+    }
+    if (op.has_coeff_values) {
+      op.coef.allocate(s * op.n_groups * N2 * op.lanes);
+      PMG_CUDA(cudaMemset(op.coef.get(), 0, op.coef.bytes()));
+      if (op.dtype == PMG_F64)
+        cell_geometry_kernel<double><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 1, prm.coeff_kind,
+                                                    coef_in.as<double>(), op.coef.as<double>(), nullptr, 0);
+      else
+        cell_geometry_kernel<float><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 1, prm.coeff_kind,
+                                                   coef_in.as<double>(), op.coef.as<float>(), nullptr, 0);
+      PMG_LAUNCH_CHECK();
+    }
+  }
+  PMG_CUDA(cudaDeviceSynchronize());
+  // persistent grids sized from the occupancy of this SM count
+  const int gc = geom_code(op);
+  const int ov = std::max(1, occupancy(false, op.degree, op.dtype, gc));
+  const int od = std::max(1, occupancy(true, op.degree, op.dtype, gc));
+  const int64_t blocks_needed = (op.n_groups + 3) / 4;
+  op.grid_vmult = (int)std::max<int64_t>(1, std::min<int64_t>(blocks_needed, (int64_t)ov * sms));
+  op.grid_diag = (int)std::max<int64_t>(1, std::min<int64_t>(blocks_needed, (int64_t)od * sms));
+  // the index lattice is only needed for building h-transfers: keep it
+}
+
+void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s, bool compute) {
+  PMG_REQUIRE(dst && src, "null vector");
+  PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");
+  const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
+  PMG_CUDA(cudaMemsetAsync(dst, 0, bytes, s)); // dst = 0 (bk3.h:134)
+  if (compute && op.n_cells > 0) {
+    SlabLaunch L = slab_launch(op, cached_tables(op.degree), s);
+    L.src = src;
+    L.dst = dst;
+    L.grid = op.grid_vmult;
+    prof::Scope scope("vmult_cell", s);
+    vmult_fn(op.degree)(L);
+  }
+  if (op.n_constrained > 0) {
+    prof::Scope scope("vmult_constrained", s);
+    const int grid = (int)std::min<int64_t>(1024, (op.n_constrained + 255) / 256);
+    if (op.dtype == PMG_F64)
+      set_constrained_kernel<double><<<grid, 256, 0, s>>>(static_cast<double *>(dst), static_cast<const double *>(src),
+                                                          op.constrained_list.as<uint32_t>(), op.n_constrained, 0.0);
+    else
+      set_constrained_kernel<float><<<grid, 256, 0, s>>>(static_cast<float *>(dst), static_cast<const float *>(src),
+                                                         op.constrained_list.as<uint32_t>(), op.n_constrained, 0.0f);
+    PMG_LAUNCH_CHECK();
+  }
+}
+
+void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s) {
+  PMG_CUDA(cudaSetDevice(op.device));
+  const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
+  if (op.inv_diag.bytes() != bytes) op.inv_diag.allocate(bytes);
+  PMG_CUDA(cudaMemsetAsync(op.inv_diag.get(), 0, bytes, s));
+  if (op.n_cells > 0) {
+    SlabLaunch L = slab_launch(op, cached_tables(op.degree), s);
+    L.dst = op.inv_diag.get();
+    L.grid = op.grid_diag;
+    prof::Scope scope("diag_cell", s);
+    diag_fn(op.degree)(L);
+  }
+  const int grid = (int)std::min<int64_t>(4096, (op.n_dofs + 255) / 256);
+  if (op.dtype == PMG_F64) {
+    invert_diagonal_kernel<double><<<grid, 256, 0, s>>>(op.inv_diag.as<double>(), op.n_dofs);
+    if (op.n_constrained)
+      set_constrained_kernel<double><<<64, 256, 0, s>>>(op.inv_diag.as<double>(), nullptr,
+                                                        op.constrained_list.as<uint32_t>(), op.n_constrained, 1.0);
+  } else {
+    invert_diagonal_kernel<float><<<grid, 256, 0, s>>>(op.inv_diag.as<float>(), op.n_dofs);
+    if (op.n_constrained)
+      set_constrained_kernel<float><<<64, 256, 0, s>>>(op.inv_diag.as<float>(), nullptr,
+                                                       op.constrained_list.as<uint32_t>(), op.n_constrained, 1.0f);
+  }
+  PMG_LAUNCH_CHECK();
+  op.has_diag = true;
+}
+
+void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, cudaStream_t s) {
+  PMG_REQUIRE(f_kind == 0 || f_kind == 1, "f_kind must be 0 or 1");
+  if (nq <= 0) nq = op.nq;
+  PMG_REQUIRE(nq >= 1 && nq <= kMaxNq, "nq must be in [1,8]");
+  PMG_CUDA(cudaSetDevice(op.device));
+  PMG_CUDA(cudaMemsetAsync(b, 0, dtype_size(op.dtype) * op.n_dofs, s));
+  DeviceBuffer xyz = upload(op.mesh.cell_xyz);
+  const GeoParams gp = make_geo_params(op, nq);
+  const int grid = (int)std::min<int64_t>(std::max<int64_t>(op.n_cells, 1), (int64_t)num_sms(op.device) * 16);
+  if (op.dtype == PMG_F64)
+    cell_geometry_kernel<double><<<grid, 128, 0, s>>>(gp, xyz.as<int32_t>(), op.n_cells, 2, 0, nullptr,
+                                                      static_cast<double *>(b), op.idx.as<uint32_t>(), f_kind);
+  else
+    cell_geometry_kernel<float><<<grid, 128, 0, s>>>(gp, xyz.as<int32_t>(), op.n_cells, 2, 0, nullptr,
+                                                     static_cast<float *>(b), op.idx.as<uint32_t>(), f_kind);
+  PMG_LAUNCH_CHECK();
+  PMG_CUDA(cudaStreamSynchronize(s)); // xyz is freed on return
+}
+
+void operator_copy_geometry(const pmg_operator &op, double *host) {
+  PMG_REQUIRE(op.geometry == PMG_GEOMETRY_FULL, "geometry copy needs the full geometry layout");
+  const int N = op.nm, N2 = N * N, N3 = N2 * N;
+  const size_t n = (size_t)op.n_groups * N2 * 6 * op.lanes;
+  std::vector<double> g(n);
+  if (op.dtype == PMG_F64) {
+    PMG_CUDA(cudaMemcpy(g.data(), op.geo.get(), n * 8, cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float> f(n);
+    PMG_CUDA(cudaMemcpy(f.data(), op.geo.get(), n * 4, cudaMemcpyDeviceToHost));
+    std::copy(f.begin(), f.end(), g.begin());
+  }
+  for (int64_t c = 0; c < op.n_cells; ++c) {
+    const int64_t grp = c / op.cpw, e = c % op.cpw;
+    for (int r = 0; r < N; ++r)
+      for (int q = 0; q < N; ++q)
+        for (int p = 0; p < N; ++p)
+          for (int comp = 0; comp < 6; ++comp)
+            host[(c * 6 + comp) * N3 + (r * N + q) * N + p] =
+                g[((grp * N2 + q * N + p) * 6 + comp) * op.lanes + e * N + r];
+  }
+}
+
+int64_t operator_bytes(const pmg_operator &op) {
+  const int64_t s = (int64_t)dtype_size(op.dtype);
+  const int64_t nm3 = (int64_t)op.nm * op.nm * op.nm, nq3 = (int64_t)op.nq * op.nq * op.nq;
+  int64_t g = 0;
+  if (op.geometry == PMG_GEOMETRY_FULL) g = 6 * nq3;
+  else g = 6 + (op.has_coeff_values ? nq3 : 0);
+  return 2 * s * op.n_dofs + 4 * nm3 * op.n_cells + g * s * op.n_cells;
+}
+
+} // namespace pmg

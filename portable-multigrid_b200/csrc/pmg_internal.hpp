@@ -1,0 +1,202 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pmg/pmg.h"
+
+namespace pmg {
+
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+constexpr int kMaxDegree = 6; // OperatorDispatchFactory::max_degree
+
+// ---------------------------------------------------------------------------------------
+// errors: every failure throws pmg::Error; the C ABI turns it into a status + message
+// ---------------------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  pmg_status status;
+  Error(pmg_status s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] inline void fail(pmg_status s, const std::string &m) { throw Error(s, m); }
+
+inline void cuda_check(cudaError_t e, const char *what, const char *file, int line) {
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError(); // clear a sticky-free error so later calls can proceed
+    fail(e == cudaErrorMemoryAllocation ? PMG_ENOMEM : PMG_ECUDA,
+         std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" +
+             std::to_string(line) + ")");
+  }
+}
+#define PMG_CUDA(call) ::pmg::cuda_check((call), #call, __FILE__, __LINE__)
+#define PMG_LAUNCH_CHECK() ::pmg::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+
+#define PMG_REQUIRE(cond, msg)                                                              \
+  do {                                                                                      \
+    if (!(cond)) ::pmg::fail(PMG_EINVAL, std::string(msg));                                 \
+  } while (0)
+
+// ---------------------------------------------------------------------------------------
+// kernel timing (profile.cu): an event pair per instrumented launch while enabled
+// ---------------------------------------------------------------------------------------
+namespace prof {
+bool enabled();
+void set_enabled(bool on);
+void reset();
+void query(const char *name, double *ms, int64_t *launches);
+struct Scope {
+  Scope(const char *name, cudaStream_t s);
+  ~Scope();
+  Scope(const Scope &) = delete;
+  Scope &operator=(const Scope &) = delete;
+  const char *name;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+};
+} // namespace prof
+
+// ---------------------------------------------------------------------------------------
+// device memory owned by library objects
+// ---------------------------------------------------------------------------------------
+class DeviceBuffer {
+public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(size_t bytes) { allocate(bytes); }
+  ~DeviceBuffer() { release(); }
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  DeviceBuffer(DeviceBuffer &&o) noexcept : ptr_(o.ptr_), bytes_(o.bytes_) {
+    o.ptr_ = nullptr;
+    o.bytes_ = 0;
+  }
+  DeviceBuffer &operator=(DeviceBuffer &&o) noexcept {
+    if (this != &o) {
+      release();
+      ptr_ = o.ptr_;
+      bytes_ = o.bytes_;
+      o.ptr_ = nullptr;
+      o.bytes_ = 0;
+    }
+    return *this;
+  }
+  void allocate(size_t bytes) {
+    release();
+    if (bytes == 0) return;
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      fail(PMG_ENOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                           cudaGetErrorString(e));
+    }
+    ptr_ = p;
+    bytes_ = bytes;
+  }
+  void release() {
+    if (ptr_) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+  }
+  template <typename T> T *as() const { return static_cast<T *>(ptr_); }
+  void *get() const { return ptr_; }
+  size_t bytes() const { return bytes_; }
+
+private:
+  void *ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+template <typename T> DeviceBuffer upload(const std::vector<T> &h) {
+  DeviceBuffer b(h.size() * sizeof(T));
+  if (!h.empty()) PMG_CUDA(cudaMemcpy(b.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return b;
+}
+
+inline size_t dtype_size(int dtype) { return dtype == PMG_F64 ? 8 : 4; }
+
+// ---------------------------------------------------------------------------------------
+// 1D tables (tables.cpp)
+// ---------------------------------------------------------------------------------------
+struct Tables1D {
+  int p = 0, nq = 0;
+  std::vector<double> S;  // [nm][nq]  GLL Lagrange basis at Gauss points
+  std::vector<double> SD; // [nm][nq]  its derivative
+  std::vector<double> D;  // [nq][nq]  collocation derivative on the Gauss points
+  std::vector<double> W;  // [nq]      Gauss weights on [0,1]
+  std::vector<double> xg, xl;
+};
+Tables1D make_tables(int p, int nq);
+std::vector<double> gauss_lobatto_points(int n);
+std::vector<double> p_transfer_matrix(int pc, int pf);  // [nc][nf]
+std::vector<double> h_transfer_matrix(int p);           // [p+1][2p+1]
+
+// ---------------------------------------------------------------------------------------
+// meshes and numbering (mesh.cpp)
+// ---------------------------------------------------------------------------------------
+struct BoxMesh {
+  pmg_box box{};
+  int64_t n[3] = {0, 0, 0};
+  int64_t n_cells = 0;
+  std::vector<int32_t> cell_xyz; // [C][3]
+};
+
+struct Numbering {
+  int p = 0;
+  int64_t n_dofs = 0;
+  std::vector<uint32_t> plain;      // [C][nm^3] lexicographic, no sentinel
+  std::vector<uint8_t> constrained; // [N]
+  std::vector<uint32_t> lattice;    // node lattice (x fastest) -> dof
+  int64_t L[3] = {0, 0, 0};         // lattice extents p*n+1
+};
+
+BoxMesh make_box(const pmg_box &b);
+Numbering make_numbering(const BoxMesh &m, int p, bool keep_lattice);
+
+} // namespace pmg
+
+// ---------------------------------------------------------------------------------------
+// opaque handle types of the C ABI
+// ---------------------------------------------------------------------------------------
+struct pmg_mesh {
+  pmg::BoxMesh m;
+};
+
+struct pmg_operator {
+  int device = 0;
+  int degree = 1, nm = 2, nq = 2;
+  int dtype = PMG_F64;
+  int geometry = PMG_GEOMETRY_FULL; // resolved: FULL or AFFINE
+  int coeff_kind = PMG_COEFF_NONE;
+  bool has_coeff_values = false;    // affine: per-qp factors stored
+  pmg::BoxMesh mesh;
+  int64_t n_cells = 0, n_dofs = 0;
+  int cpw = 1, lanes = 1;           // cells per warp group, active lanes per group
+  int64_t n_groups = 0;
+  pmg::Numbering num;               // host copy (plain indices, constrained, lattice)
+  pmg::DeviceBuffer idx;            // permuted [group][nm^2][lanes] uint32
+  pmg::DeviceBuffer geo;            // FULL: [group][nq^2][6][lanes]; AFFINE: [C][8]
+  pmg::DeviceBuffer coef;           // AFFINE with coefficient: [group][nq^2][lanes]
+  pmg::DeviceBuffer constrained_list; // uint32 [n_constrained]
+  int64_t n_constrained = 0;
+  pmg::DeviceBuffer inv_diag;       // [N] dtype
+  bool has_diag = false;
+  int grid_vmult = 0, grid_diag = 0;
+};
+
+namespace pmg {
+// operator.cu
+void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_params &prm);
+void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s,
+                    bool compute = true);
+void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s);
+void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, cudaStream_t s);
+void operator_copy_geometry(const pmg_operator &op, double *host);
+int64_t operator_bytes(const pmg_operator &op);
+} // namespace pmg

@@ -1,0 +1,267 @@
+// Chebyshev-Jacobi smoother, V-cycle and preconditioned CG, orchestrated on the host over
+// the device kernels.  The algorithms restate deal.II's PreconditionChebyshev and SolverCG
+// as the reference configures them (tests/poisson_cube_bk3/program.cc:474-515) and the
+// reference's multigrid driver (tests/common/portable_multigrid_solver.h:147-271,
+// include/multigrid/portable_v_cycle_multigrid.h:163-206).
+#include <cmath>
+#include <vector>
+
+#include "pmg_internal.hpp"
+#include "solver.hpp"
+#include "transfer.hpp"
+#include "vector_ops.hpp"
+
+namespace pmg {
+namespace {
+
+int sturm_count(const std::vector<double> &a, const std::vector<double> &b, double x) {
+  int cnt = 0;
+  double d = 1.0;
+  for (size_t i = 0; i < a.size(); ++i) {
+    d = a[i] - x - (i > 0 ? b[i - 1] * b[i - 1] / d : 0.0);
+    if (d == 0.0) d = -1e-300;
+    if (d < 0) ++cnt;
+  }
+  return cnt;
+}
+
+// extreme eigenvalue of a symmetric tridiagonal matrix by Sturm-sequence bisection
+double tridiag_extreme(const std::vector<double> &a, const std::vector<double> &b, bool largest) {
+  const size_t n = a.size();
+  double lo = 1e300, hi = -1e300;
+  for (size_t i = 0; i < n; ++i) {
+    const double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(b[i]) : 0.0);
+    lo = std::min(lo, a[i] - r);
+    hi = std::max(hi, a[i] + r);
+  }
+  const int target = largest ? (int)n : 1;
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (sturm_count(a, b, mid) >= target) hi = mid;
+    else lo = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+void check_finite(double v, const char *what) {
+  if (!std::isfinite(v)) fail(PMG_ENONFINITE, std::string("non-finite value in ") + what);
+}
+
+} // namespace
+
+void chebyshev_setup(pmg_chebyshev &c, pmg_operator &op, const pmg_chebyshev_params &prm) {
+  PMG_REQUIRE(prm.smoothing_range > 0, "smoothing_range must be positive");
+  PMG_REQUIRE(prm.eig_cg_n_iterations >= 0, "eig_cg_n_iterations must be >= 0");
+  c.op = &op;
+  c.degree = prm.degree;
+  c.range = prm.smoothing_range;
+  c.eig_its = prm.eig_cg_n_iterations;
+  const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
+  PMG_CUDA(cudaSetDevice(op.device));
+  c.xo.allocate(bytes);
+  c.Ax.allocate(bytes);
+  if (!op.has_diag) {
+    operator_compute_inverse_diagonal(op, nullptr);
+    PMG_CUDA(cudaDeviceSynchronize());
+  }
+}
+
+// deal.II PreconditionChebyshev::estimate_eigenvalues: at most eig_its CG steps (tolerance
+// 1e-10) from x = 0 on v_i = (i mod 11) - mean with the Jacobi preconditioner; Lanczos
+// matrix from the CG coefficients with a one-step lag; max scaled by 1.2; interval
+// [alpha, max] with alpha = max/range (range > 1) or min(0.9 max, min); invalid degree
+// chosen by the Chebyshev error bound for the target `range`.
+void chebyshev_estimate(pmg_chebyshev &c, cudaStream_t s) {
+  pmg_operator &op = *c.op;
+  const int dt = op.dtype;
+  const int64_t N = op.n_dofs;
+  const size_t bytes = dtype_size(dt) * N;
+  DeviceBuffer x(bytes), r(bytes), z(bytes), p(bytes), v(bytes);
+  PMG_CUDA(cudaMemsetAsync(x.get(), 0, bytes, s));
+  vec::fill_mod11(r.get(), dt, N, s);
+  std::vector<double> diag, offd;
+  double res = std::sqrt(vec::dot(r.get(), r.get(), dt, N, s));
+  int it = 0;
+  if (!(res <= 1e-10) && c.eig_its > 0) {
+    double rho = vec::jacobi_dot(z.get(), op.inv_diag.get(), r.get(), dt, N, s);
+    double rho_old = rho, alpha = 0, prev_alpha = 0, beta = 0, eig_beta_alpha = 0;
+    while (true) {
+      ++it;
+      if (it > 1) {
+        beta = rho / rho_old;
+        vec::xpay(p.get(), z.get(), beta, dt, N, s);
+      } else {
+        PMG_CUDA(cudaMemcpyAsync(p.get(), z.get(), bytes, cudaMemcpyDeviceToDevice, s));
+      }
+      operator_vmult(op, v.get(), p.get(), s);
+      prev_alpha = alpha;
+      const double pv = vec::dot(p.get(), v.get(), dt, N, s);
+      check_finite(pv, "Chebyshev eigenvalue estimate");
+      alpha = rho / pv;
+      res = std::sqrt(vec::cg_update(x.get(), r.get(), p.get(), v.get(), alpha, dt, N, s));
+      rho_old = rho;
+      rho = vec::jacobi_dot(z.get(), op.inv_diag.get(), r.get(), dt, N, s);
+      if (it > 1) {
+        diag.push_back(1.0 / prev_alpha + eig_beta_alpha);
+        eig_beta_alpha = beta / prev_alpha;
+        offd.push_back(std::sqrt(beta) / prev_alpha);
+      }
+      if (it >= c.eig_its || res <= 1e-10) break;
+    }
+  }
+  c.cg_its = it;
+  if (diag.empty()) {
+    c.min_ev = c.max_ev = 1.0;
+  } else {
+    c.min_ev = tridiag_extreme(diag, offd, false);
+    c.max_ev = 1.2 * tridiag_extreme(diag, offd, true);
+  }
+  const double alpha_ev = c.range > 1.0 ? c.max_ev / c.range : std::min(0.9 * c.max_ev, c.min_ev);
+  if (c.degree <= 0) {
+    const double actual = c.max_ev / alpha_ev;
+    const double sigma = (1.0 - std::sqrt(1.0 / actual)) / (1.0 + std::sqrt(1.0 / actual));
+    const double eps = c.range;
+    c.degree = 1 + (int)(std::log(1.0 / eps + std::sqrt(1.0 / eps / eps - 1.0)) / std::log(1.0 / sigma));
+  }
+  c.delta = (c.max_ev - alpha_ev) * 0.5;
+  c.theta = (c.max_ev + alpha_ev) * 0.5;
+  c.estimated = true;
+  PMG_CUDA(cudaStreamSynchronize(s)); // the work vectors are freed on return
+}
+
+// Chebyshev iteration of the first kind: vmult from x = 0 (degree-1 products), step from dst
+// (degree products); x_{k+1} = x_k + f1 (x_k - x_{k-1}) + f2 D^{-1}(b - A x_k).
+void chebyshev_apply(pmg_chebyshev &c, void *dst, const void *src, bool from_zero, cudaStream_t s) {
+  if (!c.estimated) chebyshev_estimate(c, s);
+  pmg_operator &op = *c.op;
+  const int dt = op.dtype;
+  const int64_t N = op.n_dofs;
+  if (from_zero) {
+    vec::cheb_init(dst, c.xo.get(), src, op.inv_diag.get(), 1.0 / c.theta, dt, N, s);
+  } else {
+    operator_vmult(op, c.Ax.get(), dst, s);
+    vec::cheb_first_step(dst, c.xo.get(), src, c.Ax.get(), op.inv_diag.get(), 1.0 / c.theta, dt, N, s);
+  }
+  if (c.degree < 2 || std::fabs(c.delta) < 1e-40) return;
+  double rhok = c.delta / c.theta;
+  const double sigma = c.theta / c.delta;
+  for (int k = 1; k < c.degree; ++k) {
+    operator_vmult(op, c.Ax.get(), dst, s);
+    const double rhokp = 1.0 / (2.0 * sigma - rhok);
+    const double f1 = rhokp * rhok, f2 = 2.0 * rhokp / c.delta;
+    rhok = rhokp;
+    vec::cheb_update(dst, c.xo.get(), src, c.Ax.get(), op.inv_diag.get(), f1, f2, dt, N, s);
+  }
+}
+
+void mg_setup(pmg_mg &mg, int n_levels, pmg_operator *const *levels, pmg_transfer *const *transfers,
+              pmg_chebyshev *const *smoothers) {
+  PMG_REQUIRE(n_levels >= 1, "need at least one level");
+  mg.levels.assign(levels, levels + n_levels);
+  mg.transfers.assign(transfers, transfers + n_levels);
+  mg.smoothers.assign(smoothers, smoothers + n_levels);
+  for (int l = 0; l < n_levels; ++l) {
+    PMG_REQUIRE(mg.levels[l] && mg.smoothers[l], "null level operator or smoother");
+    PMG_REQUIRE(mg.smoothers[l]->op == mg.levels[l], "smoother of level does not belong to its operator");
+    if (l > 0) {
+      PMG_REQUIRE(mg.transfers[l], "null transfer");
+      PMG_REQUIRE(mg.transfers[l]->n_coarse == mg.levels[l - 1]->n_dofs &&
+                      mg.transfers[l]->n_fine == mg.levels[l]->n_dofs,
+                  "transfer does not connect consecutive levels");
+    }
+  }
+  PMG_CUDA(cudaSetDevice(mg.levels.back()->device));
+  mg.sol.resize(n_levels);
+  mg.def.resize(n_levels);
+  mg.t.resize(n_levels);
+  for (int l = 0; l < n_levels; ++l) {
+    const size_t bytes = dtype_size(mg.levels[l]->dtype) * mg.levels[l]->n_dofs;
+    mg.sol[l].allocate(bytes);
+    mg.def[l].allocate(bytes);
+    mg.t[l].allocate(bytes);
+  }
+}
+
+void mg_vcycle(pmg_mg &mg, int l, cudaStream_t s) {
+  pmg_operator &op = *mg.levels[l];
+  const int dt = op.dtype;
+  const int64_t N = op.n_dofs;
+  if (l == 0) { // coarse "solve" by the level-0 Chebyshev smoother
+    chebyshev_apply(*mg.smoothers[0], mg.sol[0].get(), mg.def[0].get(), true, s);
+    return;
+  }
+  pmg_operator &opc = *mg.levels[l - 1];
+  chebyshev_apply(*mg.smoothers[l], mg.sol[l].get(), mg.def[l].get(), true, s);
+  operator_vmult(op, mg.t[l].get(), mg.sol[l].get(), s);
+  vec::residual(mg.t[l].get(), mg.def[l].get(), dt, N, s);
+  PMG_CUDA(cudaMemsetAsync(mg.def[l - 1].get(), 0, dtype_size(opc.dtype) * opc.n_dofs, s));
+  transfer_apply(*mg.transfers[l], 1, mg.def[l - 1].get(), mg.t[l].get(), s);
+  mg_vcycle(mg, l - 1, s);
+  transfer_apply(*mg.transfers[l], 0, mg.sol[l].get(), mg.sol[l - 1].get(), s);
+  chebyshev_apply(*mg.smoothers[l], mg.sol[l].get(), mg.def[l].get(), false, s);
+}
+
+void mg_vmult(pmg_mg &mg, void *dst, const void *src, int vec_dtype, cudaStream_t s) {
+  const int L = (int)mg.levels.size() - 1;
+  const pmg_operator &top = *mg.levels[L];
+  for (int l = 0; l < L; ++l) {
+    // defect[level] = 0 below the top (portable_multigrid_solver.h:180-183)
+    PMG_CUDA(cudaMemsetAsync(mg.def[l].get(), 0, dtype_size(mg.levels[l]->dtype) * mg.levels[l]->n_dofs, s));
+  }
+  vec::convert(mg.def[L].get(), top.dtype, src, vec_dtype, top.n_dofs, s);
+  mg_vcycle(mg, L, s);
+  vec::convert(dst, vec_dtype, mg.sol[L].get(), top.dtype, top.n_dofs, s);
+}
+
+// deal.II SolverCG with ReductionControl(max_it, abs_tol, reduce): stop at the first
+// iterate with ||r|| <= max(abs_tol, reduce ||r_0||).
+void cg_solve(pmg_operator &A, pmg_mg *mg, void *x, const void *b, double reduce, double abs_tol,
+              int max_it, pmg_cg_info &info, cudaStream_t s) {
+  PMG_REQUIRE(x && b, "null vector");
+  PMG_REQUIRE(max_it >= 0, "max_iterations must be >= 0");
+  if (mg) PMG_REQUIRE(mg->levels.back()->n_dofs == A.n_dofs, "preconditioner size mismatch");
+  PMG_CUDA(cudaSetDevice(A.device));
+  const int dt = A.dtype;
+  const int64_t N = A.n_dofs;
+  const size_t bytes = dtype_size(dt) * N;
+  if (!mg && !A.has_diag) operator_compute_inverse_diagonal(A, s);
+  DeviceBuffer r(bytes), z(bytes), p(bytes), v(bytes);
+  // r = b - A x
+  operator_vmult(A, v.get(), x, s);
+  PMG_CUDA(cudaMemcpyAsync(r.get(), b, bytes, cudaMemcpyDeviceToDevice, s));
+  vec::residual(v.get(), r.get(), dt, N, s);
+  PMG_CUDA(cudaMemcpyAsync(r.get(), v.get(), bytes, cudaMemcpyDeviceToDevice, s));
+  double res = std::sqrt(vec::dot(r.get(), r.get(), dt, N, s));
+  check_finite(res, "CG residual");
+  info = pmg_cg_info{};
+  info.initial_residual = res;
+  const double tol = std::max(abs_tol, reduce * res);
+  int it = 0;
+  double rho = 0, rho_old = 0;
+  while (res > tol && it < max_it) {
+    if (mg) {
+      mg_vmult(*mg, z.get(), r.get(), dt, s);
+      rho = vec::dot(r.get(), z.get(), dt, N, s);
+    } else {
+      rho = vec::jacobi_dot(z.get(), A.inv_diag.get(), r.get(), dt, N, s);
+    }
+    check_finite(rho, "CG preconditioned residual");
+    if (it == 0) PMG_CUDA(cudaMemcpyAsync(p.get(), z.get(), bytes, cudaMemcpyDeviceToDevice, s));
+    else vec::xpay(p.get(), z.get(), rho / rho_old, dt, N, s);
+    rho_old = rho;
+    ++it;
+    operator_vmult(A, v.get(), p.get(), s);
+    const double pv = vec::dot(p.get(), v.get(), dt, N, s);
+    check_finite(pv, "CG curvature");
+    if (pv <= 0) fail(PMG_ENOCONV, "CG breakdown: p.Ap <= 0");
+    res = std::sqrt(vec::cg_update(x, r.get(), p.get(), v.get(), rho / pv, dt, N, s));
+    check_finite(res, "CG residual");
+  }
+  info.iterations = it;
+  info.final_residual = res;
+  info.converged = res <= tol ? 1 : 0;
+  info.reduction_per_step = it > 0 ? std::pow(res / info.initial_residual, 1.0 / it) : 1.0;
+  PMG_CUDA(cudaStreamSynchronize(s));
+}
+
+} // namespace pmg

@@ -1,0 +1,35 @@
+// Smoother, multigrid and CG objects (solver.cu).
+#pragma once
+
+#include <vector>
+
+#include "pmg_internal.hpp"
+
+struct pmg_chebyshev {
+  pmg_operator *op = nullptr;
+  int degree = 0;
+  double range = 15.0;
+  int eig_its = 10;
+  bool estimated = false;
+  double theta = 1, delta = 0, min_ev = 1, max_ev = 1;
+  int cg_its = 0;
+  pmg::DeviceBuffer xo, Ax;
+};
+
+struct pmg_mg {
+  std::vector<pmg_operator *> levels;
+  std::vector<pmg_transfer *> transfers;
+  std::vector<pmg_chebyshev *> smoothers;
+  std::vector<pmg::DeviceBuffer> sol, def, t;
+};
+
+namespace pmg {
+void chebyshev_setup(pmg_chebyshev &c, pmg_operator &op, const pmg_chebyshev_params &prm);
+void chebyshev_estimate(pmg_chebyshev &c, cudaStream_t s);
+void chebyshev_apply(pmg_chebyshev &c, void *dst, const void *src, bool from_zero, cudaStream_t s);
+void mg_setup(pmg_mg &mg, int n_levels, pmg_operator *const *levels, pmg_transfer *const *transfers,
+              pmg_chebyshev *const *smoothers);
+void mg_vmult(pmg_mg &mg, void *dst, const void *src, int vec_dtype, cudaStream_t s);
+void cg_solve(pmg_operator &A, pmg_mg *mg, void *x, const void *b, double reduce, double abs_tol,
+              int max_it, pmg_cg_info &info, cudaStream_t s);
+} // namespace pmg

@@ -1,0 +1,21 @@
+// Multigrid transfer objects (transfer.cu).
+#pragma once
+
+#include "pmg_internal.hpp"
+
+struct pmg_transfer {
+  int device = 0;
+  int dtype = PMG_F64;
+  int kind = 0; // 0 polynomial, 1 geometric
+  int nc = 0, nf = 0;
+  int64_t n_patches = 0, n_coarse = 0, n_fine = 0;
+  pmg::DeviceBuffer P1d, coarse_idx, fine_idx, weights;
+  int ppb = 1, grid = 1;
+  size_t smem = 0;
+};
+
+namespace pmg {
+void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_operator &fine);
+// dir 0: dst_fine += P src_coarse;  dir 1: dst_coarse += P^T src_fine
+void transfer_apply(const pmg_transfer &t, int dir, void *dst, const void *src, cudaStream_t s);
+} // namespace pmg

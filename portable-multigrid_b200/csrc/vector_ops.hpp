@@ -1,0 +1,29 @@
+// Vector kernels used by the smoother, the V-cycle and CG (vector_ops.cu).  Every function
+// enqueues on `s`; the ones returning a double synchronise `s` to read the reduction.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace pmg {
+namespace vec {
+
+void fill_mod11(void *x, int dtype, int64_t n, cudaStream_t s);
+void convert(void *dst, int dt_dst, const void *src, int dt_src, int64_t n, cudaStream_t s);
+void cheb_init(void *dst, void *xo, const void *src, const void *invd, double scale, int dtype,
+               int64_t n, cudaStream_t s);
+void cheb_first_step(void *dst, void *xo, const void *src, const void *Ax, const void *invd,
+                     double scale, int dtype, int64_t n, cudaStream_t s);
+void cheb_update(void *dst, void *xo, const void *src, const void *Ax, const void *invd, double f1,
+                 double f2, int dtype, int64_t n, cudaStream_t s);
+void residual(void *t, const void *def, int dtype, int64_t n, cudaStream_t s);
+void jacobi(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s);
+void xpay(void *p, const void *z, double beta, int dtype, int64_t n, cudaStream_t s);
+double dot(const void *a, const void *b, int dtype, int64_t n, cudaStream_t s);
+double cg_update(void *x, void *r, const void *p, const void *v, double alpha, int dtype, int64_t n,
+                 cudaStream_t s);
+double jacobi_dot(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s);
+
+} // namespace vec
+} // namespace pmg

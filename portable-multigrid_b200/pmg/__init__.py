@@ -1,0 +1,460 @@
+"""Python bindings of libpmg_b200.so over its C ABI (include/pmg/pmg.h).
+
+The classes mirror the reference's C++ interfaces for the matrix-free multigrid path so
+that code written against those reads the same here:
+
+  LaplaceOperator  ~ Portable::LaplaceOperatorBase / LaplaceOperatorBK3
+                     (vmult, Tvmult, vmult_dummy, compute_diagonal,
+                      get_matrix_diagonal_inverse, m, n, el)
+  Transfer         ~ Portable::MGTransferBase (prolongate_and_add, restrict_and_add)
+  Chebyshev        ~ deal.II PreconditionChebyshev (vmult, step)
+  VCycleMultigrid  ~ Portable::VCycleMultigridBase (vmult)
+  solve_cg         ~ MultigridSolver::solve_cg
+
+Vectors are torch CUDA tensors (float64 or float32) on the operator's device; the
+library works on the tensors' memory in place, ordered on torch's current stream.
+There is no CPU fallback: without the built library or a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+REPO_ROOT = os.path.dirname(PKG_ROOT)
+LIB_PATH = os.path.join(PKG_ROOT, "libpmg_b200.so")
+HEADER_PATH = os.path.join(REPO_ROOT, "include", "pmg", "pmg.h")
+
+F64, F32 = 0, 1
+GEOMETRY_AUTO, GEOMETRY_FULL, GEOMETRY_AFFINE = 0, 1, 2
+COEFF_NONE, COEFF_KAPPA, COEFF_VALUES = 0, 1, 2
+INVALID = 0xFFFFFFFF
+STATUS = {0: "PMG_OK", -1: "PMG_EINVAL", -2: "PMG_ENOMEM", -3: "PMG_ECUDA",
+          -4: "PMG_ENONFINITE", -5: "PMG_ENOCONV", -6: "PMG_EBOUNDS", -7: "PMG_ESTATE",
+          -8: "PMG_ENODEV"}
+
+
+class PmgError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Box(C.Structure):
+    _fields_ = [("coarse", C.c_int32 * 3), ("refine", C.c_int32), ("lo", C.c_double * 3),
+                ("hi", C.c_double * 3), ("deform", C.c_int32), ("amp", C.c_double),
+                ("dirichlet_mask", C.c_int32)]
+
+    @staticmethod
+    def make(coarse=(1, 1, 1), refine=0, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), deform=0,
+             amp=0.1, dirichlet_mask=0x3F):
+        b = Box()
+        b.coarse[:] = list(coarse)
+        b.refine = refine
+        b.lo[:] = list(lo)
+        b.hi[:] = list(hi)
+        b.deform = deform
+        b.amp = amp
+        b.dirichlet_mask = dirichlet_mask
+        return b
+
+    def with_refine(self, r):
+        return Box.make(tuple(self.coarse), r, tuple(self.lo), tuple(self.hi), self.deform,
+                        self.amp, self.dirichlet_mask)
+
+    def ncells(self):
+        return int(np.prod([c << self.refine for c in self.coarse]))
+
+
+def doubling_box(cycle: int) -> Box:
+    """The "doubling" mesh of the reference benchmark (tests/poisson_cube_bk3/program.cc:937-957)."""
+    n_refine, remainder = cycle // 3, cycle % 3
+    coarse = [2 if d < remainder else 1 for d in range(3)]
+    hi = [2.8 if d < remainder else 0.9 for d in range(3)]
+    return Box.make(coarse=coarse, refine=n_refine, lo=(-1.0, -1.0, -1.0), hi=hi)
+
+
+class OperatorParams(C.Structure):
+    _fields_ = [("degree", C.c_int32), ("dtype", C.c_int32), ("geometry", C.c_int32),
+                ("coeff_kind", C.c_int32), ("coeff_qp", C.c_void_p), ("device", C.c_int32)]
+
+
+class ChebyshevParams(C.Structure):
+    _fields_ = [("degree", C.c_int32), ("smoothing_range", C.c_double),
+                ("eig_cg_n_iterations", C.c_int32)]
+
+
+class CGInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32),
+                ("initial_residual", C.c_double), ("final_residual", C.c_double),
+                ("reduction_per_step", C.c_double)]
+
+
+_lib = None
+
+
+def build(jobs: int = 8):
+    """Compile libpmg_b200.so for sm_100a (make in the package directory)."""
+    subprocess.run(["make", "-s", "-j", str(jobs)], cwd=PKG_ROOT, check=True)
+
+
+def header_functions():
+    """Names of the functions include/pmg/pmg.h declares."""
+    with open(HEADER_PATH) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pmg_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib():
+    """Load the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PmgError(-8, f"{LIB_PATH} is missing: build it with pmg.build()")
+        L = C.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L):
+    vp, i32, i64, d = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    P = C.POINTER
+    sig = {
+        "pmg_last_error": ([C.c_char_p, C.c_size_t], C.c_size_t),
+        "pmg_status_string": ([i32], C.c_char_p),
+        "pmg_version": ([P(i32), P(i32)], i32),
+        "pmg_mesh_create_box": ([P(Box), P(vp)], i32),
+        "pmg_mesh_destroy": ([vp], i32),
+        "pmg_mesh_n_cells": ([vp, P(i64)], i32),
+        "pmg_operator_create": ([vp, P(OperatorParams), P(vp)], i32),
+        "pmg_operator_destroy": ([vp], i32),
+        "pmg_operator_m": ([vp, P(i64)], i32),
+        "pmg_operator_n": ([vp, P(i64)], i32),
+        "pmg_operator_n_cells": ([vp, P(i64)], i32),
+        "pmg_operator_degree": ([vp, P(i32), P(i32)], i32),
+        "pmg_operator_vmult": ([vp, vp, vp, vp], i32),
+        "pmg_operator_tvmult": ([vp, vp, vp, vp], i32),
+        "pmg_operator_vmult_dummy": ([vp, vp, vp, i32, i32, vp], i32),
+        "pmg_operator_compute_diagonal": ([vp, vp], i32),
+        "pmg_operator_get_inverse_diagonal": ([vp, P(vp)], i32),
+        "pmg_operator_copy_inverse_diagonal": ([vp, vp, vp], i32),
+        "pmg_operator_el": ([vp, i64, i64, P(d)], i32),
+        "pmg_operator_bytes_per_vmult": ([vp, P(i64)], i32),
+        "pmg_operator_assemble_rhs": ([vp, i32, i32, vp, vp], i32),
+        "pmg_operator_copy_dof_indices": ([vp, vp], i32),
+        "pmg_operator_copy_constrained": ([vp, vp], i32),
+        "pmg_operator_copy_geometry": ([vp, vp], i32),
+        "pmg_transfer_create": ([vp, vp, P(vp)], i32),
+        "pmg_transfer_destroy": ([vp], i32),
+        "pmg_transfer_prolongate_and_add": ([vp, vp, vp, vp], i32),
+        "pmg_transfer_restrict_and_add": ([vp, vp, vp, vp], i32),
+        "pmg_chebyshev_create": ([vp, P(ChebyshevParams), P(vp)], i32),
+        "pmg_chebyshev_destroy": ([vp], i32),
+        "pmg_chebyshev_estimate": ([vp, vp], i32),
+        "pmg_chebyshev_vmult": ([vp, vp, vp, vp], i32),
+        "pmg_chebyshev_step": ([vp, vp, vp, vp], i32),
+        "pmg_chebyshev_info": ([vp, P(d), P(d), P(i32), P(i32)], i32),
+        "pmg_mg_create": ([i32, P(vp), P(vp), P(vp), P(vp)], i32),
+        "pmg_mg_destroy": ([vp], i32),
+        "pmg_mg_vmult": ([vp, vp, vp, i32, vp], i32),
+        "pmg_cg_solve": ([vp, vp, vp, vp, d, d, i32, P(CGInfo), vp], i32),
+        "pmg_profile_enable": ([i32], i32),
+        "pmg_profile_reset": ([], i32),
+        "pmg_profile_query": ([C.c_char_p, P(d), P(i64)], i32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(2048)
+    lib().pmg_last_error(buf, 2048)
+    return buf.value.decode(errors="replace")
+
+
+def check(status):
+    if status != 0:
+        raise PmgError(status, last_error())
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def profile_enable(on=True):
+    check(lib().pmg_profile_enable(int(on)))
+
+
+def profile_reset():
+    check(lib().pmg_profile_reset())
+
+
+def profile_query(kernel):
+    """(total device milliseconds, launches) of a kernel label since the last reset."""
+    ms, n = C.c_double(), C.c_int64()
+    check(lib().pmg_profile_query(kernel.encode(), C.byref(ms), C.byref(n)))
+    return ms.value, n.value
+
+
+class Mesh:
+    def __init__(self, box: Box):
+        self.box = box
+        self.h = C.c_void_p()
+        check(lib().pmg_mesh_create_box(C.byref(box), C.byref(self.h)))
+
+    def n_cells(self):
+        n = C.c_int64()
+        check(lib().pmg_mesh_n_cells(self.h, C.byref(n)))
+        return n.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pmg_mesh_destroy(self.h)
+            self.h = None
+
+
+class LaplaceOperator:
+    """Continuous FE_Q(degree) Laplace operator on a box mesh (LaplaceOperatorBK3)."""
+
+    def __init__(self, mesh: Mesh, degree: int, dtype: int = F64, geometry: int = GEOMETRY_AUTO,
+                 coeff_kind: int = COEFF_NONE, coeff_qp=None, device: int = 0):
+        self.mesh = mesh
+        self.degree = degree
+        self.dtype = dtype
+        self.device = device
+        self._coeff = None
+        prm = OperatorParams(degree, dtype, geometry, coeff_kind, None, device)
+        if coeff_qp is not None:
+            self._coeff = np.ascontiguousarray(coeff_qp, dtype=np.float64)
+            prm.coeff_qp = self._coeff.ctypes.data_as(C.c_void_p)
+        self.h = C.c_void_p()
+        check(lib().pmg_operator_create(mesh.h, C.byref(prm), C.byref(self.h)))
+
+    @property
+    def torch_dtype(self):
+        import torch
+        return torch.float64 if self.dtype == F64 else torch.float32
+
+    def m(self):
+        n = C.c_int64()
+        check(lib().pmg_operator_m(self.h, C.byref(n)))
+        return n.value
+
+    n = m
+
+    def n_cells(self):
+        n = C.c_int64()
+        check(lib().pmg_operator_n_cells(self.h, C.byref(n)))
+        return n.value
+
+    def initialize_dof_vector(self):
+        import torch
+        return torch.zeros(self.m(), dtype=self.torch_dtype, device=f"cuda:{self.device}")
+
+    def vmult(self, dst, src):
+        check(lib().pmg_operator_vmult(self.h, _ptr(dst), _ptr(src), _stream()))
+
+    def Tvmult(self, dst, src):
+        check(lib().pmg_operator_tvmult(self.h, _ptr(dst), _ptr(src), _stream()))
+
+    def vmult_dummy(self, dst, src, ghost_exchange_on=True, computation_on=True):
+        check(lib().pmg_operator_vmult_dummy(self.h, _ptr(dst), _ptr(src), int(ghost_exchange_on),
+                                             int(computation_on), _stream()))
+
+    def compute_diagonal(self):
+        check(lib().pmg_operator_compute_diagonal(self.h, _stream()))
+
+    def get_matrix_diagonal_inverse(self):
+        """Returns a torch view of the operator-owned inverse diagonal."""
+        import torch
+        p = C.c_void_p()
+        check(lib().pmg_operator_get_inverse_diagonal(self.h, C.byref(p)))
+        n = self.m()
+        out = torch.empty(n, dtype=self.torch_dtype, device=f"cuda:{self.device}")
+        # a copy, so the tensor does not alias library memory
+        check(lib().pmg_operator_copy_inverse_diagonal(self.h, _ptr(out), _stream()))
+        return out
+
+    def el(self, row, col):
+        v = C.c_double()
+        check(lib().pmg_operator_el(self.h, row, col, C.byref(v)))
+        return v.value
+
+    def bytes_per_vmult(self):
+        b = C.c_int64()
+        check(lib().pmg_operator_bytes_per_vmult(self.h, C.byref(b)))
+        return b.value
+
+    def assemble_rhs(self, f_kind=0, nq=0):
+        b = self.initialize_dof_vector()
+        check(lib().pmg_operator_assemble_rhs(self.h, f_kind, nq, _ptr(b), _stream()))
+        return b
+
+    def dof_indices(self):
+        nm3 = (self.degree + 1) ** 3
+        out = np.zeros(self.n_cells() * nm3, dtype=np.uint32)
+        check(lib().pmg_operator_copy_dof_indices(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out.reshape(-1, nm3)
+
+    def constrained(self):
+        out = np.zeros(self.m(), dtype=np.uint8)
+        check(lib().pmg_operator_copy_constrained(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def geometry(self):
+        nq3 = (self.degree + 1) ** 3
+        out = np.zeros(self.n_cells() * 6 * nq3)
+        check(lib().pmg_operator_copy_geometry(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out.reshape(-1, 6, nq3)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pmg_operator_destroy(self.h)
+            self.h = None
+
+
+class Transfer:
+    """PolynomialTransfer / GeometricTransfer between two level operators."""
+
+    def __init__(self, coarse: LaplaceOperator, fine: LaplaceOperator):
+        self.coarse, self.fine = coarse, fine
+        self.h = C.c_void_p()
+        check(lib().pmg_transfer_create(coarse.h, fine.h, C.byref(self.h)))
+
+    def prolongate_and_add(self, dst_fine, src_coarse):
+        check(lib().pmg_transfer_prolongate_and_add(self.h, _ptr(dst_fine), _ptr(src_coarse), _stream()))
+
+    def restrict_and_add(self, dst_coarse, src_fine):
+        check(lib().pmg_transfer_restrict_and_add(self.h, _ptr(dst_coarse), _ptr(src_fine), _stream()))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pmg_transfer_destroy(self.h)
+            self.h = None
+
+
+class Chebyshev:
+    """PreconditionChebyshev with the operator's inverse diagonal (degree <= 0: automatic)."""
+
+    def __init__(self, op: LaplaceOperator, degree=5, smoothing_range=15.0, eig_cg_n_iterations=10):
+        self.op = op
+        prm = ChebyshevParams(degree, smoothing_range, eig_cg_n_iterations)
+        self.h = C.c_void_p()
+        check(lib().pmg_chebyshev_create(op.h, C.byref(prm), C.byref(self.h)))
+
+    def estimate(self):
+        check(lib().pmg_chebyshev_estimate(self.h, _stream()))
+
+    def vmult(self, dst, src):
+        check(lib().pmg_chebyshev_vmult(self.h, _ptr(dst), _ptr(src), _stream()))
+
+    def step(self, dst, src):
+        check(lib().pmg_chebyshev_step(self.h, _ptr(dst), _ptr(src), _stream()))
+
+    def info(self):
+        mn, mx, deg, its = C.c_double(), C.c_double(), C.c_int32(), C.c_int32()
+        check(lib().pmg_chebyshev_info(self.h, C.byref(mn), C.byref(mx), C.byref(deg), C.byref(its)))
+        return {"min_eigenvalue": mn.value, "max_eigenvalue": mx.value, "degree": deg.value,
+                "cg_iterations": its.value}
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pmg_chebyshev_destroy(self.h)
+            self.h = None
+
+
+class VCycleMultigrid:
+    """V-cycle over levels[0] (coarsest) .. levels[-1] (finest)."""
+
+    def __init__(self, levels, transfers, smoothers):
+        self.levels, self.transfers, self.smoothers = levels, transfers, smoothers
+        n = len(levels)
+        lv = (C.c_void_p * n)(*[o.h for o in levels])
+        tr = (C.c_void_p * n)(*([None] + [t.h for t in transfers[1:]]))
+        sm = (C.c_void_p * n)(*[s.h for s in smoothers])
+        self.h = C.c_void_p()
+        check(lib().pmg_mg_create(n, lv, tr, sm, C.byref(self.h)))
+
+    def vmult(self, dst, src):
+        import torch
+        vd = F64 if src.dtype == torch.float64 else F32
+        check(lib().pmg_mg_vmult(self.h, _ptr(dst), _ptr(src), vd, _stream()))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pmg_mg_destroy(self.h)
+            self.h = None
+
+
+def solve_cg(A: LaplaceOperator, x, b, precond: VCycleMultigrid | None = None, reduce=1e-9,
+             abs_tol=1e-16, max_iterations=100, raise_on_noconv=True):
+    info = CGInfo()
+    st = lib().pmg_cg_solve(A.h, precond.h if precond is not None else None, _ptr(x), _ptr(b),
+                            reduce, abs_tol, max_iterations, C.byref(info), _stream())
+    if st != 0 and not (st == -5 and not raise_on_noconv):
+        raise PmgError(st, last_error())
+    return {"iterations": info.iterations, "converged": bool(info.converged),
+            "initial_residual": info.initial_residual, "final_residual": info.final_residual,
+            "reduction_per_step": info.reduction_per_step}
+
+
+class Hierarchy:
+    """The ph-multigrid hierarchy of the reference's LaplaceProblem
+    (tests/poisson_cube_bk3/program.cc:263-515): FE_Q(1) on every refinement of the box
+    (h-levels), then the degrees of `pseq` (descending, ending in 1) on the finest mesh;
+    Chebyshev(cheb_degree, range 15, 10 eigenvalue iterations) on levels > 0 and
+    Chebyshev-to-1e-3 on level 0.  The finest-level FP64 operator `fine64` is the CG matrix."""
+
+    def __init__(self, box: Box, pseq, mg_dtype=F32, cheb_degree=5, geometry=GEOMETRY_AUTO,
+                 coeff_kind=COEFF_NONE, coeff_qp=None, device=0, smoothing_range=15.0,
+                 eig_iterations=10, coarse_dtype=None):
+        assert pseq[-1] == 1 and list(pseq) == sorted(pseq, reverse=True)
+        self.box = box
+        coarse_dtype = mg_dtype if coarse_dtype is None else coarse_dtype
+        self.meshes = [Mesh(box.with_refine(r)) for r in range(box.refine + 1)]
+        self.levels, self.transfers, self.smoothers = [], [None], []
+        n_h = box.refine + 1
+        degrees = [1] * n_h + list(reversed(pseq))[1:]
+        for l, p in enumerate(degrees):
+            mesh = self.meshes[min(l, n_h - 1)]
+            dt = coarse_dtype if l == 0 else mg_dtype
+            finest = l == len(degrees) - 1
+            kind = coeff_kind if (coeff_kind != COEFF_VALUES or finest) else COEFF_NONE
+            self.levels.append(LaplaceOperator(mesh, p, dt, geometry, kind,
+                                               coeff_qp if finest else None, device))
+        for l in range(1, len(self.levels)):
+            if self.levels[l].dtype != self.levels[l - 1].dtype:
+                raise ValueError("all multigrid levels must share one dtype")
+            self.transfers.append(Transfer(self.levels[l - 1], self.levels[l]))
+        for l, op in enumerate(self.levels):
+            if l == 0:
+                self.smoothers.append(Chebyshev(op, 0, 1e-3, op.m()))
+            else:
+                self.smoothers.append(Chebyshev(op, cheb_degree, smoothing_range, eig_iterations))
+        self.fine64 = LaplaceOperator(self.meshes[-1], pseq[0], F64, geometry, coeff_kind, coeff_qp,
+                                      device)
+        self.mg = VCycleMultigrid(self.levels, self.transfers, self.smoothers)
+
+    def estimate(self):
+        for s in self.smoothers:
+            s.estimate()
+
+    def solve(self, b, x=None, reduce=1e-9, abs_tol=1e-16, max_iterations=100):
+        if x is None:
+            x = self.fine64.initialize_dof_vector()
+        info = solve_cg(self.fine64, x, b, self.mg, reduce, abs_tol, max_iterations)
+        return x, info
