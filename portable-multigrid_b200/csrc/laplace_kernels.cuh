@@ -7,15 +7,15 @@
 // they compute it is laid out for the B200:
 //
 //  * A warp owns a group of CPW = floor(32/N) consecutive cells (N = p+1 nodes per
-//    direction), N lanes per cell.  Lane s of a cell holds a whole slab of the cell in
-//    registers: the plane y = s ("Y-slab") while gathering, contracting along x and z and
-//    scattering, and the plane z = s ("Z-slab") while contracting along x and y and
-//    applying G.  Contractions along the held plane never leave the registers; switching
-//    slabs is one warp-local exchange through shared memory.  The operator is factored so
-//    that only two such switches (two arrays each) are needed per cell:
-//        Y-slab:  w = Sz Sx u,   wz = SDz Sx u                    (SD = S*D)
-//        Z-slab:  uq = Sy w, dy = SDy w, dz = Sy wz, dx = Dx uq;   f = G grad u
-//                 a = Sy^T SDx^T fx + SDy^T Sx^T fy,   c = Sy^T Sx^T fz
+//    direction), N lanes per cell.  Lane s of a cell works on a slab of the cell: the
+//    plane y = s ("Y-slab") while gathering, contracting along x and z and scattering,
+//    and the plane z = s ("Z-slab") while contracting along x and y and applying G.
+//    Contractions along the slab stay in registers; switching slabs is one warp-local
+//    exchange through shared memory.  The operator is factored (SD = S*D, the derivative of
+//    the nodal basis at the Gauss points) so that only two switches are needed per cell:
+//        Y-slab:  w = Sz Sx u,  wz = SDz Sx u,  wx = Sz SDx u
+//        Z-slab:  dx = Sy wx, dy = SDy w, dz = Sy wz;  f = G grad u;
+//                 a = Sy^T SDx^T fx + SDy^T Sx^T fy,  c = Sy^T Sx^T fz
 //        Y-slab:  out = Sz^T a + SDz^T c
 //    No block-wide barrier is used; warps are independent.
 //  * The index map and G are stored lane-contiguous per group ([group][point][lane]), so
@@ -57,220 +57,361 @@ template <int N> struct Layout {
   static constexpr int N3 = N * N * N;
 };
 
-__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+// L2 eviction policies: the geometry and index streams are read once and should not push
+// the reused src/dst lines out of L2; src gathers and dst atomics should stay.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes, uint64_t pol) {
+  asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(p), "r"(bytes),
+               "l"(pol)
+               : "memory");
+}
+
+// read-only loads with an L2 policy, not allocated in L1
+__device__ __forceinline__ double ld_stream(const double *p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float *p, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t *p, uint64_t pol) {
+  uint32_t v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+// gathered loads that are reused by neighbouring cells
+__device__ __forceinline__ double ld_keep(const double *p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_keep(const float *p, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
 }
 
 __device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void red_keep(double *p, double v, uint64_t pol) {
+  asm volatile("red.global.add.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void red_keep(float *p, float v, uint64_t pol) {
+  asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
+
+// ---- bulk copies into shared memory completed on an mbarrier (sm_90+ async proxy) ----
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst_smem, const void *src, uint32_t bytes,
+                                          uint64_t *bar, uint64_t pol) {
+  // order earlier generic-proxy reads of the destination before the async-proxy write
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+               " [%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst_smem)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+               "selp.u32 %0, 1, 0, p;\n\t}"
+               : "=r"(ok)
+               : "r"(smem_u32(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+// bounded wait: gives up after `limit` polls, records the event in *err and returns false
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  unsigned int *err, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (err) atomicOr(err, 1u);
+  return false;
+}
 
 // GEOM 0: full G per quadrature point, geo = [group][N^2 (q,p)][6][LANES]
 // GEOM 1: affine, geo = [cell][8] (6 used) multiplied by the tensor Gauss weight
 // GEOM 2: affine as 1, times coef = [group][N^2][LANES] per quadrature point
-template <int N, typename T, int GEOM>
-__global__ void __launch_bounds__(128) vmult_slab_kernel(const Tab<N, T> tab,
-                                                         const T *__restrict__ src,
-                                                         T *__restrict__ dst,
-                                                         const uint32_t *__restrict__ idx,
-                                                         const T *__restrict__ geo,
-                                                         const T *__restrict__ coef,
-                                                         int64_t n_groups) {
+//
+// Register budget: every phase streams over one index so that at most ~2 N^2 values are
+// live per lane (the accumulators of the back-contraction plus one column):
+//   phase 1 (Y-slab y=s), per x point p:   t = Sx u, tx = SDx u along k, then
+//            w = Sz t, wz = SDz t, wx = Sz tx  -> shared (z, y=s, p)
+//   phase 2 (Z-slab z=s), per x point p:   dx = Sy wx, dy = SDy w, dz = Sy wz at (., p),
+//            f = G grad u, a += SDx(.,p)^T (Sy^T fx) + Sx(.,p)^T (SDy^T fy);  fz -> shared
+//            (in place over the consumed column of wx), then c = Sy^T Sx^T fz
+//   phase 3 (Y-slab), per x node i:        out = Sz^T a + SDz^T c, scatter
+// Each lane overwrites only its own slab's region of the buffers between the two
+// exchanges, so only the two exchanges (and the end of a group) need a __syncwarp.
+template <int N> struct Stride {
+  // per-cell stride of the exchange buffers, padded where that lowers bank conflicts of
+  // the two exchange patterns (offsets N*s and N*N*s within a cell)
+  static constexpr int CELL = N * N * N + ((N == 3 || N == 5) ? 0 : 1);
+};
+
+template <int N, typename T, int GEOM, bool SMEM_G>
+__device__ __forceinline__ void load_g6(const T *__restrict__ geo, const T *gs,
+                                        const T *__restrict__ coef, const Tab<N, T> &tab,
+                                        int64_t g, int lane, int e, int q, int p, T wr,
+                                        uint64_t pol, T (&c)[6]) {
   using Lo = Layout<N>;
-  constexpr int CPW = Lo::CPW, LANES = Lo::LANES, N2 = Lo::N2, N3 = Lo::N3;
+  constexpr int LANES = Lo::LANES, N2 = Lo::N2, CPW = Lo::CPW;
+  if (GEOM == 0 && SMEM_G) {
+    const T *gp = gs + (q * N + p) * 6 * LANES + lane;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) c[m] = gp[m * LANES];
+  } else if (GEOM == 0) {
+    const T *gp = geo + g * (N2 * 6 * LANES) + (q * N + p) * 6 * LANES + lane;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) c[m] = ld_stream(gp + m * LANES, pol);
+  } else {
+    const T *cg = geo + (g * CPW + e) * 8;
+    T w = wr * tab.W[q] * tab.W[p];
+    if (GEOM == 2) w *= ld_stream(coef + g * (N2 * LANES) + (q * N + p) * LANES + lane, pol);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) c[m] = w * __ldg(cg + m);
+  }
+}
+
+// resident blocks of 128 threads per SM the register allocation is sized for; matches the
+// shared-memory footprint (3 exchange buffers per warp) of each degree and type
+template <int N, typename T> struct MinBlocks {
+  static constexpr int value = sizeof(T) == 8 ? (N >= 6 ? 2 : 3) : 2;
+};
+// outer streaming loops: runtime loops for FP64 (bounded live registers), unrolled for FP32
+// (registers are cheap at 4 bytes and unrolling keeps the tables as immediate operands)
+template <int N, typename T> struct Unroll {
+  static constexpr int value = sizeof(T) == 8 ? 1 : N;
+};
+
+// Shared memory per warp of vmult_slab_kernel: 3 exchange buffers, plus (SMEM_G) the
+// group's geometry block and an mbarrier.
+template <int N, typename T, bool SMEM_G> struct SlabSmem {
+  static constexpr size_t XCHG = size_t(3) * Layout<N>::CPW * Stride<N>::CELL * sizeof(T);
+  static constexpr size_t GEO = SMEM_G ? size_t(Layout<N>::N2) * 6 * Layout<N>::LANES * sizeof(T) : 0;
+  static constexpr size_t PER_WARP = ((GEO + XCHG + 15) / 16) * 16 + (SMEM_G ? 16 : 0);
+};
+
+// SMEM_G: the geometry block of each group (contiguous in the slab layout) is brought into
+// shared memory by one bulk copy issued when the group starts, so that the gather and the
+// first phase overlap with it; launched with one warp per block.
+template <int N, typename T, int GEOM, bool SMEM_G>
+__global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 4 : MinBlocks<N, T>::value))
+    vmult_slab_kernel(const __grid_constant__ Tab<N, T> tab, const T *__restrict__ src, T *__restrict__ dst,
+                      const uint32_t *__restrict__ idx, const T *__restrict__ geo,
+                      const T *__restrict__ coef, int64_t n_groups, unsigned int *err) {
+  using Lo = Layout<N>;
+  constexpr int CPW = Lo::CPW, LANES = Lo::LANES, N2 = Lo::N2;
+  constexpr int CS = Stride<N>::CELL;
   constexpr unsigned MASK = Lo::MASK;
+  constexpr int UNR = SMEM_G ? N : Unroll<N, T>::value;
+  using SM = SlabSmem<N, T, SMEM_G>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   if (lane >= LANES) return;
   const int e = lane / N;
   const int s = lane - e * N;
-  T *bufA = reinterpret_cast<T *>(smem_raw) + (threadIdx.x >> 5) * (2 * CPW * N3) + e * N3;
-  T *bufB = bufA + CPW * N3;
+  unsigned char *wsm = smem_raw + (threadIdx.x >> 5) * SM::PER_WARP;
+  T *gsm = reinterpret_cast<T *>(wsm);                      // geometry block (SMEM_G)
+  T *bufW = reinterpret_cast<T *>(wsm + SM::GEO) + e * CS;  // exchange buffers
+  T *bufZ = bufW + CPW * CS;
+  T *bufX = bufZ + CPW * CS;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(wsm + SM::PER_WARP - 16);
+  if (SMEM_G) {
+    if (lane == 0) mbar_init(bar, 1);
+    __syncwarp(MASK);
+  }
+  uint32_t parity = 0;
   const int64_t warp0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const uint64_t pol_first = policy_evict_first(), pol_last = policy_evict_last();
+  T wr = tab.W[0]; // Gauss weight of this lane's z point (affine geometry)
+#pragma unroll
+  for (int r = 1; r < N; ++r)
+    if (s == r) wr = tab.W[r];
 
   for (int64_t g = warp0; g < n_groups; g += nwarps) {
-    if (GEOM == 0 && lane == 0 && g + nwarps < n_groups)
-      prefetch_l2(geo + (g + nwarps) * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T));
-
-    // ---- gather, Y-slab (y = s): u[k][i] = src at node (i, s, k) ----
+    if (GEOM == 0 && lane == 0) {
+      if (SMEM_G) bulk_load(gsm, geo + g * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T), bar, pol_first);
+      if (g + nwarps < n_groups)
+        prefetch_l2(geo + (g + nwarps) * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T), pol_first);
+    }
     const uint32_t *ig = idx + g * (N2 * LANES) + lane;
-    T t[N][N];
+
+    // ---- phase 1: gather the Y-slab y = s, u[k][i] = src at node (i, s, k) ----
     {
       T u[N][N];
 #pragma unroll
       for (int k = 0; k < N; ++k)
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-          const uint32_t id = __ldg(ig + (k * N + i) * LANES);
-          u[k][i] = (id != kInvalidIdx) ? __ldg(src + id) : T(0);
+          const uint32_t id = ld_stream(ig + (k * N + i) * LANES, pol_first);
+          u[k][i] = (id != kInvalidIdx) ? ld_keep(src + id, pol_last) : T(0);
         }
-      // x: nodes -> Gauss points
-#pragma unroll
-      for (int k = 0; k < N; ++k)
-#pragma unroll
-        for (int p = 0; p < N; ++p) {
-          T a = T(0);
-#pragma unroll
-          for (int i = 0; i < N; ++i) a = fma(tab.S[i * N + p], u[k][i], a);
-          t[k][p] = a;
-        }
-    }
-    // z: nodes -> Gauss values (w) and Gauss derivatives (wz), to shared (r, y=s, p)
-#pragma unroll
-    for (int r = 0; r < N; ++r)
-#pragma unroll
+#pragma unroll UNR
       for (int p = 0; p < N; ++p) {
-        T a = T(0), b = T(0);
+        T t[N], tx[N];
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-          a = fma(tab.S[k * N + r], t[k][p], a);
-          b = fma(tab.SD[k * N + r], t[k][p], b);
+          T a = T(0), b = T(0);
+#pragma unroll
+          for (int i = 0; i < N; ++i) {
+            a = fma(tab.S[i * N + p], u[k][i], a);
+            b = fma(tab.SD[i * N + p], u[k][i], b);
+          }
+          t[k] = a;
+          tx[k] = b;
         }
-        bufA[(r * N + s) * N + p] = a;
-        bufB[(r * N + s) * N + p] = b;
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+          T w = T(0), wz = T(0), wx = T(0);
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            w = fma(tab.S[k * N + r], t[k], w);
+            wz = fma(tab.SD[k * N + r], t[k], wz);
+            wx = fma(tab.S[k * N + r], tx[k], wx);
+          }
+          const int o = (r * N + s) * N + p;
+          bufW[o] = w;
+          bufZ[o] = wz;
+          bufX[o] = wx;
+        }
       }
+    }
     __syncwarp(MASK);
+    if (SMEM_G && GEOM == 0) {
+      if (!mbar_wait_bounded(bar, parity, err, 1u << 24)) {
+        mbar_wait_bounded(bar, parity, err, 1u << 24); // let the copy in flight land
+        return;
+      }
+      parity ^= 1u;
+    }
 
-    // ---- Z-slab (z = s) ----
-    T fx[N][N], fy[N][N], fz[N][N]; // [q][p]
+    // ---- phase 2: Z-slab z = s, streamed over the x point p ----
     {
-      T W[N][N], WZ[N][N];
+      T a[N][N]; // [j][i]
 #pragma unroll
       for (int j = 0; j < N; ++j)
 #pragma unroll
-        for (int p = 0; p < N; ++p) {
-          W[j][p] = bufA[(s * N + j) * N + p];
-          WZ[j][p] = bufB[(s * N + j) * N + p];
-        }
-      T uq[N][N];
+        for (int i = 0; i < N; ++i) a[j][i] = T(0);
+#pragma unroll UNR
+      for (int p = 0; p < N; ++p) {
+        T Wc[N], Zc[N], Xc[N];
 #pragma unroll
-      for (int p = 0; p < N; ++p)
+        for (int j = 0; j < N; ++j) {
+          const int o = (s * N + j) * N + p;
+          Wc[j] = bufW[o];
+          Zc[j] = bufZ[o];
+          Xc[j] = bufX[o];
+        }
+        T fx[N], fy[N];
 #pragma unroll
         for (int q = 0; q < N; ++q) {
-          T a = T(0), b = T(0), c = T(0);
+          T dx = T(0), dy = T(0), dz = T(0);
 #pragma unroll
           for (int j = 0; j < N; ++j) {
-            a = fma(tab.S[j * N + q], W[j][p], a);
-            b = fma(tab.SD[j * N + q], W[j][p], b);
-            c = fma(tab.S[j * N + q], WZ[j][p], c);
+            dx = fma(tab.S[j * N + q], Xc[j], dx);
+            dy = fma(tab.SD[j * N + q], Wc[j], dy);
+            dz = fma(tab.S[j * N + q], Zc[j], dz);
           }
-          uq[q][p] = a;
-          fy[q][p] = b; // dy
-          fz[q][p] = c; // dz
+          T gc[6];
+          load_g6<N, T, GEOM, SMEM_G>(geo, gsm, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
+          fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
+          fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
+          bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
         }
 #pragma unroll
-      for (int q = 0; q < N; ++q)
+        for (int j = 0; j < N; ++j) {
+          T y1 = T(0), y2 = T(0);
 #pragma unroll
-        for (int p = 0; p < N; ++p) {
-          T a = T(0);
+          for (int q = 0; q < N; ++q) {
+            y1 = fma(tab.S[j * N + q], fx[q], y1);
+            y2 = fma(tab.SD[j * N + q], fy[q], y2);
+          }
 #pragma unroll
-          for (int m = 0; m < N; ++m) a = fma(tab.D[m * N + p], uq[q][m], a);
-          fx[q][p] = a; // dx
+          for (int i = 0; i < N; ++i) {
+            a[j][i] = fma(tab.SD[i * N + p], y1, a[j][i]);
+            a[j][i] = fma(tab.S[i * N + p], y2, a[j][i]);
+          }
         }
+      }
+      // a -> own slab region of bufW (all of this lane's reads of it are done)
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+#pragma unroll
+        for (int i = 0; i < N; ++i) bufW[(s * N + j) * N + i] = a[j][i];
     }
-    // geometry: f = G grad u at the N^2 points of this slab
-    if (GEOM == 0) {
-      const T *gg = geo + g * (N2 * 6 * LANES) + lane;
+    {
+      // c = Sy^T Sx^T fz from this lane's fz region, into its own region of bufZ
+      T c[N][N];
 #pragma unroll
-      for (int q = 0; q < N; ++q)
+      for (int j = 0; j < N; ++j)
 #pragma unroll
-        for (int p = 0; p < N; ++p) {
-          const T *gp = gg + (q * N + p) * 6 * LANES;
-          const T g0 = __ldg(gp), g1 = __ldg(gp + LANES), g2 = __ldg(gp + 2 * LANES),
-                  g3 = __ldg(gp + 3 * LANES), g4 = __ldg(gp + 4 * LANES),
-                  g5 = __ldg(gp + 5 * LANES);
-          const T dx = fx[q][p], dy = fy[q][p], dz = fz[q][p];
-          fx[q][p] = g0 * dx + g1 * dy + g2 * dz;
-          fy[q][p] = g1 * dx + g3 * dy + g4 * dz;
-          fz[q][p] = g2 * dx + g4 * dy + g5 * dz;
+        for (int i = 0; i < N; ++i) c[j][i] = T(0);
+#pragma unroll UNR
+      for (int q = 0; q < N; ++q) {
+        T fz[N];
+#pragma unroll
+        for (int p = 0; p < N; ++p) fz[p] = bufX[(s * N + q) * N + p];
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          T x3 = T(0);
+#pragma unroll
+          for (int p = 0; p < N; ++p) x3 = fma(tab.S[i * N + p], fz[p], x3);
+#pragma unroll
+          for (int j = 0; j < N; ++j) c[j][i] = fma(tab.S[j * N + q], x3, c[j][i]);
         }
-    } else {
-      const T *cg = geo + (g * CPW + e) * 8;
-      const T c0 = __ldg(cg), c1 = __ldg(cg + 1), c2 = __ldg(cg + 2), c3 = __ldg(cg + 3),
-              c4 = __ldg(cg + 4), c5 = __ldg(cg + 5);
-      T wr = tab.W[0]; // Gauss weight of this slab's z coordinate
-#pragma unroll
-      for (int r = 1; r < N; ++r)
-        if (s == r) wr = tab.W[r];
-#pragma unroll
-      for (int q = 0; q < N; ++q)
-#pragma unroll
-        for (int p = 0; p < N; ++p) {
-          T w = wr * tab.W[q] * tab.W[p];
-          if (GEOM == 2) w *= __ldg(coef + g * (N2 * LANES) + (q * N + p) * LANES + lane);
-          const T dx = fx[q][p], dy = fy[q][p], dz = fz[q][p];
-          fx[q][p] = w * (c0 * dx + c1 * dy + c2 * dz);
-          fy[q][p] = w * (c1 * dx + c3 * dy + c4 * dz);
-          fz[q][p] = w * (c2 * dx + c4 * dy + c5 * dz);
-        }
-    }
-    // integrate: X1 = SDx^T fx, X2 = Sx^T fy, X3 = Sx^T fz  (in place, row by row)
-#pragma unroll
-    for (int q = 0; q < N; ++q) {
-      T x1[N], x2[N], x3[N];
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        T a = T(0), b = T(0), c = T(0);
-#pragma unroll
-        for (int p = 0; p < N; ++p) {
-          a = fma(tab.SD[i * N + p], fx[q][p], a);
-          b = fma(tab.S[i * N + p], fy[q][p], b);
-          c = fma(tab.S[i * N + p], fz[q][p], c);
-        }
-        x1[i] = a;
-        x2[i] = b;
-        x3[i] = c;
       }
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
-        fx[q][i] = x1[i];
-        fy[q][i] = x2[i];
-        fz[q][i] = x3[i];
-      }
+      for (int j = 0; j < N; ++j)
+#pragma unroll
+        for (int i = 0; i < N; ++i) bufZ[(s * N + j) * N + i] = c[j][i];
     }
-    __syncwarp(MASK); // every lane has read the first exchange
-    // a = Sy^T X1 + SDy^T X2, c = Sy^T X3, to shared (z=s, j, i)
-#pragma unroll
-    for (int j = 0; j < N; ++j)
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        T a = T(0), c = T(0);
-#pragma unroll
-        for (int q = 0; q < N; ++q) {
-          a = fma(tab.S[j * N + q], fx[q][i], a);
-          a = fma(tab.SD[j * N + q], fy[q][i], a);
-          c = fma(tab.S[j * N + q], fz[q][i], c);
-        }
-        bufA[(s * N + j) * N + i] = a;
-        bufB[(s * N + j) * N + i] = c;
-      }
     __syncwarp(MASK);
 
-    // ---- Y-slab (y = s): out = Sz^T a + SDz^T c, scatter ----
-    {
-      T A[N][N], Cc[N][N];
+    // ---- phase 3: Y-slab y = s, out = Sz^T a + SDz^T c, scatter ----
+#pragma unroll UNR
+    for (int i = 0; i < N; ++i) {
+      T A[N], Cc[N];
 #pragma unroll
-      for (int r = 0; r < N; ++r)
+      for (int r = 0; r < N; ++r) {
+        A[r] = bufW[(r * N + s) * N + i];
+        Cc[r] = bufZ[(r * N + s) * N + i];
+      }
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
-          A[r][i] = bufA[(r * N + s) * N + i];
-          Cc[r][i] = bufB[(r * N + s) * N + i];
+      for (int k = 0; k < N; ++k) {
+        T v = T(0);
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+          v = fma(tab.S[k * N + r], A[r], v);
+          v = fma(tab.SD[k * N + r], Cc[r], v);
         }
-#pragma unroll
-      for (int k = 0; k < N; ++k)
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-          T a = T(0);
-#pragma unroll
-          for (int r = 0; r < N; ++r) {
-            a = fma(tab.S[k * N + r], A[r][i], a);
-            a = fma(tab.SD[k * N + r], Cc[r][i], a);
-          }
-          const uint32_t id = __ldg(ig + (k * N + i) * LANES);
-          if (id != kInvalidIdx) atomic_add(dst + id, a);
-        }
+        const uint32_t id = ld_stream(ig + (k * N + i) * LANES, pol_first);
+        if (id != kInvalidIdx) red_keep(dst + id, v, pol_last);
+      }
     }
-    __syncwarp(MASK); // shared buffers are reused by the next group
+    __syncwarp(MASK); // buffers are rewritten by the next group
   }
 }
 
@@ -396,7 +537,8 @@ struct SlabLaunch {
   int64_t n_groups;
   int geom; // 0 full, 1 affine, 2 affine + coefficient
   int dtype;
-  int grid;
+  int64_t resident_warps; // warps of this kernel resident on the whole device
+  unsigned int *err; // device flag set when a bounded wait gives up
   cudaStream_t stream;
   const double *S, *SD, *D, *W; // host tables (double), converted to the kernel type
 };
@@ -412,6 +554,7 @@ void launch_diag_p3(const SlabLaunch &);
 void launch_diag_p4(const SlabLaunch &);
 void launch_diag_p5(const SlabLaunch &);
 void launch_diag_p6(const SlabLaunch &);
+// resident warps per SM of the vmult / diagonal kernels
 int occupancy_vmult_p1(int dtype, int geom);
 int occupancy_vmult_p2(int dtype, int geom);
 int occupancy_vmult_p3(int dtype, int geom);

@@ -2,6 +2,11 @@
 // with PMG_DEGREE defined, so each degree compiles as its own translation unit.
 #pragma once
 
+#include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "laplace_kernels.cuh"
 #include "pmg_internal.hpp"
 
@@ -40,37 +45,52 @@ template <typename T> kern::Tab2<kN, T> make_tab2(const SlabLaunch &L) {
   return t;
 }
 
-template <typename T> constexpr size_t vmult_smem() {
-  return size_t(kWarpsPerBlock) * 2 * kern::Layout<kN>::CPW * kern::Layout<kN>::N3 * sizeof(T);
+template <typename T, bool SMEM_G> constexpr size_t vmult_smem() {
+  return size_t(SMEM_G ? 1 : kWarpsPerBlock) * kern::SlabSmem<kN, T, SMEM_G>::PER_WARP;
 }
 template <typename T> constexpr size_t diag_smem() {
   return size_t(kWarpsPerBlock) * 3 * kern::Layout<kN>::CPW * kern::Layout<kN>::N3 * sizeof(T);
 }
 
-// cudaFuncSetAttribute for the dynamic shared memory once per device and kernel
+// cudaFuncSetAttribute for the dynamic shared memory, once per device and kernel
 template <typename K> void allow_smem(K kernel, size_t bytes) {
-  static bool done[64] = {false};
+  static std::mutex mu;
+  static std::set<std::pair<int, const void *>> done;
   int dev = 0;
   PMG_CUDA(cudaGetDevice(&dev));
-  if (dev < 64 && !done[dev]) {
-    PMG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    done[dev] = true;
-  }
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(dev, reinterpret_cast<const void *>(kernel));
+  if (done.count(key)) return;
+  PMG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done.insert(key);
+}
+
+// Full geometry is staged through shared memory (one bulk copy per group) where that
+// measured faster on B200 (128^3 / 64^3 deformed-cube sweeps): every FP64 degree up to 5 and
+// FP32 except degree 4, whose 18 KB per-warp stage costs more occupancy than it saves.
+template <int GEOM, typename T> constexpr bool smem_g() {
+  return GEOM == 0 && (sizeof(T) == 8 ? kN <= 5 : kN != 5);
 }
 
 template <typename T, int GEOM> void vmult_geom(const SlabLaunch &L) {
-  auto k = kern::vmult_slab_kernel<kN, T, GEOM>;
-  allow_smem(k, vmult_smem<T>());
-  k<<<L.grid, 32 * kWarpsPerBlock, vmult_smem<T>(), L.stream>>>(
+  constexpr bool SG = smem_g<GEOM, T>();
+  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG>;
+  allow_smem(k, vmult_smem<T, SG>());
+  const int wpb = SG ? 1 : kWarpsPerBlock;
+  const int64_t want = (L.n_groups + wpb - 1) / wpb;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, L.resident_warps / wpb));
+  k<<<grid, 32 * wpb, vmult_smem<T, SG>(), L.stream>>>(
       make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
-      static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups);
+      static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err);
   PMG_LAUNCH_CHECK();
 }
 
 template <typename T, int GEOM> void diag_geom(const SlabLaunch &L) {
   auto k = kern::diag_slab_kernel<kN, T, GEOM>;
   allow_smem(k, diag_smem<T>());
-  k<<<L.grid, 32 * kWarpsPerBlock, diag_smem<T>(), L.stream>>>(
+  const int64_t want = (L.n_groups + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, L.resident_warps / kWarpsPerBlock));
+  k<<<grid, 32 * kWarpsPerBlock, diag_smem<T>(), L.stream>>>(
       make_tab2<T>(L), static_cast<T *>(L.dst), L.idx, static_cast<const T *>(L.geo),
       static_cast<const T *>(L.coef), L.n_groups);
   PMG_LAUNCH_CHECK();
@@ -89,18 +109,20 @@ template <typename T> void diag_type(const SlabLaunch &L) {
 }
 
 template <typename T, int GEOM> int occ_vmult() {
-  auto k = kern::vmult_slab_kernel<kN, T, GEOM>;
-  allow_smem(k, vmult_smem<T>());
+  constexpr bool SG = smem_g<GEOM, T>();
+  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG>;
+  allow_smem(k, vmult_smem<T, SG>());
   int nb = 0;
-  PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kWarpsPerBlock, vmult_smem<T>()));
-  return nb;
+  PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, SG ? 32 : 32 * kWarpsPerBlock,
+                                                         vmult_smem<T, SG>()));
+  return nb * (SG ? 1 : kWarpsPerBlock); // resident warps per SM
 }
 template <typename T, int GEOM> int occ_diag() {
   auto k = kern::diag_slab_kernel<kN, T, GEOM>;
   allow_smem(k, diag_smem<T>());
   int nb = 0;
   PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kWarpsPerBlock, diag_smem<T>()));
-  return nb;
+  return nb * kWarpsPerBlock; // resident warps per SM
 }
 
 } // namespace

@@ -365,13 +365,12 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
     }
   }
   PMG_CUDA(cudaDeviceSynchronize());
-  // persistent grids sized from the occupancy of this SM count
+  // persistent grids: as many warps as can be resident on this device
   const int gc = geom_code(op);
-  const int ov = std::max(1, occupancy(false, op.degree, op.dtype, gc));
-  const int od = std::max(1, occupancy(true, op.degree, op.dtype, gc));
-  const int64_t blocks_needed = (op.n_groups + 3) / 4;
-  op.grid_vmult = (int)std::max<int64_t>(1, std::min<int64_t>(blocks_needed, (int64_t)ov * sms));
-  op.grid_diag = (int)std::max<int64_t>(1, std::min<int64_t>(blocks_needed, (int64_t)od * sms));
+  op.warps_vmult = (int64_t)std::max(1, occupancy(false, op.degree, op.dtype, gc)) * sms;
+  op.warps_diag = (int64_t)std::max(1, occupancy(true, op.degree, op.dtype, gc)) * sms;
+  op.err_flag.allocate(sizeof(unsigned int));
+  PMG_CUDA(cudaMemset(op.err_flag.get(), 0, sizeof(unsigned int)));
   // the index lattice is only needed for building h-transfers: keep it
 }
 
@@ -384,7 +383,8 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
     SlabLaunch L = slab_launch(op, cached_tables(op.degree), s);
     L.src = src;
     L.dst = dst;
-    L.grid = op.grid_vmult;
+    L.resident_warps = op.warps_vmult;
+    L.err = op.err_flag.as<unsigned int>();
     prof::Scope scope("vmult_cell", s);
     vmult_fn(op.degree)(L);
   }
@@ -409,7 +409,8 @@ void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s) {
   if (op.n_cells > 0) {
     SlabLaunch L = slab_launch(op, cached_tables(op.degree), s);
     L.dst = op.inv_diag.get();
-    L.grid = op.grid_diag;
+    L.resident_warps = op.warps_diag;
+    L.err = op.err_flag.as<unsigned int>();
     prof::Scope scope("diag_cell", s);
     diag_fn(op.degree)(L);
   }

@@ -187,7 +187,8 @@ struct pmg_operator {
   int64_t n_constrained = 0;
   pmg::DeviceBuffer inv_diag;       // [N] dtype
   bool has_diag = false;
-  int grid_vmult = 0, grid_diag = 0;
+  int64_t warps_vmult = 0, warps_diag = 0; // resident warps of the cell kernels
+  pmg::DeviceBuffer err_flag;               // set by bounded device waits that give up
 };
 
 namespace pmg {
