@@ -231,6 +231,20 @@ pmg_status pmg_cg_solve(pmg_operator *A, pmg_mg *precond, void *x, const void *b
                         pmg_cg_info *info, void *stream);
 
 /* ---------------------------------------------------------------------------------- */
+/* Vector kernels on the path: LinearAlgebra::distributed::Vector operator* (the CG dot  */
+/* products) and copy_locally_owned_data_from across precisions                        */
+/* (tests/common/portable_multigrid_solver.h:185, :191)                                */
+/* ---------------------------------------------------------------------------------- */
+
+/* *result = sum_i a_i b_i over n entries of dtype, accumulated in FP64 with a fixed
+ * reduction order (deterministic); synchronises the stream to return the value. */
+pmg_status pmg_vector_dot(const void *a, const void *b, int32_t dtype, int64_t n, double *result,
+                          void *stream);
+/* dst (dt_dst) = src (dt_src), n entries, converting between FP64 and FP32. */
+pmg_status pmg_vector_copy(void *dst, int32_t dt_dst, const void *src, int32_t dt_src, int64_t n,
+                           void *stream);
+
+/* ---------------------------------------------------------------------------------- */
 /* Kernel timing (no reference counterpart; the reference times with deal.II Timer)   */
 /* ---------------------------------------------------------------------------------- */
 

@@ -8,6 +8,7 @@
 #include "pmg_internal.hpp"
 #include "solver.hpp"
 #include "transfer.hpp"
+#include "vector_ops.hpp"
 
 namespace {
 
@@ -409,6 +410,31 @@ pmg_status pmg_cg_solve(pmg_operator *A, pmg_mg *precond, void *x, const void *b
     return PMG_ENOCONV;
   }
   return st;
+}
+
+// ---------------------------------------------------------------------------------------
+pmg_status pmg_vector_dot(const void *a, const void *b, int32_t dtype, int64_t n, double *result,
+                          void *stream) {
+  return guarded(__func__, [&] {
+    NEED(a);
+    NEED(b);
+    NEED(result);
+    PMG_REQUIRE(dtype == PMG_F64 || dtype == PMG_F32, "bad dtype");
+    PMG_REQUIRE(n >= 0, "n must be >= 0");
+    *result = n == 0 ? 0.0 : pmg::vec::dot(a, b, dtype, n, as_stream(stream));
+  });
+}
+
+pmg_status pmg_vector_copy(void *dst, int32_t dt_dst, const void *src, int32_t dt_src, int64_t n,
+                           void *stream) {
+  return guarded(__func__, [&] {
+    NEED(dst);
+    NEED(src);
+    PMG_REQUIRE((dt_dst == PMG_F64 || dt_dst == PMG_F32) && (dt_src == PMG_F64 || dt_src == PMG_F32),
+                "bad dtype");
+    PMG_REQUIRE(n >= 0, "n must be >= 0");
+    if (n > 0) pmg::vec::convert(dst, dt_dst, src, dt_src, n, as_stream(stream));
+  });
 }
 
 // ---------------------------------------------------------------------------------------

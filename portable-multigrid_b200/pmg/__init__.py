@@ -165,6 +165,8 @@ def _declare(L):
         "pmg_mg_destroy": ([vp], i32),
         "pmg_mg_vmult": ([vp, vp, vp, i32, vp], i32),
         "pmg_cg_solve": ([vp, vp, vp, vp, d, d, i32, P(CGInfo), vp], i32),
+        "pmg_vector_dot": ([vp, vp, i32, i64, P(d), vp], i32),
+        "pmg_vector_copy": ([vp, i32, vp, i32, i64, vp], i32),
         "pmg_profile_enable": ([i32], i32),
         "pmg_profile_reset": ([], i32),
         "pmg_profile_query": ([C.c_char_p, P(d), P(i64)], i32),
@@ -193,6 +195,23 @@ def _stream():
 
 def _ptr(t):
     return C.c_void_p(t.data_ptr())
+
+
+def _dt(t):
+    import torch
+    return F64 if t.dtype == torch.float64 else F32
+
+
+def vector_dot(a, b):
+    """sum(a*b) of two device vectors of the same dtype, accumulated in FP64."""
+    r = C.c_double()
+    check(lib().pmg_vector_dot(_ptr(a), _ptr(b), _dt(a), a.numel(), C.byref(r), _stream()))
+    return r.value
+
+
+def vector_copy(dst, src):
+    """dst = src with precision conversion (copy_locally_owned_data_from)."""
+    check(lib().pmg_vector_copy(_ptr(dst), _dt(dst), _ptr(src), _dt(src), src.numel(), _stream()))
 
 
 def profile_enable(on=True):
