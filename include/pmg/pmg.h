@@ -240,6 +240,17 @@ pmg_status pmg_cg_solve(pmg_operator *A, pmg_mg *precond, void *x, const void *b
  * reduction order (deterministic); synchronises the stream to return the value. */
 pmg_status pmg_vector_dot(const void *a, const void *b, int32_t dtype, int64_t n, double *result,
                           void *stream);
+/* The dot product of pmg_vector_dot for callers that cannot allocate device memory at the
+ * point of the call (their allocator owns the device budget, or they cannot afford the
+ * synchronisation cudaMalloc/cudaFree may imply).  No counterpart in the reference.
+ * Allocates nothing: its scratch is a fixed 32 KB array in the library's device image,
+ * held on every GPU that loads the library until exit.  *result_dev (a caller-owned device
+ * double) receives the FP64-accumulated sum, ordered on stream, without a host
+ * synchronisation.  n is limited to 268,435,456 entries (PMG_EINVAL beyond).  The first
+ * call on a device looks up the scratch address and should come before any stream capture.
+ * Calls that overlap on the GPU share the scratch and race. */
+pmg_status pmg_vector_dot_noalloc(const void *a, const void *b, int32_t dtype, int64_t n,
+                                  double *result_dev, void *stream);
 /* dst (dt_dst) = src (dt_src), n entries, converting between FP64 and FP32. */
 pmg_status pmg_vector_copy(void *dst, int32_t dt_dst, const void *src, int32_t dt_src, int64_t n,
                            void *stream);

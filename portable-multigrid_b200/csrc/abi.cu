@@ -39,6 +39,11 @@ inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
 
 } // namespace
 
+namespace pmg {
+void vector_dot_noalloc(const void *a, const void *b, int dtype, int64_t n, double *result,
+                        cudaStream_t s); // noalloc.cu
+}
+
 extern "C" {
 
 size_t pmg_last_error(char *buf, size_t n) {
@@ -422,6 +427,13 @@ pmg_status pmg_vector_dot(const void *a, const void *b, int32_t dtype, int64_t n
     PMG_REQUIRE(dtype == PMG_F64 || dtype == PMG_F32, "bad dtype");
     PMG_REQUIRE(n >= 0, "n must be >= 0");
     *result = n == 0 ? 0.0 : pmg::vec::dot(a, b, dtype, n, as_stream(stream));
+  });
+}
+
+pmg_status pmg_vector_dot_noalloc(const void *a, const void *b, int32_t dtype, int64_t n,
+                                  double *result_dev, void *stream) {
+  return guarded(__func__, [&] {
+    pmg::vector_dot_noalloc(a, b, dtype, n, result_dev, as_stream(stream));
   });
 }
 
