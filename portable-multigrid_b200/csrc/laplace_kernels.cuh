@@ -19,8 +19,10 @@
 //        Y-slab:  out = Sz^T a + SDz^T c
 //    No block-wide barrier is used; warps are independent.
 //  * The index map and G are stored lane-contiguous per group ([group][point][lane]), so
-//    every load of them is a fully coalesced warp access, and each warp bulk-prefetches the
-//    next group's G into L2 (cp.async.bulk.prefetch.L2) while it computes the current one.
+//    every load of them is a fully coalesced warp access; G is column-major per group (one
+//    contiguous chunk per x point), each warp bulk-prefetches the next group's G into L2
+//    (cp.async.bulk.prefetch.L2) and streams the columns of the current group through a
+//    two-slot shared-memory ring filled by TMA bulk copies one column ahead.
 //  * Scatter with native FP64/FP32 atomic adds (red.global.add) into L2.
 //  * The 1D tables are kernel parameters (constant bank), indexed at compile time.
 #pragma once
@@ -150,7 +152,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return false;
 }
 
-// GEOM 0: full G per quadrature point, geo = [group][N^2 (q,p)][6][LANES]
+// GEOM 0: full G per quadrature point, geo = [group][N (x point p)][N (y point q)][6][LANES]
 // GEOM 1: affine, geo = [cell][8] (6 used) multiplied by the tensor Gauss weight
 // GEOM 2: affine as 1, times coef = [group][N^2][LANES] per quadrature point
 //
@@ -178,11 +180,11 @@ __device__ __forceinline__ void load_g6(const T *__restrict__ geo, const T *gs,
   using Lo = Layout<N>;
   constexpr int LANES = Lo::LANES, N2 = Lo::N2, CPW = Lo::CPW;
   if (GEOM == 0 && SMEM_G) {
-    const T *gp = gs + (q * N + p) * 6 * LANES + lane;
+    const T *gp = gs + q * 6 * LANES + lane; // the staged x column p
 #pragma unroll
     for (int m = 0; m < 6; ++m) c[m] = gp[m * LANES];
   } else if (GEOM == 0) {
-    const T *gp = geo + g * (N2 * 6 * LANES) + (q * N + p) * 6 * LANES + lane;
+    const T *gp = geo + g * (N2 * 6 * LANES) + (p * N + q) * 6 * LANES + lane;
 #pragma unroll
     for (int m = 0; m < 6; ++m) c[m] = ld_stream(gp + m * LANES, pol);
   } else {
@@ -209,15 +211,17 @@ template <int N, typename T> struct Unroll {
 // group's geometry block and an mbarrier.
 template <int N, typename T, bool SMEM_G> struct SlabSmem {
   static constexpr size_t XCHG = size_t(3) * Layout<N>::CPW * Stride<N>::CELL * sizeof(T);
-  static constexpr size_t GEO = SMEM_G ? size_t(Layout<N>::N2) * 6 * Layout<N>::LANES * sizeof(T) : 0;
+  static constexpr size_t CHUNK = size_t(N) * 6 * Layout<N>::LANES * sizeof(T); // one x column
+  static constexpr size_t GEO = SMEM_G ? 2 * CHUNK : 0;                         // two-slot ring
   static constexpr size_t PER_WARP = ((GEO + XCHG + 15) / 16) * 16 + (SMEM_G ? 16 : 0);
 };
 
-// SMEM_G: the geometry block of each group (contiguous in the slab layout) is brought into
-// shared memory by one bulk copy issued when the group starts, so that the gather and the
-// first phase overlap with it; launched with one warp per block.
+// SMEM_G: the x columns of each group's geometry (contiguous chunks) stream through a
+// two-slot shared-memory ring; the copy of the next column (or of the next group's first
+// column) is issued when a column starts, so it overlaps with that column's work.
+// Launched with one warp per block.
 template <int N, typename T, int GEOM, bool SMEM_G>
-__global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 4 : MinBlocks<N, T>::value))
+__global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, T>::value))
     vmult_slab_kernel(const __grid_constant__ Tab<N, T> tab, const T *__restrict__ src, T *__restrict__ dst,
                       const uint32_t *__restrict__ idx, const T *__restrict__ geo,
                       const T *__restrict__ coef, int64_t n_groups, unsigned int *err) {
@@ -233,30 +237,33 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 4 : MinBlocks<N, 
   const int e = lane / N;
   const int s = lane - e * N;
   unsigned char *wsm = smem_raw + (threadIdx.x >> 5) * SM::PER_WARP;
-  T *gsm = reinterpret_cast<T *>(wsm);                      // geometry block (SMEM_G)
+  T *ring = reinterpret_cast<T *>(wsm);                     // geometry column ring (SMEM_G)
   T *bufW = reinterpret_cast<T *>(wsm + SM::GEO) + e * CS;  // exchange buffers
   T *bufZ = bufW + CPW * CS;
   T *bufX = bufZ + CPW * CS;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(wsm + SM::PER_WARP - 16);
-  if (SMEM_G) {
-    if (lane == 0) mbar_init(bar, 1);
-    __syncwarp(MASK);
-  }
-  uint32_t parity = 0;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(wsm + SM::PER_WARP - 16);
+  constexpr int CHUNK_ELEMS = N * 6 * LANES;
+  uint32_t chunk = 0; // columns consumed so far; slot = chunk & 1, parity = (chunk >> 1) & 1
   const int64_t warp0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   const uint64_t pol_first = policy_evict_first(), pol_last = policy_evict_last();
+  if (SMEM_G && GEOM == 0) {
+    if (lane == 0) {
+      mbar_init(&bars[0], 1);
+      mbar_init(&bars[1], 1);
+      if (warp0 < n_groups)
+        bulk_load(ring, geo + warp0 * (N2 * 6 * LANES), CHUNK_ELEMS * sizeof(T), &bars[0], pol_first);
+    }
+    __syncwarp(MASK);
+  }
   T wr = tab.W[0]; // Gauss weight of this lane's z point (affine geometry)
 #pragma unroll
   for (int r = 1; r < N; ++r)
     if (s == r) wr = tab.W[r];
 
   for (int64_t g = warp0; g < n_groups; g += nwarps) {
-    if (GEOM == 0 && lane == 0) {
-      if (SMEM_G) bulk_load(gsm, geo + g * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T), bar, pol_first);
-      if (g + nwarps < n_groups)
-        prefetch_l2(geo + (g + nwarps) * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T), pol_first);
-    }
+    if (GEOM == 0 && lane == 0 && g + nwarps < n_groups)
+      prefetch_l2(geo + (g + nwarps) * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T), pol_first);
     const uint32_t *ig = idx + g * (N2 * LANES) + lane;
 
     // ---- phase 1: gather the Y-slab y = s, u[k][i] = src at node (i, s, k) ----
@@ -300,13 +307,6 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 4 : MinBlocks<N, 
       }
     }
     __syncwarp(MASK);
-    if (SMEM_G && GEOM == 0) {
-      if (!mbar_wait_bounded(bar, parity, err, 1u << 24)) {
-        mbar_wait_bounded(bar, parity, err, 1u << 24); // let the copy in flight land
-        return;
-      }
-      parity ^= 1u;
-    }
 
     // ---- phase 2: Z-slab z = s, streamed over the x point p ----
     {
@@ -317,6 +317,24 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 4 : MinBlocks<N, 
         for (int i = 0; i < N; ++i) a[j][i] = T(0);
 #pragma unroll UNR
       for (int p = 0; p < N; ++p) {
+        const T *gcol = nullptr;
+        if (SMEM_G && GEOM == 0) {
+          // issue the next column (this group's p+1, or the next group's column 0) into the
+          // other slot, whose previous column every lane finished with at the last syncwarp
+          if (lane == 0) {
+            const T *next = nullptr;
+            if (p + 1 < N) next = geo + g * (N2 * 6 * LANES) + (p + 1) * CHUNK_ELEMS;
+            else if (g + nwarps < n_groups) next = geo + (g + nwarps) * (N2 * 6 * LANES);
+            if (next)
+              bulk_load(ring + ((chunk + 1) & 1) * CHUNK_ELEMS, next, CHUNK_ELEMS * sizeof(T),
+                        &bars[(chunk + 1) & 1], pol_first);
+          }
+          if (!mbar_wait_bounded(&bars[chunk & 1], (chunk >> 1) & 1, err, 1u << 24)) {
+            if (lane == 0) mbar_wait_bounded(&bars[(chunk + 1) & 1], ((chunk + 1) >> 1) & 1, err, 1u << 24);
+            return; // the error flag is set; let copies in flight land before leaving
+          }
+          gcol = ring + (chunk & 1) * CHUNK_ELEMS;
+        }
         T Wc[N], Zc[N], Xc[N];
 #pragma unroll
         for (int j = 0; j < N; ++j) {
@@ -336,7 +354,7 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 4 : MinBlocks<N, 
             dz = fma(tab.S[j * N + q], Zc[j], dz);
           }
           T gc[6];
-          load_g6<N, T, GEOM, SMEM_G>(geo, gsm, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
+          load_g6<N, T, GEOM, SMEM_G>(geo, gcol, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
           fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
           fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
           bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
@@ -354,6 +372,10 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 4 : MinBlocks<N, 
             a[j][i] = fma(tab.SD[i * N + p], y1, a[j][i]);
             a[j][i] = fma(tab.S[i * N + p], y2, a[j][i]);
           }
+        }
+        if (SMEM_G && GEOM == 0) {
+          __syncwarp(MASK); // this slot may be refilled from the next column on
+          ++chunk;
         }
       }
       // a -> own slab region of bufW (all of this lane's reads of it are done)
@@ -452,7 +474,7 @@ __global__ void __launch_bounds__(128) diag_slab_kernel(const Tab2<N, T> tab,
       for (int p = 0; p < N; ++p) {
         T c[6];
         if (GEOM == 0) {
-          const T *gp = geo + g * (N2 * 6 * LANES) + (q * N + p) * 6 * LANES + lane;
+          const T *gp = geo + g * (N2 * 6 * LANES) + (p * N + q) * 6 * LANES + lane;
 #pragma unroll
           for (int m = 0; m < 6; ++m) c[m] = __ldg(gp + m * LANES);
         } else {
@@ -537,7 +559,8 @@ struct SlabLaunch {
   int64_t n_groups;
   int geom; // 0 full, 1 affine, 2 affine + coefficient
   int dtype;
-  int64_t resident_warps; // warps of this kernel resident on the whole device
+  int64_t resident_warps;      // warps of the kernel resident on the whole device
+  int64_t resident_warps_ring; // the same for the geometry-ring variant of vmult
   unsigned int *err; // device flag set when a bounded wait gives up
   cudaStream_t stream;
   const double *S, *SD, *D, *W; // host tables (double), converted to the kernel type

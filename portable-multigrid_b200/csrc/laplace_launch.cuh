@@ -3,6 +3,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -65,24 +66,39 @@ template <typename K> void allow_smem(K kernel, size_t bytes) {
   done.insert(key);
 }
 
-// Full geometry is staged through shared memory (one bulk copy per group) where that
-// measured faster on B200 (128^3 / 64^3 deformed-cube sweeps): every FP64 degree up to 5 and
-// FP32 except degree 4, whose 18 KB per-warp stage costs more occupancy than it saves.
-template <int GEOM, typename T> constexpr bool smem_g() {
-  return GEOM == 0 && (sizeof(T) == 8 ? kN <= 5 : kN != 5);
+// Full geometry streams through the shared-memory column ring (TMA) except where direct
+// loads measured faster on B200 (deformed-cube sweeps at 64^3/128^3): FP32 degree 4, whose
+// register-heavy unrolled form already hides the latency at 8 warps/SM, and FP64 degree 6.
+// PMG_VMULT_STAGE=0 / 1 forces direct loads / the ring (a tuning switch; both are compiled).
+inline int stage_override() {
+  static const int v = [] {
+    const char *e = std::getenv("PMG_VMULT_STAGE");
+    return e ? std::atoi(e) : -1;
+  }();
+  return v;
+}
+template <typename T> bool use_ring() {
+  const int o = stage_override();
+  if (o == 0 || o == 1) return o == 1;
+  return !((sizeof(T) == 4 && kN == 5) || (sizeof(T) == 8 && kN == 7));
 }
 
-template <typename T, int GEOM> void vmult_geom(const SlabLaunch &L) {
-  constexpr bool SG = smem_g<GEOM, T>();
+template <typename T, int GEOM, bool SG> void vmult_launch(const SlabLaunch &L) {
   auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG>;
   allow_smem(k, vmult_smem<T, SG>());
   const int wpb = SG ? 1 : kWarpsPerBlock;
   const int64_t want = (L.n_groups + wpb - 1) / wpb;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, L.resident_warps / wpb));
+  const int64_t resident = SG ? L.resident_warps_ring : L.resident_warps;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, resident / wpb));
   k<<<grid, 32 * wpb, vmult_smem<T, SG>(), L.stream>>>(
       make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
       static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err);
   PMG_LAUNCH_CHECK();
+}
+
+template <typename T, int GEOM> void vmult_geom(const SlabLaunch &L) {
+  if (GEOM == 0 && use_ring<T>()) vmult_launch<T, GEOM, true>(L);
+  else vmult_launch<T, GEOM, false>(L);
 }
 
 template <typename T, int GEOM> void diag_geom(const SlabLaunch &L) {
@@ -108,14 +124,19 @@ template <typename T> void diag_type(const SlabLaunch &L) {
   else diag_geom<T, 2>(L);
 }
 
-template <typename T, int GEOM> int occ_vmult() {
-  constexpr bool SG = smem_g<GEOM, T>();
+template <typename T, int GEOM, bool SG> int occ_vmult_variant() {
   auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG>;
   allow_smem(k, vmult_smem<T, SG>());
   int nb = 0;
   PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, SG ? 32 : 32 * kWarpsPerBlock,
                                                          vmult_smem<T, SG>()));
   return nb * (SG ? 1 : kWarpsPerBlock); // resident warps per SM
+}
+// resident warps per SM of the direct variant (low 16 bits) and of the ring variant (high)
+template <typename T, int GEOM> int occ_vmult() {
+  const int direct = occ_vmult_variant<T, GEOM, false>();
+  const int ring = GEOM == 0 ? occ_vmult_variant<T, GEOM, true>() : direct;
+  return direct | (ring << 16);
 }
 template <typename T, int GEOM> int occ_diag() {
   auto k = kern::diag_slab_kernel<kN, T, GEOM>;

@@ -107,7 +107,9 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
       if (coef_values) kap *= coef_values[c * nq3 + q];
       const int64_t grp = c / g.cpw;
       const int e = (int)(c % g.cpw);
-      const int m = q1 * g.N + q0, lane = e * g.N + q2;
+      // full geometry is column-major per group (x point outer) so that each x column of a
+      // group is one contiguous chunk; the per-point coefficient stays row-major
+      const int m = q0 * g.N + q1, m_row = q1 * g.N + q0, lane = e * g.N + q2;
       if (mode == 0) {
         const double f = fabs(det) * wq * kap;
         int comp = 0;
@@ -119,7 +121,7 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
             ++comp;
           }
       } else if (mode == 1) {
-        out[(grp * (g.N * g.N) + m) * g.lanes + lane] = (T)kap;
+        out[(grp * (g.N * g.N) + m_row) * g.lanes + lane] = (T)kap;
       } else {
         double f = 1.0;
         if (f_kind == 1) f = 3.0 * M_PI * M_PI * sin(M_PI * xq[0]) * sin(M_PI * xq[1]) * sin(M_PI * xq[2]);
@@ -367,7 +369,9 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   PMG_CUDA(cudaDeviceSynchronize());
   // persistent grids: as many warps as can be resident on this device
   const int gc = geom_code(op);
-  op.warps_vmult = (int64_t)std::max(1, occupancy(false, op.degree, op.dtype, gc)) * sms;
+  const int occ = occupancy(false, op.degree, op.dtype, gc);
+  op.warps_vmult = (int64_t)std::max(1, occ & 0xffff) * sms;
+  op.warps_vmult_ring = (int64_t)std::max(1, occ >> 16) * sms;
   op.warps_diag = (int64_t)std::max(1, occupancy(true, op.degree, op.dtype, gc)) * sms;
   op.err_flag.allocate(sizeof(unsigned int));
   PMG_CUDA(cudaMemset(op.err_flag.get(), 0, sizeof(unsigned int)));
@@ -384,6 +388,7 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
     L.src = src;
     L.dst = dst;
     L.resident_warps = op.warps_vmult;
+    L.resident_warps_ring = op.warps_vmult_ring;
     L.err = op.err_flag.as<unsigned int>();
     prof::Scope scope("vmult_cell", s);
     vmult_fn(op.degree)(L);
@@ -468,7 +473,7 @@ void operator_copy_geometry(const pmg_operator &op, double *host) {
         for (int p = 0; p < N; ++p)
           for (int comp = 0; comp < 6; ++comp)
             host[(c * 6 + comp) * N3 + (r * N + q) * N + p] =
-                g[((grp * N2 + q * N + p) * 6 + comp) * op.lanes + e * N + r];
+                g[((grp * N2 + p * N + q) * 6 + comp) * op.lanes + e * N + r];
   }
 }
 

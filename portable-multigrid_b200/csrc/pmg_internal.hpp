@@ -188,6 +188,7 @@ struct pmg_operator {
   pmg::DeviceBuffer inv_diag;       // [N] dtype
   bool has_diag = false;
   int64_t warps_vmult = 0, warps_diag = 0; // resident warps of the cell kernels
+  int64_t warps_vmult_ring = 0;             // ... of the geometry-ring vmult variant
   pmg::DeviceBuffer err_flag;               // set by bounded device waits that give up
 };
 
