@@ -89,13 +89,22 @@ pmg_status pmg_mesh_n_cells(const pmg_mesh *mesh, int64_t *n_cells);
 #define PMG_COEFF_KAPPA 1  /* kappa = 1 + 0.9 sin(2 pi x) sin(2 pi y) sin(2 pi z)      */
 #define PMG_COEFF_VALUES 2 /* caller-supplied values per quadrature point [C][nq^3]     */
 
+#define PMG_OP_LAPLACE 0 /* continuous FE_Q Laplace (LaplaceOperatorBK3)                 */
+#define PMG_OP_DG_SIPG 1 /* discontinuous FE_DGQ symmetric interior penalty Laplace
+                            (LaplaceOperatorDG, include/operators/portable_laplace_operator_dg.h);
+                            axis-aligned undeformed boxes, no coefficient, Dirichlet data
+                            enter weakly through the boundary faces                       */
+
 typedef struct {
-  int32_t degree;          /* FE_Q degree 1..6 (OperatorDispatchFactory::max_degree)    */
+  int32_t degree;          /* FE_Q / FE_DGQ degree 1..6 (OperatorDispatchFactory::max_degree) */
   int32_t dtype;           /* pmg_dtype: arithmetic and vector type                     */
   int32_t geometry;        /* PMG_GEOMETRY_*                                            */
   int32_t coeff_kind;      /* PMG_COEFF_*                                               */
   const double *coeff_qp;  /* host array [C][(degree+1)^3] for PMG_COEFF_VALUES         */
   int32_t device;          /* CUDA device ordinal                                       */
+  int32_t kind;            /* PMG_OP_*                                                  */
+  double penalty;          /* DG: sigma = penalty/h; <= 0 selects the reference's p(p+1)
+                              (portable_laplace_operator_dg.h:147-151)                     */
 } pmg_operator_params;
 
 /* LaplaceOperatorBK3 constructor + setup_dof_indices_per_color + compute_G_tensors
@@ -132,7 +141,10 @@ pmg_status pmg_operator_el(const pmg_operator *op, int64_t row, int64_t col, dou
 pmg_status pmg_operator_bytes_per_vmult(const pmg_operator *op, int64_t *bytes);
 /* Right-hand side b_i = (phi_i, f) with an nq-point Gauss rule, zero on constrained DoFs
  * (tests/poisson_cube_bk3/program.cc:517-566): f_kind 0: f = 1;
- * f_kind 1: f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z).  b has the operator's dtype. */
+ * f_kind 1: f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z);
+ * f_kind 2: u = exp(x) sin(pi y) cos(pi z), f = (2 pi^2 - 1) u, and for DG operators the
+ * weakly imposed Dirichlet data (g, 2 sigma phi_i - d_n phi_i) on Dirichlet faces.
+ * b has the operator's dtype. */
 pmg_status pmg_operator_assemble_rhs(const pmg_operator *op, int32_t f_kind, int32_t nq,
                                      void *b, void *stream);
 /* Inspection, host copies in the reference layouts: the dof index map with the
@@ -152,8 +164,10 @@ pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host);
  * (PolynomialTransfer, include/multigrid/portable_polynomial_transfer.h:1044-1361) when
  * both operators live on the same mesh with degree_coarse < degree_fine, a geometric one
  * (GeometricTransfer, include/multigrid/portable_geometric_transfer.h:944-1486) when the
- * degrees agree and the fine mesh is the coarse box refined once more.  Both operators
- * must have the same dtype. */
+ * degrees agree and the fine mesh is the coarse box refined once more, and the DG <-> CG
+ * transfer (ContinuousTransfer, include/multigrid/portable_continuous_transfer.h:110-319)
+ * when the fine operator is DG and the coarse one continuous of the same degree on the same
+ * mesh.  Both operators must have the same dtype. */
 pmg_status pmg_transfer_create(const pmg_operator *coarse, const pmg_operator *fine,
                                pmg_transfer **transfer);
 pmg_status pmg_transfer_destroy(pmg_transfer *transfer);

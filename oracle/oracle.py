@@ -299,3 +299,74 @@ def chebyshev_apply(box, p, degree, smoothing_range, eig_its, mode, src, dst):
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+# ---------------------------------------------------------------------------------------
+# DG-SIPG
+# ---------------------------------------------------------------------------------------
+def _declare_dg(L):
+    d, i32 = np.float64, np.int32
+    BP = C.POINTER(Box)
+    L.orc_dg_vmult.argtypes = [BP, C.c_int, C.c_double, _p(d), _p(d)]
+    L.orc_dg_rhs.argtypes = [BP, C.c_int, C.c_int, C.c_double, _p(d)]
+    L.orc_dg_l2_error.argtypes = [BP, C.c_int, C.c_int, _p(d)]
+    L.orc_dg_l2_error.restype = C.c_double
+    L.orc_dg_cg_transfer.argtypes = [BP, C.c_int, C.c_int, _p(d), _p(d)]
+    L.orc_dg_diagonal.argtypes = [BP, C.c_int, C.c_double, _p(d)]
+    L.orc_dg_diagonal_probe.argtypes = [BP, C.c_int, C.c_double, _p(d)]
+    L.orc_solve_dg.argtypes = [BP, C.c_int, _p(i32), C.c_int, C.c_int, C.c_double, C.c_double,
+                               C.c_int, C.c_int, C.POINTER(SolveInfo), C.c_void_p]
+
+
+def _dg_lib():
+    L = lib()
+    if not getattr(L, "_dg_declared", False):
+        _declare_dg(L)
+        L._dg_declared = True
+    return L
+
+
+def dg_n(box, p):
+    return box.ncells() * (p + 1) ** 3
+
+
+def dg_vmult(box, p, c_pen, src):
+    dst = np.zeros(dg_n(box, p))
+    _dg_lib().orc_dg_vmult(C.byref(box), p, c_pen, np.ascontiguousarray(src, dtype=np.float64), dst)
+    return dst
+
+
+def dg_rhs(box, p, nq, c_pen):
+    b = np.zeros(dg_n(box, p))
+    _dg_lib().orc_dg_rhs(C.byref(box), p, nq, c_pen, b)
+    return b
+
+
+def dg_l2_error(box, p, nq, u):
+    return _dg_lib().orc_dg_l2_error(C.byref(box), p, nq, np.ascontiguousarray(u, dtype=np.float64))
+
+
+def dg_cg_transfer(box, p, direction, src, dst):
+    """direction 0: dst_dg += P src_cg; 1: dst_cg += P^T src_dg (in place)."""
+    _dg_lib().orc_dg_cg_transfer(C.byref(box), p, direction, np.ascontiguousarray(src, dtype=np.float64), dst)
+    return dst
+
+
+def dg_diagonal(box, p, c_pen, probe=False):
+    dgl = np.zeros(dg_n(box, p))
+    fn = _dg_lib().orc_dg_diagonal_probe if probe else _dg_lib().orc_dg_diagonal
+    fn(C.byref(box), p, c_pen, dgl)
+    return dgl
+
+
+def solve_dg(box, p, pseq, cheb=5, c_pen=None, reduce=1e-10, maxit=200, nq_rhs=None, want_x=False):
+    info = SolveInfo()
+    c_pen = p * (p + 1.0) if c_pen is None else c_pen
+    nq_rhs = p + 2 if nq_rhs is None else nq_rhs
+    x = np.zeros(dg_n(box, p)) if want_x else None
+    rc = _dg_lib().orc_solve_dg(C.byref(box), p, np.ascontiguousarray(pseq, dtype=np.int32), len(pseq),
+                                cheb, c_pen, reduce, maxit, nq_rhs, C.byref(info),
+                                x.ctypes.data_as(C.c_void_p) if want_x else None)
+    if rc != 0:
+        raise ValueError("orc_solve_dg failed")
+    return info, x

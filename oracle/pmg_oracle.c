@@ -913,6 +913,8 @@ void orc_transfer_restrict_add(const orc_transfer *t, double *dst_c, const doubl
 typedef struct {
   orc_box box;
   int p;
+  int dg;       /* 1: DG-SIPG level (orc_dg_vmult), numbering cell * (p+1)^3 + l */
+  double c_pen; /* DG penalty factor */
   int64_t C, N;
   uint32_t *plain, *idx, *lattice;
   uint8_t *constrained, *color;
@@ -965,9 +967,37 @@ static void level_free(orc_level *L)
   free(L->tmp);
 }
 
+void orc_dg_vmult(const orc_box *b, int p, double c_pen, const double *src, double *dst);
+void orc_dg_diagonal(const orc_box *b, int p, double c_pen, double *diag);
+
 static void level_vmult(const orc_level *L, double *dst, const double *src)
 {
-  orc_vmult(L->p, L->C, L->N, L->idx, L->G, L->constrained, L->color, src, dst);
+  if (L->dg) orc_dg_vmult(&L->box, L->p, L->c_pen, src, dst);
+  else orc_vmult(L->p, L->C, L->N, L->idx, L->G, L->constrained, L->color, src, dst);
+}
+
+static void level_init_dg(orc_level *L, const orc_box *b, int p, double c_pen)
+{
+  memset(L, 0, sizeof(*L));
+  L->box = *b;
+  L->p = p;
+  L->dg = 1;
+  L->c_pen = c_pen;
+  L->C = orc_box_ncells(b);
+  const int nm3 = (p + 1) * (p + 1) * (p + 1);
+  L->N = L->C * nm3;
+  L->plain = (uint32_t *)malloc(sizeof(uint32_t) * L->N);
+  L->idx = (uint32_t *)malloc(sizeof(uint32_t) * L->N);
+  for (int64_t i = 0; i < L->N; ++i) L->plain[i] = L->idx[i] = (uint32_t)i;
+  L->constrained = (uint8_t *)calloc(L->N, 1);
+  L->invdiag = (double *)malloc(sizeof(double) * L->N);
+  orc_dg_diagonal(b, p, c_pen, L->invdiag);
+  for (int64_t i = 0; i < L->N; ++i) L->invdiag[i] = 1.0 / L->invdiag[i];
+  L->sol = (double *)calloc(L->N, sizeof(double));
+  L->def = (double *)calloc(L->N, sizeof(double));
+  L->t = (double *)calloc(L->N, sizeof(double));
+  L->old = (double *)calloc(L->N, sizeof(double));
+  L->tmp = (double *)calloc(L->N, sizeof(double));
 }
 
 static double dot(int64_t n, const double *a, const double *b)
@@ -1373,4 +1403,479 @@ int orc_num_threads(void)
 #else
   return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* 7. DG-SIPG operator on axis-aligned boxes                                             */
+/* ------------------------------------------------------------------------------------ */
+
+/* Discontinuous FE_DGQ(p) (Lagrange on Gauss-Lobatto points) with the symmetric interior
+ * penalty form of source/plain_laplace_solver_dg/program.cc:106-217 (and the GPU operator
+ * include/operators/portable_laplace_operator_dg.h + include/kernels/laplace_dg_kokkos_kernels.h):
+ *   inner faces:    [[v]] (sigma [[u]] - {d_n u}) - {d_n v} [[u]]
+ *   Dirichlet faces (mirror u+ = -u-, d_n u+ = d_n u-, laplace_dg_kokkos_kernels.h:1560-1569):
+ *                   v (2 sigma u - d_n u) - u d_n v
+ *   sigma = c_pen * (1/h- + 1/h+)/2 on inner faces, c_pen / h on boundary faces, h the cell
+ *   extent normal to the face; the reference uses c_pen = p (p+1)
+ *   (portable_laplace_operator_dg.h:147-151).
+ * DoFs are numbered cell by cell, dof = cell * (p+1)^3 + lexicographic local index. Faces are
+ * integrated with the (p+1)-point Gauss rule in each tangential direction. */
+
+static void box_cell_h(const orc_box *b, double h[3])
+{
+  int64_t n[3];
+  box_ncells(b, n);
+  for (int d = 0; d < 3; ++d) h[d] = (b->hi[d] - b->lo[d]) / (double)n[d];
+}
+
+/* cell index of coordinates (or -1), inverse of orc_box_cell_coords */
+static int64_t *box_cell_lookup(const orc_box *b, int32_t *cx)
+{
+  int64_t n[3];
+  box_ncells(b, n);
+  const int64_t C = n[0] * n[1] * n[2];
+  int64_t *lut = (int64_t *)malloc(sizeof(int64_t) * C);
+  for (int64_t c = 0; c < C; ++c) lut[((int64_t)cx[2 * C + c] * n[1] + cx[C + c]) * n[0] + cx[c]] = c;
+  return lut;
+}
+
+/* evaluate value and derivative along d of cell data u at reference point xi */
+static void eval_point(int N, const double *xl_unused, const double *u, const ld *nodes,
+                       const double xi[3], int d, double *val, double *dd)
+{
+  double phi[3][16], dphi[3][16];
+  for (int a = 0; a < 3; ++a)
+    for (int i = 0; i < N; ++i) {
+      phi[a][i] = (double)lagrange(N, nodes, i, (ld)xi[a]);
+      dphi[a][i] = (double)lagrange_deriv(N, nodes, i, (ld)xi[a]);
+    }
+  double v = 0, g = 0;
+  for (int k = 0; k < N; ++k)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) {
+        const double x = u[(k * N + j) * N + i];
+        v += x * phi[0][i] * phi[1][j] * phi[2][k];
+        const double f0 = d == 0 ? dphi[0][i] : phi[0][i];
+        const double f1 = d == 1 ? dphi[1][j] : phi[1][j];
+        const double f2 = d == 2 ? dphi[2][k] : phi[2][k];
+        g += x * f0 * f1 * f2;
+      }
+  *val = v;
+  *dd = g;
+}
+
+/* add test contributions tv * phi_l(xi) + tn * d_d phi_l(xi) to out[l] */
+static void test_point(int N, const ld *nodes, const double xi[3], int d, double tv, double tn,
+                       double *out)
+{
+  double phi[3][16], dphi[3][16];
+  for (int a = 0; a < 3; ++a)
+    for (int i = 0; i < N; ++i) {
+      phi[a][i] = (double)lagrange(N, nodes, i, (ld)xi[a]);
+      dphi[a][i] = (double)lagrange_deriv(N, nodes, i, (ld)xi[a]);
+    }
+  for (int k = 0; k < N; ++k)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) {
+        const double f0 = d == 0 ? dphi[0][i] : phi[0][i];
+        const double f1 = d == 1 ? dphi[1][j] : phi[1][j];
+        const double f2 = d == 2 ? dphi[2][k] : phi[2][k];
+        out[(k * N + j) * N + i] += tv * phi[0][i] * phi[1][j] * phi[2][k] + tn * f0 * f1 * f2;
+      }
+}
+
+void orc_dg_vmult(const orc_box *b, int p, double c_pen, const double *src, double *dst)
+{
+  const int N = p + 1, N3 = N * N * N;
+  const int64_t C = orc_box_ncells(b);
+  double h[3];
+  box_cell_h(b, h);
+  ld nodes[16], wl[16], xg[16], wg[16];
+  gauss_lobatto_ld(N, nodes, wl);
+  gauss_ld(N, xg, wg);
+  double S[64], D[64], W[8];
+  orc_shape_tables(p, N, S, NULL, D, W);
+  int64_t n[3];
+  box_ncells(b, n);
+  int32_t *cx = (int32_t *)malloc(sizeof(int32_t) * 3 * C);
+  orc_box_cell_coords(b, cx, cx + C, cx + 2 * C);
+  int64_t *lut = box_cell_lookup(b, cx);
+  for (int64_t i = 0; i < C * N3; ++i) dst[i] = 0.0;
+  /* cell term: affine G = w_q vol / h_d^2 on the diagonal */
+  double *Gc = (double *)calloc(6 * N3, sizeof(double));
+  const double vol = h[0] * h[1] * h[2];
+  for (int q2 = 0; q2 < N; ++q2)
+    for (int q1 = 0; q1 < N; ++q1)
+      for (int q0 = 0; q0 < N; ++q0) {
+        const int q = (q2 * N + q1) * N + q0;
+        const double w = W[q0] * W[q1] * W[q2] * vol;
+        Gc[0 * N3 + q] = w / (h[0] * h[0]);
+        Gc[3 * N3 + q] = w / (h[1] * h[1]);
+        Gc[5 * N3 + q] = w / (h[2] * h[2]);
+      }
+  double *buf = (double *)malloc(sizeof(double) * 7 * N3);
+  for (int64_t c = 0; c < C; ++c) {
+    bk3_cell(N, S, D, Gc, src + c * N3, buf + N3, buf + 2 * N3, buf + 3 * N3, buf + 4 * N3,
+             buf + 5 * N3, buf + 6 * N3);
+    for (int l = 0; l < N3; ++l) dst[c * N3 + l] += buf[N3 + l];
+  }
+  /* faces: every cell handles its +d inner faces and its boundary faces */
+  for (int64_t c = 0; c < C; ++c) {
+    const int32_t cc[3] = {cx[c], cx[C + c], cx[2 * C + c]};
+    for (int d = 0; d < 3; ++d) {
+      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+      for (int s = 0; s < 2; ++s) {
+        int32_t nc[3] = {cc[0], cc[1], cc[2]};
+        nc[d] += s ? 1 : -1;
+        const int outside = nc[d] < 0 || nc[d] >= n[d];
+        if (!outside && s == 0) continue; /* inner faces handled from the minus side */
+        const double sign = s ? 1.0 : -1.0; /* outward normal of c: sign * e_d */
+        const int64_t nb = outside ? -1 : lut[((int64_t)nc[2] * n[1] + nc[1]) * n[0] + nc[0]];
+        const int dirichlet = (b->dirichlet_mask >> (2 * d + s)) & 1;
+        if (outside && !dirichlet) continue;
+        const double sigma = c_pen / h[d];
+        const double jxw_face = h[ta] * h[tb];
+        for (int qb = 0; qb < N; ++qb)
+          for (int qa = 0; qa < N; ++qa) {
+            double xi[3], xin[3];
+            xi[d] = s ? 1.0 : 0.0;
+            xi[ta] = (double)xg[qa];
+            xi[tb] = (double)xg[qb];
+            xin[0] = xi[0]; xin[1] = xi[1]; xin[2] = xi[2];
+            xin[d] = s ? 0.0 : 1.0;
+            const double wq = (double)(wg[qa] * wg[qb]) * jxw_face;
+            double um, dm;
+            eval_point(N, NULL, src + c * N3, nodes, xi, d, &um, &dm);
+            dm *= sign / h[d]; /* normal derivative along the outward normal of c */
+            double up, dp;
+            if (outside) {
+              up = -um;
+              dp = dm;
+            } else {
+              eval_point(N, NULL, src + nb * N3, nodes, xin, d, &up, &dp);
+              dp *= sign / h[d];
+            }
+            const double jump = um - up, avg = 0.5 * (dm + dp);
+            const double tv = (sigma * jump - avg) * wq, tn = -0.5 * jump * wq;
+            test_point(N, nodes, xi, d, tv, tn * sign / h[d], dst + c * N3);
+            if (!outside) test_point(N, nodes, xin, d, -tv, tn * sign / h[d], dst + nb * N3);
+          }
+      }
+    }
+  }
+  free(buf); free(Gc); free(cx); free(lut);
+}
+
+static double dg_exact(const double x[3])
+{
+  return exp(x[0]) * sin(ORC_PI * x[1]) * cos(ORC_PI * x[2]);
+}
+
+/* right-hand side for -lap u = f with u = exp(x) sin(pi y) cos(pi z), f = (2 pi^2 - 1) u, and
+ * the Dirichlet data imposed weakly through the mirror: b_l = (f, phi_l) + sum over Dirichlet
+ * faces of (g, 2 sigma phi_l - d_n phi_l); nq-point Gauss rules */
+void orc_dg_rhs(const orc_box *b, int p, int nq, double c_pen, double *rhs)
+{
+  const int N = p + 1, N3 = N * N * N;
+  const int64_t C = orc_box_ncells(b);
+  double h[3];
+  box_cell_h(b, h);
+  ld nodes[16], wl[16], xg[16], wg[16];
+  gauss_lobatto_ld(N, nodes, wl);
+  gauss_ld(nq, xg, wg);
+  int64_t n[3];
+  box_ncells(b, n);
+  int32_t *cx = (int32_t *)malloc(sizeof(int32_t) * 3 * C);
+  orc_box_cell_coords(b, cx, cx + C, cx + 2 * C);
+  for (int64_t i = 0; i < C * N3; ++i) rhs[i] = 0.0;
+  for (int64_t c = 0; c < C; ++c) {
+    const int32_t cc[3] = {cx[c], cx[C + c], cx[2 * C + c]};
+    for (int q2 = 0; q2 < nq; ++q2)
+      for (int q1 = 0; q1 < nq; ++q1)
+        for (int q0 = 0; q0 < nq; ++q0) {
+          const double xi[3] = {(double)xg[q0], (double)xg[q1], (double)xg[q2]};
+          double x[3];
+          for (int d = 0; d < 3; ++d) x[d] = b->lo[d] + (cc[d] + xi[d]) * h[d];
+          const double w = (double)(wg[q0] * wg[q1] * wg[q2]) * h[0] * h[1] * h[2];
+          const double f = (2.0 * ORC_PI * ORC_PI - 1.0) * dg_exact(x);
+          test_point(N, nodes, xi, 0, f * w, 0.0, rhs + c * N3);
+        }
+    for (int d = 0; d < 3; ++d) {
+      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+      for (int s = 0; s < 2; ++s) {
+        const int outside = s ? (cc[d] == n[d] - 1) : (cc[d] == 0);
+        if (!outside || !((b->dirichlet_mask >> (2 * d + s)) & 1)) continue;
+        const double sign = s ? 1.0 : -1.0, sigma = c_pen / h[d];
+        for (int qb = 0; qb < nq; ++qb)
+          for (int qa = 0; qa < nq; ++qa) {
+            double xi[3], x[3];
+            xi[d] = s ? 1.0 : 0.0;
+            xi[ta] = (double)xg[qa];
+            xi[tb] = (double)xg[qb];
+            for (int a = 0; a < 3; ++a) x[a] = b->lo[a] + (cc[a] + xi[a]) * h[a];
+            const double w = (double)(wg[qa] * wg[qb]) * h[ta] * h[tb];
+            const double g = dg_exact(x);
+            test_point(N, nodes, xi, d, 2.0 * sigma * g * w, -g * w * sign / h[d], rhs + c * N3);
+          }
+      }
+    }
+  }
+  free(cx);
+}
+
+double orc_dg_l2_error(const orc_box *b, int p, int nq, const double *u)
+{
+  const int N = p + 1, N3 = N * N * N;
+  const int64_t C = orc_box_ncells(b);
+  double h[3];
+  box_cell_h(b, h);
+  ld nodes[16], wl[16], xg[16], wg[16];
+  gauss_lobatto_ld(N, nodes, wl);
+  gauss_ld(nq, xg, wg);
+  int32_t *cx = (int32_t *)malloc(sizeof(int32_t) * 3 * C);
+  orc_box_cell_coords(b, cx, cx + C, cx + 2 * C);
+  double err = 0;
+  for (int64_t c = 0; c < C; ++c) {
+    const int32_t cc[3] = {cx[c], cx[C + c], cx[2 * C + c]};
+    for (int q2 = 0; q2 < nq; ++q2)
+      for (int q1 = 0; q1 < nq; ++q1)
+        for (int q0 = 0; q0 < nq; ++q0) {
+          const double xi[3] = {(double)xg[q0], (double)xg[q1], (double)xg[q2]};
+          double x[3], v, dummy;
+          for (int d = 0; d < 3; ++d) x[d] = b->lo[d] + (cc[d] + xi[d]) * h[d];
+          eval_point(N, NULL, u + c * N3, nodes, xi, 0, &v, &dummy);
+          const double w = (double)(wg[q0] * wg[q1] * wg[q2]) * h[0] * h[1] * h[2];
+          err += (v - dg_exact(x)) * (v - dg_exact(x)) * w;
+        }
+  }
+  free(cx);
+  return sqrt(err);
+}
+
+/* DG <-> CG transfer at equal degree on the same mesh (ContinuousTransfer,
+ * include/multigrid/portable_continuous_transfer.h:110-319): prolongate u_dg[i] += u_cg[map(i)]
+ * for CG DoFs that are not constrained; restrict u_cg[map(i)] += u_dg[i] likewise. */
+void orc_dg_cg_transfer(const orc_box *b, int p, int direction, const double *src, double *dst)
+{
+  const int N3 = (p + 1) * (p + 1) * (p + 1);
+  const int64_t C = orc_box_ncells(b);
+  int64_t n[3];
+  box_ncells(b, n);
+  const int64_t nlat = (p * n[0] + 1) * (p * n[1] + 1) * (p * n[2] + 1);
+  uint32_t *plain = (uint32_t *)malloc(sizeof(uint32_t) * C * N3);
+  uint8_t *cons = (uint8_t *)malloc(nlat);
+  orc_box_dofs(b, p, plain, cons, NULL);
+  for (int64_t c = 0; c < C; ++c)
+    for (int l = 0; l < N3; ++l) {
+      const uint32_t g = plain[c * N3 + l];
+      if (cons[g]) continue;
+      if (direction == 0) dst[c * N3 + l] += src[g];
+      else dst[g] += src[c * N3 + l];
+    }
+  free(plain);
+  free(cons);
+}
+
+/* DG diagonal, brute force: a(phi_l, phi_l) by applying the operator to unit vectors (tiny
+ * meshes only; checks the closed form below). */
+void orc_dg_diagonal_probe(const orc_box *b, int p, double c_pen, double *diag)
+{
+  const int64_t n = orc_box_ncells(b) * (p + 1) * (p + 1) * (p + 1);
+  double *e = (double *)calloc(n, sizeof(double));
+  double *y = (double *)malloc(sizeof(double) * n);
+  for (int64_t i = 0; i < n; ++i) {
+    e[i] = 1.0;
+    orc_dg_vmult(b, p, c_pen, e, y);
+    diag[i] = y[i];
+    e[i] = 0.0;
+  }
+  free(e);
+  free(y);
+}
+
+/* DG diagonal: the cell term by local probing, plus the face self terms in closed form.
+ * A node (i along d, tangential (a,b)) on the face layer of face (d, side s) with
+ * g = phi_i'(s) * (+-1)/h (normal derivative of its basis function) gets
+ *   m (sigma - g) on inner faces and m (2 sigma - 2 g) on Dirichlet faces,
+ * m = h_a h_b M1[a][a] M1[b][b] with M1 the exact 1D mass matrix on the GLL basis. */
+void orc_dg_diagonal(const orc_box *b, int p, double c_pen, double *diag)
+{
+  const int N = p + 1, N3 = N * N * N;
+  const int64_t C = orc_box_ncells(b);
+  double h[3];
+  box_cell_h(b, h);
+  double S[64], SD[64], D[64], W[8];
+  orc_shape_tables(p, N, S, SD, D, W);
+  ld nodes[16], wl[16];
+  gauss_lobatto_ld(N, nodes, wl);
+  double M1[64], dphi0[8], dphi1[8];
+  for (int i = 0; i < N; ++i) {
+    for (int j = 0; j < N; ++j) {
+      double s = 0;
+      for (int q = 0; q < N; ++q) s += S[i * N + q] * S[j * N + q] * W[q];
+      M1[i * N + j] = s;
+    }
+    dphi0[i] = (double)lagrange_deriv(N, nodes, i, 0.0L);
+    dphi1[i] = (double)lagrange_deriv(N, nodes, i, 1.0L);
+  }
+  int64_t n[3];
+  box_ncells(b, n);
+  int32_t *cx = (int32_t *)malloc(sizeof(int32_t) * 3 * C);
+  orc_box_cell_coords(b, cx, cx + C, cx + 2 * C);
+  double *Gc = (double *)calloc(6 * N3, sizeof(double));
+  const double vol = h[0] * h[1] * h[2];
+  for (int q = 0; q < N3; ++q) {
+    const int q0 = q % N, q1 = (q / N) % N, q2 = q / (N * N);
+    const double w = W[q0] * W[q1] * W[q2] * vol;
+    Gc[q] = w / (h[0] * h[0]);
+    Gc[3 * N3 + q] = w / (h[1] * h[1]);
+    Gc[5 * N3 + q] = w / (h[2] * h[2]);
+  }
+  double *buf = (double *)malloc(sizeof(double) * 7 * N3);
+  for (int64_t c = 0; c < C; ++c) {
+    for (int l = 0; l < N3; ++l) {
+      for (int m = 0; m < N3; ++m) buf[m] = (m == l) ? 1.0 : 0.0;
+      bk3_cell(N, S, D, Gc, buf, buf + N3, buf + 2 * N3, buf + 3 * N3, buf + 4 * N3, buf + 5 * N3,
+               buf + 6 * N3);
+      diag[c * N3 + l] = buf[N3 + l];
+    }
+    const int32_t cc[3] = {cx[c], cx[C + c], cx[2 * C + c]};
+    for (int d = 0; d < 3; ++d) {
+      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+      for (int s = 0; s < 2; ++s) {
+        const int outside = s ? (cc[d] == n[d] - 1) : (cc[d] == 0);
+        const int dirichlet = (b->dirichlet_mask >> (2 * d + s)) & 1;
+        if (outside && !dirichlet) continue;
+        const double sigma = c_pen / h[d];
+        const int il = s ? N - 1 : 0;
+        const double g = (s ? dphi1[il] : dphi0[il]) * (s ? 1.0 : -1.0) / h[d];
+        for (int bb = 0; bb < N; ++bb)
+          for (int aa = 0; aa < N; ++aa) {
+            int idx[3];
+            idx[d] = il;
+            idx[ta] = aa;
+            idx[tb] = bb;
+            const int l = (idx[2] * N + idx[1]) * N + idx[0];
+            const double m = h[ta] * h[tb] * M1[aa * N + aa] * M1[bb * N + bb];
+            diag[c * N3 + l] += outside ? m * (2.0 * sigma - 2.0 * g) : m * (sigma - g);
+          }
+      }
+    }
+  }
+  free(buf); free(Gc); free(cx);
+}
+
+/* DG <-> CG patch transfer for the multigrid: P = identity, unit weights */
+static void build_dg_transfer(orc_transfer *t, const orc_level *Lc, const orc_level *Lf)
+{
+  const int n = Lc->p + 1, n3 = n * n * n;
+  t->nc = n;
+  t->nf = n;
+  t->n_patches = Lc->C;
+  t->prolong_times = 1;
+  t->coarse_idx = (uint32_t *)malloc(sizeof(uint32_t) * Lc->C * n3);
+  t->fine_idx = (uint32_t *)malloc(sizeof(uint32_t) * Lc->C * n3);
+  memcpy(t->coarse_idx, Lc->idx, sizeof(uint32_t) * Lc->C * n3);
+  for (int64_t e = 0; e < Lc->C * n3; ++e) t->fine_idx[e] = (uint32_t)e;
+  t->P1d = (double *)calloc(n * n, sizeof(double));
+  for (int i = 0; i < n; ++i) t->P1d[i * n + i] = 1.0;
+  t->weights = (double *)malloc(sizeof(double) * Lc->C * n3);
+  for (int64_t e = 0; e < Lc->C * n3; ++e) t->weights[e] = 1.0;
+}
+
+/* The DG multigrid of the DG benchmark restated: FE_DGQ(p) on the box, ContinuousTransfer
+ * to FE_Q(p), then the continuous hierarchy of orc_solve_box (p-levels pseq, Q1 h-levels);
+ * PCG on the DG operator with rhs_kind 2 (exp(x) sin(pi y) cos(pi z), weak Dirichlet data). */
+int orc_solve_dg(const orc_box *box, int p, const int32_t *pseq, int n_pseq, int cheb,
+                 double c_pen, double reduce, int maxit, int nq_rhs, orc_solve_info *info,
+                 double *x_out)
+{
+  memset(info, 0, sizeof(*info));
+  const int n_h = box->refine + 1;
+  const int n_cg = n_h + n_pseq - 1;
+  const int n_levels = n_cg + 1;
+  if (n_levels > 32 || pseq[n_pseq - 1] != 1 || pseq[0] != p) return -1;
+  orc_mg mg;
+  mg.n_levels = n_levels;
+  mg.levels = (orc_level *)calloc(n_levels, sizeof(orc_level));
+  mg.transfers = (orc_transfer *)calloc(n_levels, sizeof(orc_transfer));
+  for (int l = 0; l < n_levels; ++l) {
+    orc_level *L = &mg.levels[l];
+    if (l < n_cg) {
+      orc_box b = *box;
+      int pl = 1;
+      if (l < n_h) b.refine = l;
+      else pl = pseq[n_pseq - 1 - (l - n_h + 1)];
+      level_init(L, &b, pl, 0);
+    } else {
+      level_init_dg(L, box, p, c_pen);
+    }
+    if (l > 0) {
+      L->cheb_degree = cheb;
+      L->smoothing_range = 15.0;
+      L->eig_iterations = 10;
+    } else {
+      L->cheb_degree = 0;
+      L->smoothing_range = 1e-3;
+      L->eig_iterations = (int)L->N;
+    }
+    cheb_estimate(L);
+    info->level_degree[l] = L->p;
+    info->level_cheb_degree[l] = L->cheb_degree;
+    info->level_max_ev[l] = L->max_ev;
+    info->level_min_ev[l] = L->min_ev;
+    info->level_dofs[l] = L->N;
+  }
+  for (int l = 1; l < n_levels; ++l) {
+    if (l < n_h) build_h_transfer(&mg.transfers[l], &mg.levels[l - 1], &mg.levels[l], 1);
+    else if (l < n_cg) build_p_transfer(&mg.transfers[l], &mg.levels[l - 1], &mg.levels[l]);
+    else build_dg_transfer(&mg.transfers[l], &mg.levels[l - 1], &mg.levels[l]);
+  }
+  orc_level *F = &mg.levels[n_levels - 1];
+  const int64_t N = F->N;
+  info->n_dofs = N;
+  info->n_levels = n_levels;
+  double *b = (double *)malloc(sizeof(double) * N);
+  orc_dg_rhs(box, p, nq_rhs, c_pen, b);
+  double *x = (double *)calloc(N, sizeof(double));
+  double *r = (double *)malloc(sizeof(double) * N);
+  double *z = (double *)malloc(sizeof(double) * N);
+  double *pv = (double *)malloc(sizeof(double) * N);
+  double *v = (double *)malloc(sizeof(double) * N);
+  memcpy(r, b, sizeof(double) * N);
+  double res = sqrt(dot(N, r, r));
+  info->initial_residual = res;
+  const double tol = reduce * res;
+  int it = 0;
+  double rho = 0, rho_old = 0;
+  while (res > tol && it < maxit) {
+    for (int l = 0; l < n_levels - 1; ++l)
+      for (int64_t i = 0; i < mg.levels[l].N; ++i) mg.levels[l].def[i] = 0.0;
+    memcpy(F->def, r, sizeof(double) * N);
+    vcycle(&mg, n_levels - 1);
+    memcpy(z, F->sol, sizeof(double) * N);
+    rho_old = rho;
+    rho = dot(N, r, z);
+    if (it == 0) memcpy(pv, z, sizeof(double) * N);
+    else {
+      const double beta = rho / rho_old;
+      for (int64_t i = 0; i < N; ++i) pv[i] = z[i] + beta * pv[i];
+    }
+    ++it;
+    level_vmult(F, v, pv);
+    const double alpha = rho / dot(N, pv, v);
+    for (int64_t i = 0; i < N; ++i) { x[i] += alpha * pv[i]; r[i] -= alpha * v[i]; }
+    res = sqrt(dot(N, r, r));
+  }
+  info->iterations = it;
+  info->final_residual = res;
+  info->reduction_per_step = it > 0 ? pow(res / info->initial_residual, 1.0 / it) : 1.0;
+  info->l2_error = orc_dg_l2_error(box, p, p + 2, x);
+  if (x_out) memcpy(x_out, x, sizeof(double) * N);
+  free(b); free(x); free(r); free(z); free(pv); free(v);
+  for (int l = 1; l < n_levels; ++l) transfer_free(&mg.transfers[l]);
+  for (int l = 0; l < n_levels; ++l) level_free(&mg.levels[l]);
+  free(mg.levels);
+  free(mg.transfers);
+  return 0;
 }

@@ -1,0 +1,334 @@
+// DG-SIPG face terms on axis-aligned boxes (the interior-penalty operator of
+// include/operators/portable_laplace_operator_dg.h with the fluxes of
+// include/kernels/laplace_dg_kokkos_kernels.h:833-2026 and
+// source/plain_laplace_solver_dg/program.cc:128-217).
+//
+// The cell stiffness term comes from the continuous slab kernel run on the discontinuous
+// numbering (dof = cell * N^3 + l).  This file adds the face terms with one fused kernel:
+// a block takes a batch of cells, and for each of the six faces of each cell it forms its
+// own trace (the node layer on the face and the reference normal derivative) and the
+// neighbour's trace, recomputed from the neighbour's DoFs straight from L2.  The reference
+// instead writes every trace to global face buffers and reads them back in three more
+// launches.  Each face is evaluated from both sides; every cell writes only its own DoFs,
+// so there are no atomics and no face buffers.
+//
+// On GLL nodes with the (p+1)-point Gauss face rule the face integrals of products of
+// basis functions are exact, so the face quadrature is applied as the 1D GLL mass matrix
+// M1 = S diag(w) S^T in each tangential direction.
+#include <algorithm>
+#include <vector>
+
+#include "dg.hpp"
+#include "pmg_internal.hpp"
+
+namespace pmg {
+namespace {
+
+template <int N, typename T> struct DGTab {
+  T M1[N * N];  // 1D mass matrix of the GLL Lagrange basis
+  T dphi0[N];   // phi_i'(0)
+  T dphi1[N];   // phi_i'(1)
+};
+
+struct DGGeo {
+  double h[3];   // cell extents
+  double c_pen;  // sigma = c_pen / h_normal
+  int dirichlet; // face mask (x-, x+, y-, y+, z-, z+)
+};
+
+// local index of the node with coordinate `layer` along d and tangential (a, b)
+template <int N> __device__ __forceinline__ int face_node(int d, int layer, int a, int b) {
+  // tangential directions in increasing axis order: d=0 -> (y, z); d=1 -> (x, z); d=2 -> (x, y)
+  const int i = d == 0 ? layer : a;
+  const int j = d == 1 ? layer : (d == 0 ? a : b);
+  const int k = d == 2 ? layer : b;
+  return (k * N + j) * N + i;
+}
+
+template <int N> constexpr int dg_batch() { return (128 / (N * N)) > 0 ? 128 / (N * N) : 1; }
+
+template <int N, typename T>
+__global__ void __launch_bounds__(128) dg_face_kernel(const DGTab<N, T> tab, const DGGeo geo,
+                                                      const T *__restrict__ src,
+                                                      T *__restrict__ dst,
+                                                      const int32_t *__restrict__ nbr,
+                                                      int64_t n_cells) {
+  constexpr int N2 = N * N, N3 = N2 * N, B = dg_batch<N>();
+  __shared__ T own[B][N3];
+  __shared__ T out[B][N3];
+  __shared__ T F1[B][N2], F2[B][N2], G1[B][N2], G2[B][N2];
+  const int t = threadIdx.x;
+  for (int64_t base = int64_t(blockIdx.x) * B; base < n_cells; base += int64_t(gridDim.x) * B) {
+    for (int e = t; e < B * N3; e += blockDim.x) {
+      const int b = e / N3, l = e - b * N3;
+      const int64_t c = base + b;
+      own[b][l] = c < n_cells ? src[c * N3 + l] : T(0);
+      out[b][l] = T(0);
+    }
+    __syncthreads();
+    for (int f = 0; f < 6; ++f) {
+      const int d = f >> 1, s = f & 1;
+      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+      const T hd = (T)geo.h[d];
+      const T sgn_h = (s ? T(1) : T(-1)) / hd; // n . grad = sgn_h * d/dxi_d
+      const T area = (T)(geo.h[ta] * geo.h[tb]);
+      const T sigma = (T)(geo.c_pen / geo.h[d]);
+      const T *dphi_own = s ? tab.dphi1 : tab.dphi0;
+      const T *dphi_nb = s ? tab.dphi0 : tab.dphi1;
+      const int own_layer = s ? N - 1 : 0, nb_layer = s ? 0 : N - 1;
+      const bool bc_dirichlet = (geo.dirichlet >> f) & 1;
+      if (t < B * N2) {
+        const int b = t / N2, ab = t - b * N2, a = ab % N, bb = ab / N;
+        const int64_t c = base + b;
+        T f1 = T(0), f2 = T(0);
+        if (c < n_cells) {
+          T vo = own[b][face_node<N>(d, own_layer, a, bb)], dn = T(0);
+#pragma unroll
+          for (int i = 0; i < N; ++i) dn += dphi_own[i] * own[b][face_node<N>(d, i, a, bb)];
+          dn *= sgn_h;
+          const int32_t nb = nbr[c * 6 + f];
+          if (nb >= 0) {
+            const T *un = src + int64_t(nb) * N3;
+            const T vn = un[face_node<N>(d, nb_layer, a, bb)];
+            T dnn = T(0);
+#pragma unroll
+            for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * un[face_node<N>(d, i, a, bb)];
+            dnn *= sgn_h;
+            const T jump = vo - vn;
+            f1 = sigma * jump - T(0.5) * (dn + dnn);
+            f2 = T(-0.5) * jump;
+          } else if (bc_dirichlet) { // mirror: u+ = -u-, d_n u+ = d_n u-
+            f1 = sigma * T(2) * vo - dn;
+            f2 = -vo;
+          }
+        }
+        F1[b][ab] = f1 * area;
+        F2[b][ab] = f2 * area;
+      }
+      __syncthreads();
+      // face mass along a, then along b
+      if (t < B * N2) {
+        const int b = t / N2, ab = t - b * N2, a = ab % N, bb = ab / N;
+        T g1 = T(0), g2 = T(0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          g1 += tab.M1[a * N + k] * F1[b][bb * N + k];
+          g2 += tab.M1[a * N + k] * F2[b][bb * N + k];
+        }
+        G1[b][ab] = g1;
+        G2[b][ab] = g2;
+      }
+      __syncthreads();
+      if (t < B * N2) {
+        const int b = t / N2, ab = t - b * N2, a = ab % N, bb = ab / N;
+        T tv = T(0), tn = T(0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          tv += tab.M1[bb * N + k] * G1[b][k * N + a];
+          tn += tab.M1[bb * N + k] * G2[b][k * N + a];
+        }
+        // value test on the face layer, normal-derivative test on every layer along d
+        out[b][face_node<N>(d, own_layer, a, bb)] += tv;
+        tn *= sgn_h;
+#pragma unroll
+        for (int i = 0; i < N; ++i) out[b][face_node<N>(d, i, a, bb)] += tn * dphi_own[i];
+      }
+      __syncthreads();
+    }
+    for (int e = t; e < B * N3; e += blockDim.x) {
+      const int b = e / N3, l = e - b * N3;
+      const int64_t c = base + b;
+      if (c < n_cells) dst[c * N3 + l] += out[b][l];
+    }
+    __syncthreads();
+  }
+}
+
+// face self terms of the diagonal: a node on the face layer of face (d, s) with
+// g = phi'(s) (+-1)/h gets m (sigma - g) (inner) or m (2 sigma - 2 g) (Dirichlet),
+// m = h_a h_b M1[a][a] M1[b][b]
+template <int N, typename T>
+__global__ void dg_face_diag_kernel(const DGTab<N, T> tab, const DGGeo geo, T *__restrict__ diag,
+                                    const int32_t *__restrict__ nbr, int64_t n_cells) {
+  constexpr int N3 = N * N * N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_cells * N3;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = e / N3;
+    const int l = int(e - c * N3);
+    const int idx[3] = {l % N, (l / N) % N, l / (N * N)};
+    T add = T(0);
+    for (int f = 0; f < 6; ++f) {
+      const int d = f >> 1, s = f & 1;
+      if (idx[d] != (s ? N - 1 : 0)) continue;
+      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+      const int32_t nb = nbr[c * 6 + f];
+      const bool dir = (geo.dirichlet >> f) & 1;
+      if (nb < 0 && !dir) continue;
+      const T sigma = (T)(geo.c_pen / geo.h[d]);
+      const T g = (s ? tab.dphi1[N - 1] : -tab.dphi0[0]) / (T)geo.h[d];
+      const T m = (T)(geo.h[ta] * geo.h[tb]) * tab.M1[idx[ta] * N + idx[ta]] * tab.M1[idx[tb] * N + idx[tb]];
+      add += nb >= 0 ? m * (sigma - g) : T(2) * m * (sigma - g);
+    }
+    diag[e] += add;
+  }
+}
+
+template <typename T> __global__ void add_kernel(T *__restrict__ dst, const double *__restrict__ src, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] += (T)src[i];
+}
+
+template <int N, typename T> DGTab<N, T> make_dg_tab(const DGHost &h) {
+  DGTab<N, T> t;
+  for (int a = 0; a < N * N; ++a) t.M1[a] = (T)h.M1[a];
+  for (int a = 0; a < N; ++a) {
+    t.dphi0[a] = (T)h.dphi0[a];
+    t.dphi1[a] = (T)h.dphi1[a];
+  }
+  return t;
+}
+
+DGGeo make_geo(const DGHost &h) {
+  DGGeo g;
+  for (int d = 0; d < 3; ++d) g.h[d] = h.h[d];
+  g.c_pen = h.c_pen;
+  g.dirichlet = h.dirichlet;
+  return g;
+}
+
+template <int N, typename T>
+void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms, cudaStream_t s,
+                 bool diag) {
+  if (diag) {
+    const int grid = (int)std::min<int64_t>((n_cells * N * N * N + 255) / 256, (int64_t)sms * 16);
+    dg_face_diag_kernel<N, T><<<std::max(grid, 1), 256, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
+                                                                  static_cast<T *>(dst), h.nbr.as<int32_t>(), n_cells);
+  } else {
+    constexpr int B = dg_batch<N>();
+    const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 16);
+    dg_face_kernel<N, T><<<std::max(grid, 1), 128, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
+                                                            static_cast<const T *>(src), static_cast<T *>(dst),
+                                                            h.nbr.as<int32_t>(), n_cells);
+  }
+  PMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+void face_dispatch(int degree, const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms,
+                   cudaStream_t s, bool diag) {
+  switch (degree) {
+  case 1: face_launch<2, T>(h, src, dst, n_cells, sms, s, diag); break;
+  case 2: face_launch<3, T>(h, src, dst, n_cells, sms, s, diag); break;
+  case 3: face_launch<4, T>(h, src, dst, n_cells, sms, s, diag); break;
+  case 4: face_launch<5, T>(h, src, dst, n_cells, sms, s, diag); break;
+  case 5: face_launch<6, T>(h, src, dst, n_cells, sms, s, diag); break;
+  case 6: face_launch<7, T>(h, src, dst, n_cells, sms, s, diag); break;
+  default: fail(PMG_EINVAL, "DG degree must be in [1,6]");
+  }
+}
+
+} // namespace
+
+void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen) {
+  const int N = degree + 1;
+  const Tables1D t = make_tables(degree, N);
+  h.M1.assign(N * N, 0.0);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      double s = 0;
+      for (int q = 0; q < N; ++q) s += t.S[i * N + q] * t.S[j * N + q] * t.W[q];
+      h.M1[i * N + j] = s;
+    }
+  h.dphi0 = lagrange_derivative_at(degree, 0.0);
+  h.dphi1 = lagrange_derivative_at(degree, 1.0);
+  for (int d = 0; d < 3; ++d) h.h[d] = (mesh.box.hi[d] - mesh.box.lo[d]) / double(mesh.n[d]);
+  h.c_pen = c_pen > 0 ? c_pen : degree * (degree + 1.0);
+  h.dirichlet = mesh.box.dirichlet_mask;
+  // neighbour table [cell][2 d + s], -1 on the boundary
+  const int64_t C = mesh.n_cells, nx = mesh.n[0], ny = mesh.n[1];
+  std::vector<int32_t> lut(C);
+  for (int64_t c = 0; c < C; ++c) {
+    const int64_t x = mesh.cell_xyz[3 * c], y = mesh.cell_xyz[3 * c + 1], z = mesh.cell_xyz[3 * c + 2];
+    lut[(z * ny + y) * nx + x] = (int32_t)c;
+  }
+  std::vector<int32_t> nb(C * 6);
+  for (int64_t c = 0; c < C; ++c) {
+    const int64_t xyz[3] = {mesh.cell_xyz[3 * c], mesh.cell_xyz[3 * c + 1], mesh.cell_xyz[3 * c + 2]};
+    for (int f = 0; f < 6; ++f) {
+      int64_t q[3] = {xyz[0], xyz[1], xyz[2]};
+      const int d = f >> 1;
+      q[d] += (f & 1) ? 1 : -1;
+      nb[c * 6 + f] = (q[d] < 0 || q[d] >= mesh.n[d]) ? -1 : lut[(q[2] * ny + q[1]) * nx + q[0]];
+    }
+  }
+  h.nbr = upload(nb);
+}
+
+void dg_apply_faces(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells,
+                    int sms, cudaStream_t s) {
+  if (dtype == PMG_F64) face_dispatch<double>(degree, h, src, dst, n_cells, sms, s, false);
+  else face_dispatch<float>(degree, h, src, dst, n_cells, sms, s, false);
+}
+
+void dg_add_face_diagonal(const DGHost &h, int degree, int dtype, void *diag, int64_t n_cells, int sms,
+                          cudaStream_t s) {
+  if (dtype == PMG_F64) face_dispatch<double>(degree, h, nullptr, diag, n_cells, sms, s, true);
+  else face_dispatch<float>(degree, h, nullptr, diag, n_cells, sms, s, true);
+}
+
+// weak Dirichlet data of u = exp(x) sin(pi y) cos(pi z): b_l += (g, 2 sigma phi_l - d_n phi_l)
+// on Dirichlet faces, nq-point Gauss rule per tangential direction (host, setup only)
+void dg_add_boundary_rhs(const DGHost &h, const BoxMesh &mesh, int degree, int nq, int dtype, void *b,
+                         cudaStream_t s) {
+  const int N = degree + 1, N3 = N * N * N;
+  const Tables1D t = make_tables(degree, nq);
+  const int64_t C = mesh.n_cells;
+  std::vector<double> add(C * N3, 0.0);
+  bool any = false;
+  for (int64_t c = 0; c < C; ++c) {
+    const int64_t xyz[3] = {mesh.cell_xyz[3 * c], mesh.cell_xyz[3 * c + 1], mesh.cell_xyz[3 * c + 2]};
+    for (int f = 0; f < 6; ++f) {
+      const int d = f >> 1, sd = f & 1;
+      const bool outside = sd ? xyz[d] == mesh.n[d] - 1 : xyz[d] == 0;
+      if (!outside || !((h.dirichlet >> f) & 1)) continue;
+      any = true;
+      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+      const double sigma = h.c_pen / h.h[d], sgn_h = (sd ? 1.0 : -1.0) / h.h[d];
+      for (int bb = 0; bb < N; ++bb)
+        for (int a = 0; a < N; ++a) {
+          double gab = 0.0; // (g, phi_a phi_b) over the face
+          for (int qb = 0; qb < nq; ++qb)
+            for (int qa = 0; qa < nq; ++qa) {
+              double x[3];
+              x[d] = mesh.box.lo[d] + (xyz[d] + (sd ? 1.0 : 0.0)) * h.h[d];
+              x[ta] = mesh.box.lo[ta] + (xyz[ta] + t.xg[qa]) * h.h[ta];
+              x[tb] = mesh.box.lo[tb] + (xyz[tb] + t.xg[qb]) * h.h[tb];
+              const double g = std::exp(x[0]) * std::sin(M_PI * x[1]) * std::cos(M_PI * x[2]);
+              gab += g * t.W[qa] * t.W[qb] * h.h[ta] * h.h[tb] * t.S[a * nq + qa] * t.S[bb * nq + qb];
+            }
+          for (int i = 0; i < N; ++i) {
+            int idx[3];
+            idx[d] = i;
+            idx[ta] = a;
+            idx[tb] = bb;
+            const int l = (idx[2] * N + idx[1]) * N + idx[0];
+            const double phi_face = (i == (sd ? N - 1 : 0)) ? 1.0 : 0.0;
+            const double dphi = (sd ? h.dphi1[i] : h.dphi0[i]) * sgn_h;
+            add[c * N3 + l] += gab * (2.0 * sigma * phi_face - dphi);
+          }
+        }
+    }
+  }
+  if (!any) return;
+  DeviceBuffer tmp = upload(add);
+  int sms = 0, dev = 0;
+  PMG_CUDA(cudaGetDevice(&dev));
+  PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int grid = (int)std::min<int64_t>((C * N3 + 255) / 256, (int64_t)sms * 16);
+  if (dtype == PMG_F64) add_kernel<double><<<grid, 256, 0, s>>>(static_cast<double *>(b), tmp.as<double>(), C * N3);
+  else add_kernel<float><<<grid, 256, 0, s>>>(static_cast<float *>(b), tmp.as<double>(), C * N3);
+  PMG_LAUNCH_CHECK();
+  PMG_CUDA(cudaStreamSynchronize(s)); // tmp is freed on return
+}
+
+} // namespace pmg

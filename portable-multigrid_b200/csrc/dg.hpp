@@ -1,0 +1,26 @@
+// DG-SIPG face terms (dg.cu).
+#pragma once
+
+#include <vector>
+
+#include "pmg_internal.hpp"
+
+namespace pmg {
+
+struct DGHost {
+  std::vector<double> M1, dphi0, dphi1; // 1D GLL mass matrix, basis derivatives at 0 and 1
+  double h[3] = {0, 0, 0};
+  double c_pen = 0;  // sigma = c_pen / h on every face (uniform boxes)
+  int dirichlet = 0; // face mask
+  DeviceBuffer nbr;  // int32 [cell][6] neighbour cells, -1 on the boundary
+};
+
+void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen);
+void dg_apply_faces(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells,
+                    int sms, cudaStream_t s);
+void dg_add_face_diagonal(const DGHost &h, int degree, int dtype, void *diag, int64_t n_cells, int sms,
+                          cudaStream_t s);
+void dg_add_boundary_rhs(const DGHost &h, const BoxMesh &mesh, int degree, int nq, int dtype, void *b,
+                         cudaStream_t s);
+
+} // namespace pmg

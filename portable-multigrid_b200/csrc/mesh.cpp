@@ -83,4 +83,19 @@ Numbering make_numbering(const BoxMesh &m, int p, bool keep_lattice) {
   return nb;
 }
 
+// FE_DGQ(p): every cell owns its (p+1)^3 DoFs, numbered cell by cell in lexicographic order
+// (deal.II numbers FE_DGQ DoFs the same way); nothing is constrained, Dirichlet data enter
+// weakly through the face terms.
+Numbering make_numbering_dg(const BoxMesh &m, int p) {
+  Numbering nb;
+  nb.p = p;
+  const int64_t nm3 = int64_t(p + 1) * (p + 1) * (p + 1);
+  PMG_REQUIRE(m.n_cells * nm3 < (int64_t(1) << 32) - 1, "too many DoFs for 32-bit indices");
+  nb.n_dofs = m.n_cells * nm3;
+  nb.plain.resize(nb.n_dofs);
+  for (int64_t i = 0; i < nb.n_dofs; ++i) nb.plain[i] = (uint32_t)i;
+  nb.constrained.assign(nb.n_dofs, 0);
+  return nb;
+}
+
 } // namespace pmg

@@ -4,6 +4,7 @@
 #include <cmath>
 
 #include "laplace_kernels.cuh"
+#include "dg.hpp"
 #include "pmg_internal.hpp"
 
 namespace pmg {
@@ -125,6 +126,7 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
       } else {
         double f = 1.0;
         if (f_kind == 1) f = 3.0 * M_PI * M_PI * sin(M_PI * xq[0]) * sin(M_PI * xq[1]) * sin(M_PI * xq[2]);
+        if (f_kind == 2) f = (2.0 * M_PI * M_PI - 1.0) * exp(xq[0]) * sin(M_PI * xq[1]) * cos(M_PI * xq[2]);
         fq[q] = f * fabs(det) * wq;
       }
     }
@@ -255,6 +257,11 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   PMG_REQUIRE(prm.dtype == PMG_F64 || prm.dtype == PMG_F32, "dtype must be PMG_F64 or PMG_F32");
   PMG_REQUIRE(prm.coeff_kind >= 0 && prm.coeff_kind <= 2, "bad coeff_kind");
   PMG_REQUIRE(prm.coeff_kind != PMG_COEFF_VALUES || prm.coeff_qp, "coeff_qp is required");
+  PMG_REQUIRE(prm.kind == PMG_OP_LAPLACE || prm.kind == PMG_OP_DG_SIPG, "bad operator kind");
+  if (prm.kind == PMG_OP_DG_SIPG) {
+    PMG_REQUIRE(mesh.m.box.deform == 0, "the DG operator needs an undeformed (axis-aligned) box");
+    PMG_REQUIRE(prm.coeff_kind == PMG_COEFF_NONE, "the DG operator has no coefficient");
+  }
   int n_dev = 0;
   if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
     (void)cudaGetLastError();
@@ -269,8 +276,10 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   op.coeff_kind = prm.coeff_kind;
   op.mesh = mesh.m;
   op.n_cells = mesh.m.n_cells;
+  op.kind = prm.kind;
   int geometry = prm.geometry;
-  if (geometry == PMG_GEOMETRY_AUTO) geometry = mesh.m.box.deform ? PMG_GEOMETRY_FULL : PMG_GEOMETRY_AFFINE;
+  if (geometry == PMG_GEOMETRY_AUTO || op.kind == PMG_OP_DG_SIPG)
+    geometry = mesh.m.box.deform ? PMG_GEOMETRY_FULL : PMG_GEOMETRY_AFFINE;
   PMG_REQUIRE(geometry == PMG_GEOMETRY_FULL || geometry == PMG_GEOMETRY_AFFINE, "bad geometry");
   PMG_REQUIRE(!(geometry == PMG_GEOMETRY_AFFINE && mesh.m.box.deform), "affine geometry needs an undeformed box");
   op.geometry = geometry;
@@ -282,8 +291,14 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   op.n_groups = (op.n_cells + op.cpw - 1) / op.cpw;
 
   // numbering (setup_dof_indices_per_color, bk3.h:360-437)
-  op.num = make_numbering(mesh.m, op.degree, true);
+  op.num = op.kind == PMG_OP_DG_SIPG ? make_numbering_dg(mesh.m, op.degree)
+                                     : make_numbering(mesh.m, op.degree, true);
   op.n_dofs = op.num.n_dofs;
+  op.sms = num_sms(op.device);
+  if (op.kind == PMG_OP_DG_SIPG) {
+    op.dg = std::make_shared<DGHost>();
+    dg_setup(*op.dg, mesh.m, op.degree, prm.penalty);
+  }
 
   // index map with the sentinel, permuted into the Y-slab layout [group][k*N+i][e*N+j]
   {
@@ -390,8 +405,14 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
     L.resident_warps = op.warps_vmult;
     L.resident_warps_ring = op.warps_vmult_ring;
     L.err = op.err_flag.as<unsigned int>();
-    prof::Scope scope("vmult_cell", s);
-    vmult_fn(op.degree)(L);
+    {
+      prof::Scope scope("vmult_cell", s);
+      vmult_fn(op.degree)(L);
+    }
+    if (op.dg) {
+      prof::Scope scope("vmult_dg_faces", s);
+      dg_apply_faces(*op.dg, op.degree, op.dtype, src, dst, op.n_cells, op.sms, s);
+    }
   }
   if (op.n_constrained > 0) {
     prof::Scope scope("vmult_constrained", s);
@@ -419,6 +440,7 @@ void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s) {
     prof::Scope scope("diag_cell", s);
     diag_fn(op.degree)(L);
   }
+  if (op.dg) dg_add_face_diagonal(*op.dg, op.degree, op.dtype, op.inv_diag.get(), op.n_cells, op.sms, s);
   const int grid = (int)std::min<int64_t>(4096, (op.n_dofs + 255) / 256);
   if (op.dtype == PMG_F64) {
     invert_diagonal_kernel<double><<<grid, 256, 0, s>>>(op.inv_diag.as<double>(), op.n_dofs);
@@ -436,7 +458,7 @@ void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s) {
 }
 
 void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, cudaStream_t s) {
-  PMG_REQUIRE(f_kind == 0 || f_kind == 1, "f_kind must be 0 or 1");
+  PMG_REQUIRE(f_kind >= 0 && f_kind <= 2, "f_kind must be 0, 1 or 2");
   if (nq <= 0) nq = op.nq;
   PMG_REQUIRE(nq >= 1 && nq <= kMaxNq, "nq must be in [1,8]");
   PMG_CUDA(cudaSetDevice(op.device));
@@ -452,6 +474,7 @@ void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, 
                                                      static_cast<float *>(b), op.idx.as<uint32_t>(), f_kind);
   PMG_LAUNCH_CHECK();
   PMG_CUDA(cudaStreamSynchronize(s)); // xyz is freed on return
+  if (op.dg && f_kind == 2) dg_add_boundary_rhs(*op.dg, op.mesh, op.degree, nq, op.dtype, b, s);
 }
 
 void operator_copy_geometry(const pmg_operator &op, double *host) {

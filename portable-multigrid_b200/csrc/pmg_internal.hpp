@@ -134,6 +134,7 @@ struct Tables1D {
 };
 Tables1D make_tables(int p, int nq);
 std::vector<double> gauss_lobatto_points(int n);
+std::vector<double> lagrange_derivative_at(int p, double x); // FE_Q(p) basis derivatives at x
 std::vector<double> p_transfer_matrix(int pc, int pf);  // [nc][nf]
 std::vector<double> h_transfer_matrix(int p);           // [p+1][2p+1]
 
@@ -158,6 +159,7 @@ struct Numbering {
 
 BoxMesh make_box(const pmg_box &b);
 Numbering make_numbering(const BoxMesh &m, int p, bool keep_lattice);
+Numbering make_numbering_dg(const BoxMesh &m, int p); // dof = cell * (p+1)^3 + l
 
 } // namespace pmg
 
@@ -168,8 +170,14 @@ struct pmg_mesh {
   pmg::BoxMesh m;
 };
 
+namespace pmg {
+struct DGHost;
+}
+
 struct pmg_operator {
   int device = 0;
+  int kind = PMG_OP_LAPLACE;        // PMG_OP_LAPLACE or PMG_OP_DG_SIPG
+  std::shared_ptr<pmg::DGHost> dg;  // face data of a DG operator
   int degree = 1, nm = 2, nq = 2;
   int dtype = PMG_F64;
   int geometry = PMG_GEOMETRY_FULL; // resolved: FULL or AFFINE
@@ -189,6 +197,7 @@ struct pmg_operator {
   bool has_diag = false;
   int64_t warps_vmult = 0, warps_diag = 0; // resident warps of the cell kernels
   int64_t warps_vmult_ring = 0;             // ... of the geometry-ring vmult variant
+  int sms = 0;                              // SM count of the device
   pmg::DeviceBuffer err_flag;               // set by bounded device waits that give up
 };
 

@@ -118,6 +118,14 @@ Tables1D make_tables(int p, int nq) {
   return t;
 }
 
+std::vector<double> lagrange_derivative_at(int p, double x) {
+  std::vector<ld> xl;
+  gauss_lobatto(p + 1, xl);
+  std::vector<double> d(p + 1);
+  for (int i = 0; i <= p; ++i) d[i] = (double)lagrange_derivative(xl, i, (ld)x);
+  return d;
+}
+
 std::vector<double> gauss_lobatto_points(int n) {
   std::vector<ld> x;
   gauss_lobatto(n, x);

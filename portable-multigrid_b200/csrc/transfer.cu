@@ -107,7 +107,24 @@ void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_opera
   const int pc = coarse.degree, pf = fine.degree;
   std::vector<double> P;
   std::vector<uint32_t> cidx, fidx;
-  if (coarse.mesh.box.refine == fine.mesh.box.refine) {
+  if (fine.kind == PMG_OP_DG_SIPG) {
+    // DG <-> CG at equal degree (ContinuousTransfer): identity on every cell, unit weights
+    PMG_REQUIRE(coarse.kind == PMG_OP_LAPLACE, "the coarse level of a DG transfer must be continuous");
+    PMG_REQUIRE(pc == pf && coarse.mesh.box.refine == fine.mesh.box.refine,
+                "DG <-> CG transfer needs equal degrees on the same mesh");
+    t.kind = 2;
+    t.nc = t.nf = pc + 1;
+    t.n_patches = fine.n_cells;
+    P.assign(t.nc * t.nf, 0.0);
+    for (int i = 0; i < t.nc; ++i) P[i * t.nf + i] = 1.0;
+    cidx.resize(coarse.num.plain.size());
+    for (size_t e = 0; e < cidx.size(); ++e) {
+      const uint32_t d = coarse.num.plain[e];
+      cidx[e] = coarse.num.constrained[d] ? kInvalid : d;
+    }
+    fidx = fine.num.plain;
+  } else if (coarse.mesh.box.refine == fine.mesh.box.refine) {
+    PMG_REQUIRE(coarse.kind == PMG_OP_LAPLACE, "a DG level can only be the finest level of a transfer");
     PMG_REQUIRE(pc < pf, "polynomial transfer needs degree_coarse < degree_fine");
     t.kind = 0;
     t.nc = pc + 1;

@@ -6,7 +6,7 @@
 struct pmg_transfer {
   int device = 0;
   int dtype = PMG_F64;
-  int kind = 0; // 0 polynomial, 1 geometric
+  int kind = 0; // 0 polynomial, 1 geometric, 2 DG <-> CG
   int nc = 0, nf = 0;
   int64_t n_patches = 0, n_coarse = 0, n_fine = 0;
   pmg::DeviceBuffer P1d, coarse_idx, fine_idx, weights;

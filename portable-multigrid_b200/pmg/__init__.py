@@ -33,6 +33,7 @@ HEADER_PATH = os.path.join(REPO_ROOT, "include", "pmg", "pmg.h")
 F64, F32 = 0, 1
 GEOMETRY_AUTO, GEOMETRY_FULL, GEOMETRY_AFFINE = 0, 1, 2
 COEFF_NONE, COEFF_KAPPA, COEFF_VALUES = 0, 1, 2
+OP_LAPLACE, OP_DG_SIPG = 0, 1
 INVALID = 0xFFFFFFFF
 STATUS = {0: "PMG_OK", -1: "PMG_EINVAL", -2: "PMG_ENOMEM", -3: "PMG_ECUDA",
           -4: "PMG_ENONFINITE", -5: "PMG_ENOCONV", -6: "PMG_EBOUNDS", -7: "PMG_ESTATE",
@@ -81,7 +82,8 @@ def doubling_box(cycle: int) -> Box:
 
 class OperatorParams(C.Structure):
     _fields_ = [("degree", C.c_int32), ("dtype", C.c_int32), ("geometry", C.c_int32),
-                ("coeff_kind", C.c_int32), ("coeff_qp", C.c_void_p), ("device", C.c_int32)]
+                ("coeff_kind", C.c_int32), ("coeff_qp", C.c_void_p), ("device", C.c_int32),
+                ("kind", C.c_int32), ("penalty", C.c_double)]
 
 
 class ChebyshevParams(C.Structure):
@@ -250,13 +252,15 @@ class LaplaceOperator:
     """Continuous FE_Q(degree) Laplace operator on a box mesh (LaplaceOperatorBK3)."""
 
     def __init__(self, mesh: Mesh, degree: int, dtype: int = F64, geometry: int = GEOMETRY_AUTO,
-                 coeff_kind: int = COEFF_NONE, coeff_qp=None, device: int = 0):
+                 coeff_kind: int = COEFF_NONE, coeff_qp=None, device: int = 0,
+                 kind: int = OP_LAPLACE, penalty: float = 0.0):
         self.mesh = mesh
         self.degree = degree
         self.dtype = dtype
         self.device = device
+        self.kind = kind
         self._coeff = None
-        prm = OperatorParams(degree, dtype, geometry, coeff_kind, None, device)
+        prm = OperatorParams(degree, dtype, geometry, coeff_kind, None, device, kind, penalty)
         if coeff_qp is not None:
             self._coeff = np.ascontiguousarray(coeff_qp, dtype=np.float64)
             prm.coeff_qp = self._coeff.ctypes.data_as(C.c_void_p)
@@ -419,6 +423,13 @@ class VCycleMultigrid:
             self.h = None
 
 
+def DGLaplaceOperator(mesh: Mesh, degree: int, dtype: int = F64, penalty: float = 0.0, device: int = 0):
+    """FE_DGQ(degree) symmetric interior penalty operator (LaplaceOperatorDG); penalty <= 0
+    selects the reference's p(p+1)."""
+    return LaplaceOperator(mesh, degree, dtype, GEOMETRY_AFFINE, COEFF_NONE, None, device,
+                           OP_DG_SIPG, penalty)
+
+
 def solve_cg(A: LaplaceOperator, x, b, precond: VCycleMultigrid | None = None, reduce=1e-9,
              abs_tol=1e-16, max_iterations=100, raise_on_noconv=True):
     info = CGInfo()
@@ -436,11 +447,13 @@ class Hierarchy:
     (tests/poisson_cube_bk3/program.cc:263-515): FE_Q(1) on every refinement of the box
     (h-levels), then the degrees of `pseq` (descending, ending in 1) on the finest mesh;
     Chebyshev(cheb_degree, range 15, 10 eigenvalue iterations) on levels > 0 and
-    Chebyshev-to-1e-3 on level 0.  The finest-level FP64 operator `fine64` is the CG matrix."""
+    Chebyshev-to-1e-3 on level 0.  With dg=True an FE_DGQ(pseq[0]) SIPG level sits on top,
+    connected by the DG <-> CG transfer.  The finest-level FP64 operator `fine64` is the CG
+    matrix."""
 
     def __init__(self, box: Box, pseq, mg_dtype=F32, cheb_degree=5, geometry=GEOMETRY_AUTO,
                  coeff_kind=COEFF_NONE, coeff_qp=None, device=0, smoothing_range=15.0,
-                 eig_iterations=10, coarse_dtype=None):
+                 eig_iterations=10, coarse_dtype=None, dg=False, penalty=0.0):
         assert pseq[-1] == 1 and list(pseq) == sorted(pseq, reverse=True)
         self.box = box
         coarse_dtype = mg_dtype if coarse_dtype is None else coarse_dtype
@@ -451,10 +464,12 @@ class Hierarchy:
         for l, p in enumerate(degrees):
             mesh = self.meshes[min(l, n_h - 1)]
             dt = coarse_dtype if l == 0 else mg_dtype
-            finest = l == len(degrees) - 1
+            finest = l == len(degrees) - 1 and not dg
             kind = coeff_kind if (coeff_kind != COEFF_VALUES or finest) else COEFF_NONE
             self.levels.append(LaplaceOperator(mesh, p, dt, geometry, kind,
                                                coeff_qp if finest else None, device))
+        if dg:
+            self.levels.append(DGLaplaceOperator(self.meshes[-1], pseq[0], mg_dtype, penalty, device))
         for l in range(1, len(self.levels)):
             if self.levels[l].dtype != self.levels[l - 1].dtype:
                 raise ValueError("all multigrid levels must share one dtype")
@@ -464,8 +479,11 @@ class Hierarchy:
                 self.smoothers.append(Chebyshev(op, 0, 1e-3, op.m()))
             else:
                 self.smoothers.append(Chebyshev(op, cheb_degree, smoothing_range, eig_iterations))
-        self.fine64 = LaplaceOperator(self.meshes[-1], pseq[0], F64, geometry, coeff_kind, coeff_qp,
-                                      device)
+        if dg:
+            self.fine64 = DGLaplaceOperator(self.meshes[-1], pseq[0], F64, penalty, device)
+        else:
+            self.fine64 = LaplaceOperator(self.meshes[-1], pseq[0], F64, geometry, coeff_kind,
+                                          coeff_qp, device)
         self.mg = VCycleMultigrid(self.levels, self.transfers, self.smoothers)
 
     def estimate(self):

@@ -1,0 +1,115 @@
+"""Parity of the DG-SIPG operator (cell + fused face kernel), its diagonal, right-hand side
+with weakly imposed Dirichlet data, the DG <-> CG transfer and the DG multigrid solve with
+the CPU oracle, through the C ABI.  FP64 to 1e-12 relative, FP32 to 2e-5."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+import pmg  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+TOL = {pmg.F64: 1e-12, pmg.F32: 2e-5}
+
+
+def rel_err(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def obox(oracle, b):
+    return oracle.Box.make(coarse=tuple(b.coarse), refine=b.refine, lo=tuple(b.lo), hi=tuple(b.hi),
+                           deform=b.deform, amp=b.amp, dirichlet_mask=b.dirichlet_mask)
+
+
+BOXES = {
+    "cube_r2": dict(refine=2),
+    "ragged_3x2x1": dict(coarse=(3, 2, 1), refine=1, hi=(3.0, 2.0, 0.5)),
+    "neumann_x": dict(coarse=(2, 1, 1), refine=1, hi=(2.0, 1.0, 1.0), dirichlet_mask=0x3C),
+    "single_cell": dict(refine=0),
+}
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 6])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+@pytest.mark.parametrize("boxname", list(BOXES))
+def test_dg_vmult_matches_oracle(oracle, p, dtype, boxname):
+    box = pmg.Box.make(**BOXES[boxname])
+    ob = obox(oracle, box)
+    for c_pen in (0.0, 2.0 * (p + 1) ** 2):
+        op = pmg.DGLaplaceOperator(pmg.Mesh(box), p, dtype, c_pen)
+        assert op.m() == oracle.dg_n(ob, p)
+        src = np.random.default_rng(p).uniform(-1, 1, op.m())
+        ref = oracle.dg_vmult(ob, p, c_pen if c_pen > 0 else p * (p + 1.0), src)
+        td = torch.float64 if dtype == pmg.F64 else torch.float32
+        d = op.initialize_dof_vector()
+        op.vmult(d, torch.tensor(src, dtype=td, device="cuda"))
+        torch.cuda.synchronize()
+        assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype], c_pen
+
+
+@pytest.mark.parametrize("p", [1, 3, 5])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+def test_dg_diagonal_matches_oracle(oracle, p, dtype):
+    box = pmg.Box.make(coarse=(2, 1, 1), refine=1, hi=(2.0, 1.0, 1.0), dirichlet_mask=0x3E)
+    ob = obox(oracle, box)
+    op = pmg.DGLaplaceOperator(pmg.Mesh(box), p, dtype)
+    op.compute_diagonal()
+    inv = op.get_matrix_diagonal_inverse()
+    torch.cuda.synchronize()
+    ref = oracle.dg_diagonal(ob, p, p * (p + 1.0))
+    assert rel_err(1.0 / inv.double().cpu().numpy(), ref) < TOL[dtype] * 10
+
+
+@pytest.mark.parametrize("p", [1, 3])
+def test_dg_rhs_matches_oracle(oracle, p):
+    box = pmg.Box.make(refine=2)
+    ob = obox(oracle, box)
+    c_pen = 2.0 * (p + 1) ** 2
+    op = pmg.DGLaplaceOperator(pmg.Mesh(box), p, pmg.F64, c_pen)
+    b = op.assemble_rhs(2, p + 2)
+    torch.cuda.synchronize()
+    assert rel_err(b.cpu().numpy(), oracle.dg_rhs(ob, p, p + 2, c_pen)) < 1e-12
+
+
+@pytest.mark.parametrize("p", [1, 3])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+def test_dg_cg_transfer_matches_oracle(oracle, p, dtype):
+    box = pmg.Box.make(coarse=(2, 1, 1), refine=1, hi=(2.0, 1.0, 1.0))
+    ob = obox(oracle, box)
+    mesh = pmg.Mesh(box)
+    cg = pmg.LaplaceOperator(mesh, p, dtype)
+    dg = pmg.DGLaplaceOperator(mesh, p, dtype)
+    t = pmg.Transfer(cg, dg)
+    td = torch.float64 if dtype == pmg.F64 else torch.float32
+    rng = np.random.default_rng(3)
+    xc, xf = rng.uniform(-1, 1, cg.m()), rng.uniform(-1, 1, dg.m())
+    ref = oracle.dg_cg_transfer(ob, p, 0, xc, np.zeros(dg.m()))
+    d = torch.zeros(dg.m(), dtype=td, device="cuda")
+    t.prolongate_and_add(d, torch.tensor(xc, dtype=td, device="cuda"))
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype]
+    ref = oracle.dg_cg_transfer(ob, p, 1, xf, np.zeros(cg.m()))
+    d = torch.zeros(cg.m(), dtype=td, device="cuda")
+    t.restrict_and_add(d, torch.tensor(xf, dtype=td, device="cuda"))
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype] * 10
+
+
+@pytest.mark.parametrize("mg_dtype", [pmg.F64, pmg.F32])
+def test_dg_multigrid_solve_matches_oracle(oracle, mg_dtype):
+    """DG Q3 -> CG Q3 -> CG Q1 -> h-levels, penalty 2 (p+1)^2, manufactured
+    u = exp(x) sin(pi y) cos(pi z) with weak Dirichlet data, FP64 CG to 1e-10."""
+    p = 3
+    box = pmg.Box.make(refine=2)
+    ob = obox(oracle, box)
+    c_pen = 2.0 * (p + 1) ** 2
+    info_o, x_o = oracle.solve_dg(ob, p, [3, 1], cheb=5, c_pen=c_pen, reduce=1e-10, nq_rhs=p + 2,
+                                  want_x=True)
+    h = pmg.Hierarchy(box, [3, 1], mg_dtype=mg_dtype, cheb_degree=5, dg=True, penalty=c_pen)
+    b = h.fine64.assemble_rhs(2, p + 2)
+    x, info = h.solve(b, reduce=1e-10, max_iterations=200)
+    torch.cuda.synchronize()
+    assert info["converged"]
+    assert abs(info["iterations"] - info_o.iterations) <= (0 if mg_dtype == pmg.F64 else 1)
+    assert rel_err(x.cpu().numpy(), x_o) < 1e-7
+    assert abs(oracle.dg_l2_error(ob, p, p + 2, x.cpu().numpy()) / info_o.l2_error - 1) < 1e-6
