@@ -198,6 +198,7 @@ struct pmg_operator {
   int64_t warps_vmult = 0, warps_diag = 0; // resident warps of the cell kernels
   int64_t warps_vmult_ring = 0;             // ... of the geometry-ring vmult variant
   int sms = 0;                              // SM count of the device
+  std::vector<pmg::DeviceBuffer> cg_work;   // CG work vectors kept between solves
   pmg::DeviceBuffer err_flag;               // set by bounded device waits that give up
 };
 

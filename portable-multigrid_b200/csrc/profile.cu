@@ -52,6 +52,11 @@ void reset() {
 
 Scope::Scope(const char *name_, cudaStream_t s_) : name(name_), s(s_) {
   if (!g_on) return;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) {
+    (void)cudaGetLastError();
+    return; // no timing events inside a stream capture
+  }
   PMG_CUDA(cudaEventCreate(&a));
   PMG_CUDA(cudaEventRecord(a, s));
 }

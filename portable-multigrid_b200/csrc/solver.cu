@@ -4,6 +4,7 @@
 // reference's multigrid driver (tests/common/portable_multigrid_solver.h:147-271,
 // include/multigrid/portable_v_cycle_multigrid.h:163-206).
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "pmg_internal.hpp"
@@ -201,15 +202,67 @@ void mg_vcycle(pmg_mg &mg, int l, cudaStream_t s) {
   chebyshev_apply(*mg.smoothers[l], mg.sol[l].get(), mg.def[l].get(), false, s);
 }
 
+namespace {
+
+// defect[level] = 0 below the top (portable_multigrid_solver.h:180-183), then the cycle
+void mg_cycle_body(pmg_mg &mg, cudaStream_t s) {
+  const int L = (int)mg.levels.size() - 1;
+  for (int l = 0; l < L; ++l)
+    PMG_CUDA(cudaMemsetAsync(mg.def[l].get(), 0, dtype_size(mg.levels[l]->dtype) * mg.levels[l]->n_dofs, s));
+  mg_vcycle(mg, L, s);
+}
+
+bool graphs_allowed() {
+  static const bool on = [] {
+    const char *e = std::getenv("PMG_MG_GRAPH");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// Capture the cycle into a graph on a private stream (the eigenvalue estimates, which
+// synchronise and allocate, must have run before).  Any failure leaves graph == nullptr
+// and the cycle runs as plain launches.
+void mg_capture(pmg_mg &mg) {
+  for (auto *sm : mg.smoothers)
+    if (!sm->estimated) return;
+  cudaStream_t cs = nullptr;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+    (void)cudaGetLastError();
+    mg.graph_enabled = false;
+    return;
+  }
+  cudaGraph_t g = nullptr;
+  bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    try {
+      mg_cycle_body(mg, cs);
+    } catch (const Error &) {
+      ok = false;
+    }
+    ok = (cudaStreamEndCapture(cs, &g) == cudaSuccess) && ok;
+  }
+  if (ok) ok = cudaGraphInstantiate(&mg.graph, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  if (!ok) {
+    (void)cudaGetLastError();
+    mg.graph = nullptr;
+    mg.graph_enabled = false;
+  }
+}
+
+} // namespace
+
 void mg_vmult(pmg_mg &mg, void *dst, const void *src, int vec_dtype, cudaStream_t s) {
   const int L = (int)mg.levels.size() - 1;
   const pmg_operator &top = *mg.levels[L];
-  for (int l = 0; l < L; ++l) {
-    // defect[level] = 0 below the top (portable_multigrid_solver.h:180-183)
-    PMG_CUDA(cudaMemsetAsync(mg.def[l].get(), 0, dtype_size(mg.levels[l]->dtype) * mg.levels[l]->n_dofs, s));
-  }
+  for (auto *sm : mg.smoothers)
+    if (!sm->estimated) chebyshev_estimate(*sm, s);
   vec::convert(mg.def[L].get(), top.dtype, src, vec_dtype, top.n_dofs, s);
-  mg_vcycle(mg, L, s);
+  if (mg.graph_enabled && graphs_allowed() && !prof::enabled() && !mg.graph) mg_capture(mg);
+  if (mg.graph && !prof::enabled()) PMG_CUDA(cudaGraphLaunch(mg.graph, s));
+  else mg_cycle_body(mg, s);
   vec::convert(dst, vec_dtype, mg.sol[L].get(), top.dtype, top.n_dofs, s);
 }
 
@@ -225,7 +278,12 @@ void cg_solve(pmg_operator &A, pmg_mg *mg, void *x, const void *b, double reduce
   const int64_t N = A.n_dofs;
   const size_t bytes = dtype_size(dt) * N;
   if (!mg && !A.has_diag) operator_compute_inverse_diagonal(A, s);
-  DeviceBuffer r(bytes), z(bytes), p(bytes), v(bytes);
+  // work vectors persist on the operator between solves (no allocation per solve)
+  if (A.cg_work.size() != 4 || A.cg_work[0].bytes() != bytes) {
+    A.cg_work.clear();
+    for (int i = 0; i < 4; ++i) A.cg_work.emplace_back(bytes);
+  }
+  DeviceBuffer &r = A.cg_work[0], &z = A.cg_work[1], &p = A.cg_work[2], &v = A.cg_work[3];
   // r = b - A x
   operator_vmult(A, v.get(), x, s);
   PMG_CUDA(cudaMemcpyAsync(r.get(), b, bytes, cudaMemcpyDeviceToDevice, s));

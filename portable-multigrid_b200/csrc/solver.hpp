@@ -21,6 +21,13 @@ struct pmg_mg {
   std::vector<pmg_transfer *> transfers;
   std::vector<pmg_chebyshev *> smoothers;
   std::vector<pmg::DeviceBuffer> sol, def, t;
+  // The V-cycle below the finest level's input and output buffers is a fixed sequence of
+  // launches on fixed buffers: it is captured once into a CUDA graph and replayed.
+  cudaGraphExec_t graph = nullptr;
+  bool graph_enabled = true;
+  ~pmg_mg() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
 };
 
 namespace pmg {

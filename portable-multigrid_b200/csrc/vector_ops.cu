@@ -172,6 +172,7 @@ double finish(Workspace &w, int grid, int slot, cudaStream_t s) {
   } while (0)
 
 void fill_mod11(void *x, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   // mean of (i mod 11) over i < n, exactly
   const int64_t full = n / 11, rem = n % 11;
   const double sum = double(full) * 55.0 + double(rem * (rem - 1) / 2);
@@ -181,6 +182,7 @@ void fill_mod11(void *x, int dtype, int64_t n, cudaStream_t s) {
 }
 
 void convert(void *dst, int dt_dst, const void *src, int dt_src, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   if (dt_dst == dt_src) {
     PMG_CUDA(cudaMemcpyAsync(dst, src, dtype_size(dt_dst) * n, cudaMemcpyDeviceToDevice, s));
     return;
@@ -194,6 +196,7 @@ void convert(void *dst, int dt_dst, const void *src, int dt_src, int64_t n, cuda
 
 void cheb_init(void *dst, void *xo, const void *src, const void *invd, double scale, int dtype,
                int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   DISPATCH(dtype, cheb_init_k<T><<<grid_for(n), kBlock, 0, s>>>(static_cast<T *>(dst), static_cast<T *>(xo),
                                                                  static_cast<const T *>(src), static_cast<const T *>(invd), (T)scale, n));
   PMG_LAUNCH_CHECK();
@@ -201,6 +204,7 @@ void cheb_init(void *dst, void *xo, const void *src, const void *invd, double sc
 
 void cheb_first_step(void *dst, void *xo, const void *src, const void *Ax, const void *invd,
                      double scale, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   DISPATCH(dtype, cheb_first_step_k<T><<<grid_for(n), kBlock, 0, s>>>(
                       static_cast<T *>(dst), static_cast<T *>(xo), static_cast<const T *>(src),
                       static_cast<const T *>(Ax), static_cast<const T *>(invd), (T)scale, n));
@@ -209,6 +213,7 @@ void cheb_first_step(void *dst, void *xo, const void *src, const void *Ax, const
 
 void cheb_update(void *dst, void *xo, const void *src, const void *Ax, const void *invd, double f1,
                  double f2, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   DISPATCH(dtype, cheb_update_k<T><<<grid_for(n), kBlock, 0, s>>>(
                       static_cast<T *>(dst), static_cast<T *>(xo), static_cast<const T *>(src),
                       static_cast<const T *>(Ax), static_cast<const T *>(invd), (T)f1, (T)f2, n));
@@ -216,22 +221,26 @@ void cheb_update(void *dst, void *xo, const void *src, const void *Ax, const voi
 }
 
 void residual(void *t, const void *def, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   DISPATCH(dtype, residual_k<T><<<grid_for(n), kBlock, 0, s>>>(static_cast<T *>(t), static_cast<const T *>(def), n));
   PMG_LAUNCH_CHECK();
 }
 
 void jacobi(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   DISPATCH(dtype, jacobi_k<T><<<grid_for(n), kBlock, 0, s>>>(static_cast<T *>(z), static_cast<const T *>(invd),
                                                               static_cast<const T *>(r), n));
   PMG_LAUNCH_CHECK();
 }
 
 void xpay(void *p, const void *z, double beta, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
   DISPATCH(dtype, xpay_k<T><<<grid_for(n), kBlock, 0, s>>>(static_cast<T *>(p), static_cast<const T *>(z), (T)beta, n));
   PMG_LAUNCH_CHECK();
 }
 
 double dot(const void *a, const void *b, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_reduce", s);
   Workspace &w = workspace();
   const int grid = reduce_grid(n);
   DISPATCH(dtype, dot_partial_k<T><<<grid, kBlock, 0, s>>>(static_cast<const T *>(a), static_cast<const T *>(b), n,
@@ -242,6 +251,7 @@ double dot(const void *a, const void *b, int dtype, int64_t n, cudaStream_t s) {
 
 double cg_update(void *x, void *r, const void *p, const void *v, double alpha, int dtype, int64_t n,
                  cudaStream_t s) {
+  prof::Scope scope_("vector_reduce", s);
   Workspace &w = workspace();
   const int grid = reduce_grid(n);
   DISPATCH(dtype, cg_update_k<T><<<grid, kBlock, 0, s>>>(static_cast<T *>(x), static_cast<T *>(r),
@@ -252,6 +262,7 @@ double cg_update(void *x, void *r, const void *p, const void *v, double alpha, i
 }
 
 double jacobi_dot(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_reduce", s);
   Workspace &w = workspace();
   const int grid = reduce_grid(n);
   DISPATCH(dtype, jacobi_dot_k<T><<<grid, kBlock, 0, s>>>(static_cast<T *>(z), static_cast<const T *>(invd),
