@@ -87,20 +87,25 @@ pmg_status pmg_mesh_n_cells(const pmg_mesh *mesh, int64_t *n_cells);
 
 #define PMG_COEFF_NONE 0   /* -lap u                                                   */
 #define PMG_COEFF_KAPPA 1  /* kappa = 1 + 0.9 sin(2 pi x) sin(2 pi y) sin(2 pi z)      */
-#define PMG_COEFF_VALUES 2 /* caller-supplied values per quadrature point [C][nq^3]     */
+#define PMG_COEFF_VALUES 2 /* caller-supplied values per quadrature point [C][nq^3],
+                              cell order of the mesh, points lexicographic (x fastest) on
+                              the (degree+1)-point Gauss rule; NULL coeff_qp means 1      */
 
 #define PMG_OP_LAPLACE 0 /* continuous FE_Q Laplace (LaplaceOperatorBK3)                 */
 #define PMG_OP_DG_SIPG 1 /* discontinuous FE_DGQ symmetric interior penalty Laplace
                             (LaplaceOperatorDG, include/operators/portable_laplace_operator_dg.h);
                             axis-aligned undeformed boxes, no coefficient, Dirichlet data
                             enter weakly through the boundary faces                       */
+#define PMG_OP_MASS 2    /* continuous FE_Q mass matrix (phi_i, kappa phi_j) with identity
+                            rows on constrained DoFs; no counterpart in the reference (the
+                            adjoint misfit J = 1/2 (u - u_d)^T M (u - u_d))               */
 
 typedef struct {
   int32_t degree;          /* FE_Q / FE_DGQ degree 1..6 (OperatorDispatchFactory::max_degree) */
   int32_t dtype;           /* pmg_dtype: arithmetic and vector type                     */
   int32_t geometry;        /* PMG_GEOMETRY_*                                            */
   int32_t coeff_kind;      /* PMG_COEFF_*                                               */
-  const double *coeff_qp;  /* host array [C][(degree+1)^3] for PMG_COEFF_VALUES         */
+  const double *coeff_qp;  /* host array [C][(degree+1)^3] for PMG_COEFF_VALUES or NULL */
   int32_t device;          /* CUDA device ordinal                                       */
   int32_t kind;            /* PMG_OP_*                                                  */
   double penalty;          /* DG: sigma = penalty/h; <= 0 selects the reference's p(p+1)
@@ -154,6 +159,25 @@ pmg_status pmg_operator_assemble_rhs(const pmg_operator *op, int32_t f_kind, int
 pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host);
 pmg_status pmg_operator_copy_constrained(const pmg_operator *op, uint8_t *host);
 pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host);
+
+/* Coefficient fields and per-point forms (the adjoint path; no counterpart in the reference).
+ * set_coefficient: new PMG_COEFF_VALUES values [C][nq^3] (FP64; on_device selects a device
+ * or a host pointer), rebuilding G / the per-point factors / the mass weights on the stream.
+ * The inverse diagonal keeps describing the old values until pmg_operator_compute_diagonal. */
+pmg_status pmg_operator_set_coefficient(pmg_operator *op, const double *coeff_qp, int32_t on_device,
+                                        void *stream);
+/* dst's coefficient := src's coefficient field at dst's quadrature points: both on the same box,
+ * src refined at least as often; log(coefficient) is interpolated by the tensor Lagrange
+ * polynomial through src's Gauss points of the containing cell, so values stay positive. */
+pmg_status pmg_operator_interpolate_coefficient(pmg_operator *dst, pmg_operator *src, void *stream);
+/* Quadrature points of the operator's Gauss rule, device array xq[C][nq^3][3] (FP64). */
+pmg_status pmg_operator_quadrature_points(const pmg_operator *op, double *xq, void *stream);
+/* out[c][q] = alpha * grad u(x_q)^T kappa_q |det J| w_q J^{-1} J^{-T} grad v(x_q) in reference
+ * gradients, i.e. the integrand of a(u, v) per quadrature point (FP64 device array [C][nq^3];
+ * u and v have the operator's dtype, constrained entries read as 0).  For kappa = exp(m):
+ * d(u^T A v)/dm_q = out with alpha = 1. */
+pmg_status pmg_operator_qp_form(const pmg_operator *op, const void *u, const void *v, double alpha,
+                                double *out, void *stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Transfers: Portable::MGTransferBase<3,number>                                      */
@@ -243,6 +267,27 @@ typedef struct {
 pmg_status pmg_cg_solve(pmg_operator *A, pmg_mg *precond, void *x, const void *b,
                         double reduce, double abs_tol, int32_t max_iterations,
                         pmg_cg_info *info, void *stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Adjoint gradient of J(m) = 1/2 ||u(m) - u_d||^2_{L2} for -div(exp(m) grad u) = f     */
+/* (no counterpart in the reference)                                                  */
+/* ---------------------------------------------------------------------------------- */
+
+/* New coefficient values on a whole hierarchy: A (may be NULL) and the finest level take
+ * coeff_qp, every coarser level interpolates the one above it
+ * (pmg_operator_interpolate_coefficient); then every level's inverse diagonal and smoother
+ * eigenvalue estimate are recomputed.  Every level needs PMG_COEFF_VALUES.  Synchronises. */
+pmg_status pmg_mg_set_coefficient(pmg_mg *mg, pmg_operator *A, const double *coeff_qp,
+                                  int32_t on_device, void *stream);
+/* Given the forward solution u of A u = b (A FP64 with coefficient exp(m), M the FP64 mass
+ * operator of the same space): J = 1/2 (u-u_d)^T M (u-u_d), the adjoint solve
+ * A lambda = M (u - u_d) by CG with the multigrid preconditioner (NULL: Jacobi) from
+ * lambda = 0, and g_qp[c][q] = dJ/dm_q = -exp(m_q) grad lambda^T G grad u (FP64 device
+ * array [C][nq^3]).  info describes the adjoint solve.  Synchronises. */
+pmg_status pmg_adjoint_gradient(pmg_operator *A, const pmg_operator *M, pmg_mg *precond, const void *u,
+                                const void *u_d, void *lambda, double *g_qp, double *J, double reduce,
+                                double abs_tol, int32_t max_iterations, pmg_cg_info *info,
+                                void *stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Vector kernels on the path: LinearAlgebra::distributed::Vector operator* (the CG dot  */

@@ -370,3 +370,91 @@ def solve_dg(box, p, pseq, cheb=5, c_pen=None, reduce=1e-10, maxit=200, nq_rhs=N
     if rc != 0:
         raise ValueError("orc_solve_dg failed")
     return info, x
+
+
+# ---------------------------------------------------------------------------------------
+# Mass matrix, per-quadrature-point forms, coefficient fields (adjoint path)
+# ---------------------------------------------------------------------------------------
+def _declare_adjoint(L):
+    d, u32, u8 = np.float64, np.uint32, np.uint8
+    BP = C.POINTER(Box)
+    L.orc_mass_vmult.argtypes = [C.c_int, C.c_int64, C.c_int64, _p(u32), _p(d), _p(u8), _p(d), _p(d)]
+    L.orc_mass_diagonal.argtypes = [C.c_int, C.c_int64, C.c_int64, _p(u32), _p(d), _p(u8), _p(d)]
+    L.orc_qp_form.argtypes = [C.c_int, C.c_int64, _p(u32), _p(d), _p(d), _p(d), C.c_double, _p(d)]
+    L.orc_coef_interpolate.argtypes = [BP, C.c_int, _p(d), BP, C.c_int, _p(d)]
+
+
+def _adj_lib():
+    L = lib()
+    if not getattr(L, "_adj_declared", False):
+        _declare_adjoint(L)
+        L._adj_declared = True
+    return L
+
+
+def quadrature(box, p, nq=None):
+    """Gauss points xq[C, nq^3, 3] and |det J| w_q [C, nq^3] on every cell."""
+    nq = p + 1 if nq is None else nq
+    C_ = box.ncells()
+    xq = np.zeros(C_ * nq ** 3 * 3)
+    jxw = np.zeros(C_ * nq ** 3)
+    lib().orc_box_quadrature(C.byref(box), p, nq, xq, jxw)
+    return xq.reshape(C_, nq ** 3, 3), jxw.reshape(C_, nq ** 3)
+
+
+def mass_vmult(p, idx, jxw, constrained, src):
+    N = constrained.shape[0]
+    dst = np.zeros(N)
+    _adj_lib().orc_mass_vmult(p, idx.shape[0], N, np.ascontiguousarray(idx.reshape(-1)),
+                              np.ascontiguousarray(jxw.reshape(-1), dtype=np.float64), constrained,
+                              np.ascontiguousarray(src, dtype=np.float64), dst)
+    return dst
+
+
+def mass_diagonal(p, idx, jxw, constrained):
+    N = constrained.shape[0]
+    d = np.zeros(N)
+    _adj_lib().orc_mass_diagonal(p, idx.shape[0], N, np.ascontiguousarray(idx.reshape(-1)),
+                                 np.ascontiguousarray(jxw.reshape(-1), dtype=np.float64), constrained, d)
+    return d
+
+
+def qp_form(p, idx, G, u, v, alpha=1.0):
+    """out[C, nq^3] = alpha * grad_ref(u)^T G grad_ref(v) at every Gauss point."""
+    C_ = idx.shape[0]
+    out = np.zeros(C_ * (p + 1) ** 3)
+    _adj_lib().orc_qp_form(p, C_, np.ascontiguousarray(idx.reshape(-1)),
+                           np.ascontiguousarray(G.reshape(-1)), np.ascontiguousarray(u, dtype=np.float64),
+                           np.ascontiguousarray(v, dtype=np.float64), alpha, out)
+    return out.reshape(C_, (p + 1) ** 3)
+
+
+def coef_interpolate(src_box, nq_src, src, dst_box, nq_dst):
+    dst = np.zeros(dst_box.ncells() * nq_dst ** 3)
+    _adj_lib().orc_coef_interpolate(C.byref(src_box), nq_src,
+                                    np.ascontiguousarray(src.reshape(-1), dtype=np.float64),
+                                    C.byref(dst_box), nq_dst, dst)
+    return dst.reshape(dst_box.ncells(), nq_dst ** 3)
+
+
+def cg(apply, b, diag, tol, max_iterations=5000):
+    """Jacobi-preconditioned CG from x = 0 to ||r|| <= tol ||b|| (numpy; small test cases)."""
+    x = np.zeros_like(b)
+    r = b.copy()
+    r0 = float(np.sqrt(r @ r))
+    if r0 == 0.0:
+        return x
+    z = r / diag
+    p = z.copy()
+    rz = r @ z
+    for _ in range(max_iterations):
+        Ap = apply(p)
+        a = rz / (p @ Ap)
+        x += a * p
+        r -= a * Ap
+        if np.sqrt(r @ r) <= tol * r0:
+            return x
+        z = r / diag
+        rz, rz_old = r @ z, rz
+        p = z + (rz / rz_old) * p
+    raise RuntimeError("CG did not converge")

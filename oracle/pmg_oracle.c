@@ -1879,3 +1879,159 @@ int orc_solve_dg(const orc_box *box, int p, const int32_t *pseq, int n_pseq, int
   free(mg.transfers);
   return 0;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* 8. Mass matrix, per-quadrature-point forms and coefficient fields (adjoint path)       */
+/* ------------------------------------------------------------------------------------ */
+/* Not in the reference: the adjoint gradient of J(m) = 1/2 ||u(m) - u_d||^2_{L2} for
+ * -div(exp(m) grad u) = f needs the FE mass matrix (values-only sum factorization), the
+ * per-quadrature-point density of the Laplace form, and coefficient fields carried across
+ * the multigrid levels.  Restated here from the definitions; the pins are the round trips
+ * in tests/test_oracle_adjoint.py (mass matrix against exact integrals, the adjoint
+ * gradient against central finite differences). */
+
+/* dst = sum_c P_c^T S^T diag(jxw_c) S P_c src with identity rows on constrained DoFs;
+ * jxw[C][nq^3] holds |det J| w_q (times any weight) at the (p+1)-point Gauss rule. */
+void orc_mass_vmult(int p, int64_t C, int64_t N, const uint32_t *idx, const double *jxw,
+                    const uint8_t *constrained, const double *src, double *dst)
+{
+  const int n = p + 1, n3 = n * n * n;
+  double S[64];
+  orc_shape_tables(p, n, S, NULL, NULL, NULL);
+  double *buf = (double *)malloc(sizeof(double) * 5 * n3);
+  double *u = buf, *v = buf + n3, *out = buf + 2 * n3, *t1 = buf + 3 * n3, *t2 = buf + 4 * n3;
+  for (int64_t i = 0; i < N; ++i) dst[i] = 0.0;
+  for (int64_t c = 0; c < C; ++c) {
+    const uint32_t *ci = idx + c * n3;
+    for (int l = 0; l < n3; ++l) u[l] = (ci[l] == ORC_INVALID) ? 0.0 : src[ci[l]];
+    tensor_apply(n, n, S, 0, u, v, t1, t2);
+    for (int q = 0; q < n3; ++q) v[q] *= jxw[c * n3 + q];
+    tensor_apply(n, n, S, 1, v, out, t1, t2);
+    for (int l = 0; l < n3; ++l)
+      if (ci[l] != ORC_INVALID) dst[ci[l]] += out[l];
+  }
+  for (int64_t i = 0; i < N; ++i)
+    if (constrained[i]) dst[i] = src[i];
+  free(buf);
+}
+
+/* diag(M)_i = sum_c sum_q phi_i(x_q)^2 jxw_c(q); 1 on constrained rows. */
+void orc_mass_diagonal(int p, int64_t C, int64_t N, const uint32_t *idx, const double *jxw,
+                       const uint8_t *constrained, double *diag)
+{
+  const int n = p + 1, n3 = n * n * n;
+  double S[64];
+  orc_shape_tables(p, n, S, NULL, NULL, NULL);
+  for (int64_t i = 0; i < N; ++i) diag[i] = 0.0;
+  for (int64_t c = 0; c < C; ++c)
+    for (int l = 0; l < n3; ++l) {
+      const uint32_t d = idx[c * n3 + l];
+      if (d == ORC_INVALID) continue;
+      const int i = l % n, j = (l / n) % n, k = l / (n * n);
+      double s = 0;
+      for (int q2 = 0; q2 < n; ++q2)
+        for (int q1 = 0; q1 < n; ++q1)
+          for (int q0 = 0; q0 < n; ++q0) {
+            const double phi = S[i * n + q0] * S[j * n + q1] * S[k * n + q2];
+            s += phi * phi * jxw[c * n3 + (q2 * n + q1) * n + q0];
+          }
+      diag[d] += s;
+    }
+  for (int64_t i = 0; i < N; ++i)
+    if (constrained[i]) diag[i] = 1.0;
+}
+
+/* out[c][q] = alpha * grad_ref(u)(x_q)^T G_c(q) grad_ref(v)(x_q), with G[C][6][nq^3] as
+ * orc_box_G stores it (coefficient included): the integrand of a(u, v) = sum_c sum_q out.
+ * Reference gradients are taken straight from the nodal values with the derivative table
+ * SD (constrained entries of idx read as 0). */
+void orc_qp_form(int p, int64_t C, const uint32_t *idx, const double *G, const double *u,
+                 const double *v, double alpha, double *out)
+{
+  const int n = p + 1, n3 = n * n * n;
+  double S[64], SD[64];
+  orc_shape_tables(p, n, S, SD, NULL, NULL);
+#pragma omp parallel
+  {
+    double *cu = (double *)malloc(sizeof(double) * 2 * n3);
+    double *cv = cu + n3;
+#pragma omp for schedule(static)
+    for (int64_t c = 0; c < C; ++c) {
+      const uint32_t *ci = idx + c * n3;
+      for (int l = 0; l < n3; ++l) {
+        cu[l] = (ci[l] == ORC_INVALID) ? 0.0 : u[ci[l]];
+        cv[l] = (ci[l] == ORC_INVALID) ? 0.0 : v[ci[l]];
+      }
+      for (int q2 = 0; q2 < n; ++q2)
+        for (int q1 = 0; q1 < n; ++q1)
+          for (int q0 = 0; q0 < n; ++q0) {
+            double gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0};
+            for (int k = 0; k < n; ++k)
+              for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                  const double b0 = SD[i * n + q0] * S[j * n + q1] * S[k * n + q2];
+                  const double b1 = S[i * n + q0] * SD[j * n + q1] * S[k * n + q2];
+                  const double b2 = S[i * n + q0] * S[j * n + q1] * SD[k * n + q2];
+                  const int l = (k * n + j) * n + i;
+                  gu[0] += b0 * cu[l]; gu[1] += b1 * cu[l]; gu[2] += b2 * cu[l];
+                  gv[0] += b0 * cv[l]; gv[1] += b1 * cv[l]; gv[2] += b2 * cv[l];
+                }
+            const int q = (q2 * n + q1) * n + q0;
+            const double *g = G + c * 6 * n3;
+            const double g00 = g[0 * n3 + q], g01 = g[1 * n3 + q], g02 = g[2 * n3 + q];
+            const double g11 = g[3 * n3 + q], g12 = g[4 * n3 + q], g22 = g[5 * n3 + q];
+            const double Gv0 = g00 * gv[0] + g01 * gv[1] + g02 * gv[2];
+            const double Gv1 = g01 * gv[0] + g11 * gv[1] + g12 * gv[2];
+            const double Gv2 = g02 * gv[0] + g12 * gv[1] + g22 * gv[2];
+            out[c * n3 + q] = alpha * (gu[0] * Gv0 + gu[1] * Gv1 + gu[2] * Gv2);
+          }
+    }
+    free(cu);
+  }
+}
+
+/* A positive field given at the nq_src-point Gauss points of every cell of src_box, carried
+ * to the nq_dst-point Gauss points of dst_box (the same box, equally or less refined): the
+ * logarithm is interpolated by the tensor-product Lagrange polynomial through the source
+ * cell's Gauss points at the target point, then exponentiated (so the result stays
+ * positive).  A target point on a face of two source cells takes the upper cell. */
+void orc_coef_interpolate(const orc_box *src_box, int nq_src, const double *src,
+                          const orc_box *dst_box, int nq_dst, double *dst)
+{
+  int64_t ns[3], nd[3];
+  box_ncells(src_box, ns);
+  box_ncells(dst_box, nd);
+  const int64_t Cs = ns[0] * ns[1] * ns[2], Cd = nd[0] * nd[1] * nd[2];
+  int32_t *cs = (int32_t *)malloc(sizeof(int32_t) * 3 * Cs);
+  int32_t *cd = (int32_t *)malloc(sizeof(int32_t) * 3 * Cd);
+  orc_box_cell_coords(src_box, cs, cs + Cs, cs + 2 * Cs);
+  orc_box_cell_coords(dst_box, cd, cd + Cd, cd + 2 * Cd);
+  int64_t *lut = box_cell_lookup(src_box, cs);
+  ld xs[32], ws[32], xd[32], wd[32];
+  gauss_ld(nq_src, xs, ws);
+  gauss_ld(nq_dst, xd, wd);
+  const int64_t r = ns[0] / nd[0];
+  const int nqs3 = nq_src * nq_src * nq_src, nqd3 = nq_dst * nq_dst * nq_dst;
+  for (int64_t c = 0; c < Cd; ++c)
+    for (int q = 0; q < nqd3; ++q) {
+      const int qd[3] = {q % nq_dst, (q / nq_dst) % nq_dst, q / (nq_dst * nq_dst)};
+      int64_t sc[3];
+      double L[3][32];
+      for (int d = 0; d < 3; ++d) {
+        const double X = ((double)cd[d * Cd + c] + (double)xd[qd[d]]) * (double)r;
+        int64_t s = (int64_t)floor(X);
+        if (s > ns[d] - 1) s = ns[d] - 1;
+        sc[d] = s;
+        const ld xi = (ld)(X - (double)s);
+        for (int a = 0; a < nq_src; ++a) L[d][a] = (double)lagrange(nq_src, xs, a, xi);
+      }
+      const int64_t cell = lut[(sc[2] * ns[1] + sc[1]) * ns[0] + sc[0]];
+      double s = 0;
+      for (int k = 0; k < nq_src; ++k)
+        for (int j = 0; j < nq_src; ++j)
+          for (int i = 0; i < nq_src; ++i)
+            s += L[0][i] * L[1][j] * L[2][k] * log(src[cell * nqs3 + (k * nq_src + j) * nq_src + i]);
+      dst[c * nqd3 + q] = exp(s);
+    }
+  free(cs); free(cd); free(lut);
+}

@@ -266,6 +266,43 @@ pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host) {
   });
 }
 
+pmg_status pmg_operator_set_coefficient(pmg_operator *op, const double *coeff_qp, int32_t on_device,
+                                        void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(coeff_qp);
+    PMG_CUDA(cudaSetDevice(op->device));
+    pmg::operator_set_coefficient(*op, coeff_qp, on_device != 0, as_stream(stream));
+  });
+}
+
+pmg_status pmg_operator_interpolate_coefficient(pmg_operator *dst, pmg_operator *src, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(dst);
+    NEED(src);
+    pmg::operator_interpolate_coefficient(*dst, *src, as_stream(stream));
+  });
+}
+
+pmg_status pmg_operator_quadrature_points(const pmg_operator *op, double *xq, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(xq);
+    pmg::operator_quadrature_points(*op, xq, as_stream(stream));
+  });
+}
+
+pmg_status pmg_operator_qp_form(const pmg_operator *op, const void *u, const void *v, double alpha,
+                                double *out, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(u);
+    NEED(v);
+    NEED(out);
+    pmg::operator_qp_form(*op, u, v, alpha, out, as_stream(stream));
+  });
+}
+
 // ---------------------------------------------------------------------------------------
 pmg_status pmg_transfer_create(const pmg_operator *coarse, const pmg_operator *fine,
                                pmg_transfer **transfer) {
@@ -412,6 +449,40 @@ pmg_status pmg_cg_solve(pmg_operator *A, pmg_mg *precond, void *x, const void *b
   if (info) *info = local;
   if (st == PMG_OK && !local.converged) {
     g_last_error = "pmg_cg_solve: iteration limit reached";
+    return PMG_ENOCONV;
+  }
+  return st;
+}
+
+pmg_status pmg_mg_set_coefficient(pmg_mg *mg, pmg_operator *A, const double *coeff_qp, int32_t on_device,
+                                  void *stream) {
+  return guarded(__func__, [&] {
+    NEED(mg);
+    NEED(coeff_qp);
+    PMG_CUDA(cudaSetDevice(mg->levels.back()->device));
+    pmg::mg_set_coefficient(*mg, A, coeff_qp, on_device != 0, as_stream(stream));
+    PMG_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  });
+}
+
+pmg_status pmg_adjoint_gradient(pmg_operator *A, const pmg_operator *M, pmg_mg *precond, const void *u,
+                                const void *u_d, void *lambda, double *g_qp, double *J, double reduce,
+                                double abs_tol, int32_t max_iterations, pmg_cg_info *info,
+                                void *stream) {
+  pmg_cg_info local{};
+  double j = 0.0;
+  pmg_status st = guarded(__func__, [&] {
+    NEED(A);
+    NEED(M);
+    NEED(J);
+    pmg::adjoint_gradient(*A, *M, precond, u, u_d, lambda, g_qp, j, reduce, abs_tol, max_iterations, local,
+                          as_stream(stream));
+    PMG_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  });
+  if (info) *info = local;
+  if (J) *J = j;
+  if (st == PMG_OK && !local.converged) {
+    g_last_error = "pmg_adjoint_gradient: iteration limit reached in the adjoint solve";
     return PMG_ENOCONV;
   }
   return st;

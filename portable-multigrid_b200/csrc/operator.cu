@@ -5,6 +5,7 @@
 
 #include "laplace_kernels.cuh"
 #include "dg.hpp"
+#include "fields.hpp"
 #include "pmg_internal.hpp"
 
 namespace pmg {
@@ -46,7 +47,9 @@ __device__ __forceinline__ double coefficient(int kind, const double x[3]) {
 // point the Jacobian of the isoparametric Q_p map, its inverse and determinant.
 // mode 0: write G = coef * |det J| w_q J^{-1} J^{-T} into the slab layout (full geometry);
 // mode 1: write coef * (per-point factor) into the affine coefficient layout;
-// mode 2: right-hand side, b_i += sum_q phi_i(x_q) f(x_q) |det J| w_q (atomic).
+// mode 2: right-hand side, b_i += sum_q phi_i(x_q) f(x_q) |det J| w_q (atomic);
+// mode 3: the quadrature points, out[cell][q][3];
+// mode 4: coef * |det J| w_q into the affine coefficient layout (mass-matrix weights).
 template <typename T>
 __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restrict__ cell_xyz,
                                      int64_t n_cells, int mode, int coeff_kind,
@@ -123,6 +126,10 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
           }
       } else if (mode == 1) {
         out[(grp * (g.N * g.N) + m_row) * g.lanes + lane] = (T)kap;
+      } else if (mode == 3) {
+        for (int d = 0; d < 3; ++d) out[(c * nq3 + q) * 3 + d] = (T)xq[d];
+      } else if (mode == 4) {
+        out[(grp * (g.N * g.N) + m_row) * g.lanes + lane] = (T)(fabs(det) * wq * kap);
       } else {
         double f = 1.0;
         if (f_kind == 1) f = 3.0 * M_PI * M_PI * sin(M_PI * xq[0]) * sin(M_PI * xq[1]) * sin(M_PI * xq[2]);
@@ -240,24 +247,14 @@ SlabLaunch slab_launch(const pmg_operator &op, const Tables1D &t, cudaStream_t s
   return L;
 }
 
-const Tables1D &cached_tables(int degree) {
-  static Tables1D tabs[kMaxDegree + 1];
-  static bool ready[kMaxDegree + 1] = {false};
-  if (!ready[degree]) {
-    tabs[degree] = make_tables(degree, degree + 1);
-    ready[degree] = true;
-  }
-  return tabs[degree];
-}
-
 } // namespace
 
 void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_params &prm) {
   PMG_REQUIRE(prm.degree >= 1 && prm.degree <= kMaxDegree, "degree must be in [1,6]");
   PMG_REQUIRE(prm.dtype == PMG_F64 || prm.dtype == PMG_F32, "dtype must be PMG_F64 or PMG_F32");
   PMG_REQUIRE(prm.coeff_kind >= 0 && prm.coeff_kind <= 2, "bad coeff_kind");
-  PMG_REQUIRE(prm.coeff_kind != PMG_COEFF_VALUES || prm.coeff_qp, "coeff_qp is required");
-  PMG_REQUIRE(prm.kind == PMG_OP_LAPLACE || prm.kind == PMG_OP_DG_SIPG, "bad operator kind");
+  PMG_REQUIRE(prm.kind == PMG_OP_LAPLACE || prm.kind == PMG_OP_DG_SIPG || prm.kind == PMG_OP_MASS,
+              "bad operator kind");
   if (prm.kind == PMG_OP_DG_SIPG) {
     PMG_REQUIRE(mesh.m.box.deform == 0, "the DG operator needs an undeformed (axis-aligned) box");
     PMG_REQUIRE(prm.coeff_kind == PMG_COEFF_NONE, "the DG operator has no coefficient");
@@ -328,25 +325,62 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   }
   // geometry (compute_G_tensors, bk3.h:456-515), computed on the device
   const size_t s = dtype_size(op.dtype);
-  DeviceBuffer xyz = upload(mesh.m.cell_xyz);
-  DeviceBuffer coef_in;
+  op.cell_xyz = upload(mesh.m.cell_xyz);
+  const DeviceBuffer &xyz = op.cell_xyz;
+  // coefficient values (PMG_COEFF_VALUES): kept on the device in FP64 so that coarser levels
+  // can interpolate them; no array given means the constant 1
   if (prm.coeff_kind == PMG_COEFF_VALUES) {
-    coef_in.allocate(sizeof(double) * op.n_cells * N3);
-    PMG_CUDA(cudaMemcpy(coef_in.get(), prm.coeff_qp, sizeof(double) * op.n_cells * N3,
-                        cudaMemcpyHostToDevice));
+    op.coef_qp.allocate(sizeof(double) * std::max<int64_t>(1, op.n_cells * N3));
+    if (prm.coeff_qp) {
+      PMG_CUDA(cudaMemcpy(op.coef_qp.get(), prm.coeff_qp, sizeof(double) * op.n_cells * N3,
+                          cudaMemcpyHostToDevice));
+    } else {
+      std::vector<double> ones((size_t)op.n_cells * N3, 1.0);
+      if (!ones.empty())
+        PMG_CUDA(cudaMemcpy(op.coef_qp.get(), ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
   }
+  const double *coef_in = op.coef_qp.as<double>();
   const GeoParams gp = make_geo_params(op, op.nq);
   const int sms = num_sms(op.device);
-  const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)sms * 16);
-  if (geometry == PMG_GEOMETRY_FULL) {
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(op.n_cells, (int64_t)sms * 16));
+  if (op.kind == PMG_OP_MASS) {
+    // mass matrix: the volume of an affine cell without a coefficient, else |det J| w_q
+    // (times the coefficient) per quadrature point
+    op.mass_geom = (geometry == PMG_GEOMETRY_AFFINE && prm.coeff_kind == PMG_COEFF_NONE) ? 1 : 0;
+    op.has_coeff_values = false;
+    if (op.mass_geom == 1) {
+      double h[3];
+      for (int d = 0; d < 3; ++d) h[d] = (mesh.m.box.hi[d] - mesh.m.box.lo[d]) / double(mesh.m.n[d]);
+      const int64_t n_slots = op.n_groups * op.cpw;
+      std::vector<double> v(n_slots * 8, 0.0);
+      for (int64_t c = 0; c < op.n_cells; ++c) v[8 * c + 6] = h[0] * h[1] * h[2];
+      if (op.dtype == PMG_F64) {
+        op.geo = upload(v);
+      } else {
+        std::vector<float> f(v.begin(), v.end());
+        op.geo = upload(f);
+      }
+    } else {
+      op.coef.allocate(s * op.n_groups * N2 * op.lanes);
+      PMG_CUDA(cudaMemset(op.coef.get(), 0, op.coef.bytes()));
+      if (op.dtype == PMG_F64)
+        cell_geometry_kernel<double><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 4, prm.coeff_kind,
+                                                    coef_in, op.coef.as<double>(), nullptr, 0);
+      else
+        cell_geometry_kernel<float><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 4, prm.coeff_kind,
+                                                   coef_in, op.coef.as<float>(), nullptr, 0);
+      PMG_LAUNCH_CHECK();
+    }
+  } else if (geometry == PMG_GEOMETRY_FULL) {
     op.geo.allocate(s * op.n_groups * N2 * 6 * op.lanes);
     PMG_CUDA(cudaMemset(op.geo.get(), 0, op.geo.bytes()));
     if (op.dtype == PMG_F64)
       cell_geometry_kernel<double><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 0, prm.coeff_kind,
-                                                  coef_in.as<double>(), op.geo.as<double>(), nullptr, 0);
+                                                  coef_in, op.geo.as<double>(), nullptr, 0);
     else
       cell_geometry_kernel<float><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 0, prm.coeff_kind,
-                                                 coef_in.as<double>(), op.geo.as<float>(), nullptr, 0);
+                                                 coef_in, op.geo.as<float>(), nullptr, 0);
     PMG_LAUNCH_CHECK();
   } else {
     // affine: C = |det J| J^{-1} J^{-T} / (w-independent) per cell; axis-aligned boxes give
@@ -358,6 +392,7 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
     c8[0] = vol / (h[0] * h[0]);
     c8[3] = vol / (h[1] * h[1]);
     c8[5] = vol / (h[2] * h[2]);
+    c8[6] = vol;
     const int64_t n_slots = op.n_groups * op.cpw;
     if (op.dtype == PMG_F64) {
       std::vector<double> v(n_slots * 8, 0.0);
@@ -374,10 +409,10 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
       PMG_CUDA(cudaMemset(op.coef.get(), 0, op.coef.bytes()));
       if (op.dtype == PMG_F64)
         cell_geometry_kernel<double><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 1, prm.coeff_kind,
-                                                    coef_in.as<double>(), op.coef.as<double>(), nullptr, 0);
+                                                    coef_in, op.coef.as<double>(), nullptr, 0);
       else
         cell_geometry_kernel<float><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 1, prm.coeff_kind,
-                                                   coef_in.as<double>(), op.coef.as<float>(), nullptr, 0);
+                                                   coef_in, op.coef.as<float>(), nullptr, 0);
       PMG_LAUNCH_CHECK();
     }
   }
@@ -398,7 +433,10 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
   PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");
   const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
   PMG_CUDA(cudaMemsetAsync(dst, 0, bytes, s)); // dst = 0 (bk3.h:134)
-  if (compute && op.n_cells > 0) {
+  if (compute && op.n_cells > 0 && op.kind == PMG_OP_MASS) {
+    prof::Scope scope("vmult_mass", s);
+    mass_vmult_cells(op, src, dst, s);
+  } else if (compute && op.n_cells > 0) {
     SlabLaunch L = slab_launch(op, cached_tables(op.degree), s);
     L.src = src;
     L.dst = dst;
@@ -432,7 +470,10 @@ void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s) {
   const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
   if (op.inv_diag.bytes() != bytes) op.inv_diag.allocate(bytes);
   PMG_CUDA(cudaMemsetAsync(op.inv_diag.get(), 0, bytes, s));
-  if (op.n_cells > 0) {
+  if (op.n_cells > 0 && op.kind == PMG_OP_MASS) {
+    prof::Scope scope("diag_mass", s);
+    mass_diagonal_cells(op, op.inv_diag.get(), s);
+  } else if (op.n_cells > 0) {
     SlabLaunch L = slab_launch(op, cached_tables(op.degree), s);
     L.dst = op.inv_diag.get();
     L.resident_warps = op.warps_diag;
@@ -463,7 +504,7 @@ void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, 
   PMG_REQUIRE(nq >= 1 && nq <= kMaxNq, "nq must be in [1,8]");
   PMG_CUDA(cudaSetDevice(op.device));
   PMG_CUDA(cudaMemsetAsync(b, 0, dtype_size(op.dtype) * op.n_dofs, s));
-  DeviceBuffer xyz = upload(op.mesh.cell_xyz);
+  const DeviceBuffer &xyz = op.cell_xyz;
   const GeoParams gp = make_geo_params(op, nq);
   const int grid = (int)std::min<int64_t>(std::max<int64_t>(op.n_cells, 1), (int64_t)num_sms(op.device) * 16);
   if (op.dtype == PMG_F64)
@@ -473,7 +514,6 @@ void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, 
     cell_geometry_kernel<float><<<grid, 128, 0, s>>>(gp, xyz.as<int32_t>(), op.n_cells, 2, 0, nullptr,
                                                      static_cast<float *>(b), op.idx.as<uint32_t>(), f_kind);
   PMG_LAUNCH_CHECK();
-  PMG_CUDA(cudaStreamSynchronize(s)); // xyz is freed on return
   if (op.dg && f_kind == 2) dg_add_boundary_rhs(*op.dg, op.mesh, op.degree, nq, op.dtype, b, s);
 }
 
@@ -504,9 +544,85 @@ int64_t operator_bytes(const pmg_operator &op) {
   const int64_t s = (int64_t)dtype_size(op.dtype);
   const int64_t nm3 = (int64_t)op.nm * op.nm * op.nm, nq3 = (int64_t)op.nq * op.nq * op.nq;
   int64_t g = 0;
-  if (op.geometry == PMG_GEOMETRY_FULL) g = 6 * nq3;
+  if (op.kind == PMG_OP_MASS) g = op.mass_geom == 1 ? 1 : nq3;
+  else if (op.geometry == PMG_GEOMETRY_FULL) g = 6 * nq3;
   else g = 6 + (op.has_coeff_values ? nq3 : 0);
   return 2 * s * op.n_dofs + 4 * nm3 * op.n_cells + g * s * op.n_cells;
+}
+
+// Replace the coefficient values (PMG_COEFF_VALUES) and rebuild what depends on them: G
+// (full geometry), the per-point factors (affine), or the mass weights.  The inverse
+// diagonal is not recomputed here.
+void operator_set_coefficient(pmg_operator &op, const double *values, bool on_device, cudaStream_t s) {
+  PMG_REQUIRE(op.coeff_kind == PMG_COEFF_VALUES, "the operator was not created with PMG_COEFF_VALUES");
+  PMG_REQUIRE(values, "null coefficient array");
+  PMG_CUDA(cudaSetDevice(op.device));
+  const int64_t n = op.n_cells * op.nq * op.nq * op.nq;
+  if (values != op.coef_qp.as<double>())
+    PMG_CUDA(cudaMemcpyAsync(op.coef_qp.get(), values, sizeof(double) * n,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  if (op.n_cells == 0) return;
+  const GeoParams gp = make_geo_params(op, op.nq);
+  const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)op.sms * 16);
+  int mode = 0;
+  void *out = nullptr;
+  if (op.kind == PMG_OP_MASS) {
+    mode = 4;
+    out = op.coef.get();
+  } else if (op.geometry == PMG_GEOMETRY_FULL) {
+    mode = 0;
+    out = op.geo.get();
+  } else {
+    mode = 1;
+    out = op.coef.get();
+  }
+  if (op.dtype == PMG_F64)
+    cell_geometry_kernel<double><<<grid, 128, 0, s>>>(gp, op.cell_xyz.as<int32_t>(), op.n_cells, mode, op.coeff_kind,
+                                                      op.coef_qp.as<double>(), static_cast<double *>(out), nullptr, 0);
+  else
+    cell_geometry_kernel<float><<<grid, 128, 0, s>>>(gp, op.cell_xyz.as<int32_t>(), op.n_cells, mode, op.coeff_kind,
+                                                     op.coef_qp.as<double>(), static_cast<float *>(out), nullptr, 0);
+  PMG_LAUNCH_CHECK();
+}
+
+// dst's coefficient := src's coefficient field at dst's quadrature points (nested boxes).
+void operator_interpolate_coefficient(pmg_operator &dst, pmg_operator &src, cudaStream_t s) {
+  PMG_REQUIRE(dst.coeff_kind == PMG_COEFF_VALUES && src.coeff_kind == PMG_COEFF_VALUES,
+              "both operators need PMG_COEFF_VALUES");
+  PMG_REQUIRE(dst.device == src.device, "operators on different devices");
+  PMG_CUDA(cudaSetDevice(dst.device));
+  if (!src.cell_lut.get()) {
+    std::vector<int32_t> lut((size_t)src.n_cells);
+    for (int64_t c = 0; c < src.n_cells; ++c) {
+      const int32_t *x = &src.mesh.cell_xyz[3 * c];
+      lut[((int64_t)x[2] * src.mesh.n[1] + x[1]) * src.mesh.n[0] + x[0]] = (int32_t)c;
+    }
+    src.cell_lut = upload(lut);
+  }
+  if (dst.n_cells == 0) return;
+  coefficient_interpolate(src, dst, dst.coef_qp.as<double>(), s);
+  operator_set_coefficient(dst, dst.coef_qp.as<double>(), true, s);
+}
+
+void operator_quadrature_points(const pmg_operator &op, double *xq, cudaStream_t s) {
+  PMG_REQUIRE(xq, "null output");
+  PMG_CUDA(cudaSetDevice(op.device));
+  if (op.n_cells == 0) return;
+  const GeoParams gp = make_geo_params(op, op.nq);
+  const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)op.sms * 16);
+  cell_geometry_kernel<double><<<grid, 128, 0, s>>>(gp, op.cell_xyz.as<int32_t>(), op.n_cells, 3, 0, nullptr, xq,
+                                                    nullptr, 0);
+  PMG_LAUNCH_CHECK();
+}
+
+void operator_qp_form(const pmg_operator &op, const void *u, const void *v, double alpha, double *out,
+                      cudaStream_t s) {
+  PMG_REQUIRE(op.kind == PMG_OP_LAPLACE, "the per-point form is defined for the continuous Laplace operator");
+  PMG_REQUIRE(u && v && out, "null vector");
+  PMG_CUDA(cudaSetDevice(op.device));
+  if (op.n_cells == 0) return;
+  prof::Scope scope("qp_form", s);
+  qp_form_cells(op, u, v, alpha, out, s);
 }
 
 } // namespace pmg

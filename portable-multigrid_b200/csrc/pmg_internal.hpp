@@ -176,7 +176,7 @@ struct DGHost;
 
 struct pmg_operator {
   int device = 0;
-  int kind = PMG_OP_LAPLACE;        // PMG_OP_LAPLACE or PMG_OP_DG_SIPG
+  int kind = PMG_OP_LAPLACE;        // PMG_OP_LAPLACE, PMG_OP_DG_SIPG or PMG_OP_MASS
   std::shared_ptr<pmg::DGHost> dg;  // face data of a DG operator
   int degree = 1, nm = 2, nq = 2;
   int dtype = PMG_F64;
@@ -190,7 +190,12 @@ struct pmg_operator {
   pmg::Numbering num;               // host copy (plain indices, constrained, lattice)
   pmg::DeviceBuffer idx;            // permuted [group][nm^2][lanes] uint32
   pmg::DeviceBuffer geo;            // FULL: [group][nq^2][6][lanes]; AFFINE: [C][8]
-  pmg::DeviceBuffer coef;           // AFFINE with coefficient: [group][nq^2][lanes]
+  pmg::DeviceBuffer coef;           // AFFINE with coefficient: [group][nq^2][lanes];
+                                    // MASS with mass_geom 0: |det J| w_q (times coefficient)
+  int mass_geom = 0;                // MASS: 1 = affine volume in geo[cell][6], 0 = coef
+  pmg::DeviceBuffer coef_qp;        // PMG_COEFF_VALUES: the values [C][nq^3] FP64
+  pmg::DeviceBuffer cell_xyz;       // [C][3] int32 lattice coordinates of the cells
+  pmg::DeviceBuffer cell_lut;       // lattice (x fastest) -> cell, int32 (built on demand)
   pmg::DeviceBuffer constrained_list; // uint32 [n_constrained]
   int64_t n_constrained = 0;
   pmg::DeviceBuffer inv_diag;       // [N] dtype
@@ -199,6 +204,7 @@ struct pmg_operator {
   int64_t warps_vmult_ring = 0;             // ... of the geometry-ring vmult variant
   int sms = 0;                              // SM count of the device
   std::vector<pmg::DeviceBuffer> cg_work;   // CG work vectors kept between solves
+  std::vector<pmg::DeviceBuffer> adj_work;  // adjoint-gradient work vectors
   pmg::DeviceBuffer err_flag;               // set by bounded device waits that give up
 };
 
@@ -211,4 +217,9 @@ void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s);
 void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, cudaStream_t s);
 void operator_copy_geometry(const pmg_operator &op, double *host);
 int64_t operator_bytes(const pmg_operator &op);
+void operator_set_coefficient(pmg_operator &op, const double *values, bool on_device, cudaStream_t s);
+void operator_interpolate_coefficient(pmg_operator &dst, pmg_operator &src, cudaStream_t s);
+void operator_quadrature_points(const pmg_operator &op, double *xq, cudaStream_t s);
+void operator_qp_form(const pmg_operator &op, const void *u, const void *v, double alpha, double *out,
+                      cudaStream_t s);
 } // namespace pmg

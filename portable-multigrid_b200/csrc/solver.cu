@@ -55,6 +55,7 @@ void chebyshev_setup(pmg_chebyshev &c, pmg_operator &op, const pmg_chebyshev_par
   PMG_REQUIRE(prm.eig_cg_n_iterations >= 0, "eig_cg_n_iterations must be >= 0");
   c.op = &op;
   c.degree = prm.degree;
+  c.requested_degree = prm.degree;
   c.range = prm.smoothing_range;
   c.eig_its = prm.eig_cg_n_iterations;
   const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
@@ -118,7 +119,7 @@ void chebyshev_estimate(pmg_chebyshev &c, cudaStream_t s) {
     c.max_ev = 1.2 * tridiag_extreme(diag, offd, true);
   }
   const double alpha_ev = c.range > 1.0 ? c.max_ev / c.range : std::min(0.9 * c.max_ev, c.min_ev);
-  if (c.degree <= 0) {
+  if (c.requested_degree <= 0) {
     const double actual = c.max_ev / alpha_ev;
     const double sigma = (1.0 - std::sqrt(1.0 / actual)) / (1.0 + std::sqrt(1.0 / actual));
     const double eps = c.range;
@@ -127,6 +128,7 @@ void chebyshev_estimate(pmg_chebyshev &c, cudaStream_t s) {
   c.delta = (c.max_ev - alpha_ev) * 0.5;
   c.theta = (c.max_ev + alpha_ev) * 0.5;
   c.estimated = true;
+  ++c.generation;
   PMG_CUDA(cudaStreamSynchronize(s)); // the work vectors are freed on return
 }
 
@@ -243,6 +245,8 @@ void mg_capture(pmg_mg &mg) {
     ok = (cudaStreamEndCapture(cs, &g) == cudaSuccess) && ok;
   }
   if (ok) ok = cudaGraphInstantiate(&mg.graph, g, 0) == cudaSuccess;
+  mg.graph_generations.clear();
+  for (auto *sm : mg.smoothers) mg.graph_generations.push_back(sm->generation);
   if (g) cudaGraphDestroy(g);
   cudaStreamDestroy(cs);
   if (!ok) {
@@ -259,6 +263,17 @@ void mg_vmult(pmg_mg &mg, void *dst, const void *src, int vec_dtype, cudaStream_
   const pmg_operator &top = *mg.levels[L];
   for (auto *sm : mg.smoothers)
     if (!sm->estimated) chebyshev_estimate(*sm, s);
+  // a graph captured before a smoother was re-estimated holds the old Chebyshev coefficients
+  if (mg.graph) {
+    bool stale = mg.graph_generations.size() != mg.smoothers.size();
+    for (size_t l = 0; !stale && l < mg.smoothers.size(); ++l)
+      stale = mg.graph_generations[l] != mg.smoothers[l]->generation;
+    if (stale) {
+      PMG_CUDA(cudaStreamSynchronize(s));
+      cudaGraphExecDestroy(mg.graph);
+      mg.graph = nullptr;
+    }
+  }
   vec::convert(mg.def[L].get(), top.dtype, src, vec_dtype, top.n_dofs, s);
   if (mg.graph_enabled && graphs_allowed() && !prof::enabled() && !mg.graph) mg_capture(mg);
   if (mg.graph && !prof::enabled()) PMG_CUDA(cudaGraphLaunch(mg.graph, s));
@@ -320,6 +335,59 @@ void cg_solve(pmg_operator &A, pmg_mg *mg, void *x, const void *b, double reduce
   info.converged = res <= tol ? 1 : 0;
   info.reduction_per_step = it > 0 ? std::pow(res / info.initial_residual, 1.0 / it) : 1.0;
   PMG_CUDA(cudaStreamSynchronize(s));
+}
+
+// New coefficient values on a hierarchy: A (optional, the CG matrix) and the finest level get
+// the values, every coarser level interpolates the level above it; then every level's
+// inverse diagonal and smoother eigenvalue estimate are recomputed.
+void mg_set_coefficient(pmg_mg &mg, pmg_operator *A, const double *values, bool on_device, cudaStream_t s) {
+  for (auto *op : mg.levels)
+    PMG_REQUIRE(op->coeff_kind == PMG_COEFF_VALUES, "every level needs PMG_COEFF_VALUES");
+  pmg_operator *above = nullptr;
+  if (A) {
+    operator_set_coefficient(*A, values, on_device, s);
+    above = A;
+  }
+  for (int l = (int)mg.levels.size() - 1; l >= 0; --l) {
+    pmg_operator &op = *mg.levels[l];
+    if (above) operator_interpolate_coefficient(op, *above, s);
+    else operator_set_coefficient(op, values, on_device, s);
+    above = &op;
+  }
+  if (A && A->has_diag) operator_compute_inverse_diagonal(*A, s);
+  for (size_t l = 0; l < mg.levels.size(); ++l) {
+    operator_compute_inverse_diagonal(*mg.levels[l], s);
+    chebyshev_estimate(*mg.smoothers[l], s);
+  }
+}
+
+// Gradient of J(m) = 1/2 (u - u_d)^T M (u - u_d) for A(m) u = b with A = sum_q exp(m_q) (...):
+// lambda solves A lambda = M (u - u_d) (A is symmetric), and
+// dJ/dm_q = -exp(m_q) grad lambda_q^T G_q grad u_q = the per-point form of (lambda, u) times -1.
+void adjoint_gradient(pmg_operator &A, const pmg_operator &M, pmg_mg *mg, const void *u, const void *u_d,
+                      void *lambda, double *g_qp, double &J, double reduce, double abs_tol, int max_it,
+                      pmg_cg_info &info, cudaStream_t s) {
+  PMG_REQUIRE(A.kind == PMG_OP_LAPLACE && M.kind == PMG_OP_MASS, "A must be a Laplace and M a mass operator");
+  PMG_REQUIRE(A.dtype == PMG_F64 && M.dtype == PMG_F64, "the adjoint runs in FP64");
+  PMG_REQUIRE(A.n_dofs == M.n_dofs && A.n_cells == M.n_cells && A.degree == M.degree,
+              "A and M must share the mesh and the element");
+  PMG_REQUIRE(u && u_d && lambda && g_qp, "null vector");
+  PMG_CUDA(cudaSetDevice(A.device));
+  const int64_t N = A.n_dofs;
+  const size_t bytes = sizeof(double) * N;
+  if (A.adj_work.size() != 2 || A.adj_work[0].bytes() != bytes) {
+    A.adj_work.clear();
+    for (int i = 0; i < 2; ++i) A.adj_work.emplace_back(bytes);
+  }
+  DeviceBuffer &e = A.adj_work[0], &r = A.adj_work[1];
+  PMG_CUDA(cudaMemcpyAsync(e.get(), u_d, bytes, cudaMemcpyDeviceToDevice, s));
+  vec::xpay(e.get(), u, -1.0, PMG_F64, N, s); // e = u - u_d
+  operator_vmult(M, r.get(), e.get(), s);      // r = M e
+  J = 0.5 * vec::dot(e.get(), r.get(), PMG_F64, N, s);
+  check_finite(J, "the misfit");
+  PMG_CUDA(cudaMemsetAsync(lambda, 0, bytes, s));
+  cg_solve(A, mg, lambda, r.get(), reduce, abs_tol, max_it, info, s);
+  operator_qp_form(A, lambda, u, -1.0, g_qp, s);
 }
 
 } // namespace pmg

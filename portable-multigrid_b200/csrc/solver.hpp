@@ -8,6 +8,8 @@
 struct pmg_chebyshev {
   pmg_operator *op = nullptr;
   int degree = 0;
+  int requested_degree = 0; // <= 0: the degree is chosen by every eigenvalue estimate
+  int generation = 0;       // incremented by every eigenvalue estimate
   double range = 15.0;
   int eig_its = 10;
   bool estimated = false;
@@ -25,6 +27,7 @@ struct pmg_mg {
   // launches on fixed buffers: it is captured once into a CUDA graph and replayed.
   cudaGraphExec_t graph = nullptr;
   bool graph_enabled = true;
+  std::vector<int> graph_generations; // smoother estimates the graph was captured with
   ~pmg_mg() {
     if (graph) cudaGraphExecDestroy(graph);
   }
@@ -39,4 +42,8 @@ void mg_setup(pmg_mg &mg, int n_levels, pmg_operator *const *levels, pmg_transfe
 void mg_vmult(pmg_mg &mg, void *dst, const void *src, int vec_dtype, cudaStream_t s);
 void cg_solve(pmg_operator &A, pmg_mg *mg, void *x, const void *b, double reduce, double abs_tol,
               int max_it, pmg_cg_info &info, cudaStream_t s);
+void mg_set_coefficient(pmg_mg &mg, pmg_operator *A, const double *values, bool on_device, cudaStream_t s);
+void adjoint_gradient(pmg_operator &A, const pmg_operator &M, pmg_mg *mg, const void *u, const void *u_d,
+                      void *lambda, double *g_qp, double &J, double reduce, double abs_tol, int max_it,
+                      pmg_cg_info &info, cudaStream_t s);
 } // namespace pmg

@@ -33,7 +33,7 @@ HEADER_PATH = os.path.join(REPO_ROOT, "include", "pmg", "pmg.h")
 F64, F32 = 0, 1
 GEOMETRY_AUTO, GEOMETRY_FULL, GEOMETRY_AFFINE = 0, 1, 2
 COEFF_NONE, COEFF_KAPPA, COEFF_VALUES = 0, 1, 2
-OP_LAPLACE, OP_DG_SIPG = 0, 1
+OP_LAPLACE, OP_DG_SIPG, OP_MASS = 0, 1, 2
 INVALID = 0xFFFFFFFF
 STATUS = {0: "PMG_OK", -1: "PMG_EINVAL", -2: "PMG_ENOMEM", -3: "PMG_ECUDA",
           -4: "PMG_ENONFINITE", -5: "PMG_ENOCONV", -6: "PMG_EBOUNDS", -7: "PMG_ESTATE",
@@ -153,6 +153,12 @@ def _declare(L):
         "pmg_operator_copy_dof_indices": ([vp, vp], i32),
         "pmg_operator_copy_constrained": ([vp, vp], i32),
         "pmg_operator_copy_geometry": ([vp, vp], i32),
+        "pmg_operator_set_coefficient": ([vp, vp, i32, vp], i32),
+        "pmg_operator_interpolate_coefficient": ([vp, vp, vp], i32),
+        "pmg_operator_quadrature_points": ([vp, vp, vp], i32),
+        "pmg_operator_qp_form": ([vp, vp, vp, d, vp, vp], i32),
+        "pmg_mg_set_coefficient": ([vp, vp, vp, i32, vp], i32),
+        "pmg_adjoint_gradient": ([vp, vp, vp, vp, vp, vp, vp, P(d), d, d, i32, P(CGInfo), vp], i32),
         "pmg_transfer_create": ([vp, vp, P(vp)], i32),
         "pmg_transfer_destroy": ([vp], i32),
         "pmg_transfer_prolongate_and_add": ([vp, vp, vp, vp], i32),
@@ -344,6 +350,37 @@ class LaplaceOperator:
         check(lib().pmg_operator_copy_geometry(self.h, out.ctypes.data_as(C.c_void_p)))
         return out.reshape(-1, 6, nq3)
 
+    # -- coefficient fields and per-point forms (adjoint path) --------------------------
+    def set_coefficient(self, values):
+        """New PMG_COEFF_VALUES values [C, nq^3]: a float64 CUDA tensor or a host array."""
+        if hasattr(values, "is_cuda") and values.is_cuda:
+            v = values.contiguous()
+            check(lib().pmg_operator_set_coefficient(self.h, _ptr(v), 1, _stream()))
+        else:
+            v = np.ascontiguousarray(values, dtype=np.float64)
+            check(lib().pmg_operator_set_coefficient(self.h, v.ctypes.data_as(C.c_void_p), 0, _stream()))
+
+    def interpolate_coefficient(self, src: "LaplaceOperator"):
+        """This operator's coefficient := src's coefficient field at this operator's points."""
+        check(lib().pmg_operator_interpolate_coefficient(self.h, src.h, _stream()))
+
+    def quadrature_points(self):
+        """Gauss points of every cell, float64 CUDA tensor [C, nq^3, 3]."""
+        import torch
+        nq3 = (self.degree + 1) ** 3
+        xq = torch.empty(self.n_cells(), nq3, 3, dtype=torch.float64, device=f"cuda:{self.device}")
+        check(lib().pmg_operator_quadrature_points(self.h, _ptr(xq), _stream()))
+        return xq
+
+    def qp_form(self, u, v, alpha=1.0, out=None):
+        """alpha * grad u^T (coefficient) G grad v at every Gauss point, float64 [C, nq^3]."""
+        import torch
+        nq3 = (self.degree + 1) ** 3
+        if out is None:
+            out = torch.empty(self.n_cells(), nq3, dtype=torch.float64, device=f"cuda:{self.device}")
+        check(lib().pmg_operator_qp_form(self.h, _ptr(u), _ptr(v), alpha, _ptr(out), _stream()))
+        return out
+
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.pmg_operator_destroy(self.h)
@@ -423,6 +460,12 @@ class VCycleMultigrid:
             self.h = None
 
 
+def MassOperator(mesh: Mesh, degree: int, dtype: int = F64, geometry: int = GEOMETRY_AUTO,
+                 coeff_kind: int = COEFF_NONE, coeff_qp=None, device: int = 0):
+    """FE_Q(degree) mass matrix (phi_i, coefficient phi_j), identity rows on constrained DoFs."""
+    return LaplaceOperator(mesh, degree, dtype, geometry, coeff_kind, coeff_qp, device, OP_MASS)
+
+
 def DGLaplaceOperator(mesh: Mesh, degree: int, dtype: int = F64, penalty: float = 0.0, device: int = 0):
     """FE_DGQ(degree) symmetric interior penalty operator (LaplaceOperatorDG); penalty <= 0
     selects the reference's p(p+1)."""
@@ -465,9 +508,12 @@ class Hierarchy:
             mesh = self.meshes[min(l, n_h - 1)]
             dt = coarse_dtype if l == 0 else mg_dtype
             finest = l == len(degrees) - 1 and not dg
-            kind = coeff_kind if (coeff_kind != COEFF_VALUES or finest) else COEFF_NONE
-            self.levels.append(LaplaceOperator(mesh, p, dt, geometry, kind,
+            self.levels.append(LaplaceOperator(mesh, p, dt, geometry, coeff_kind,
                                                coeff_qp if finest else None, device))
+        if coeff_kind == COEFF_VALUES:
+            # coarser levels carry the finest level's field, interpolated level by level
+            for l in range(len(self.levels) - 2, -1, -1):
+                self.levels[l].interpolate_coefficient(self.levels[l + 1])
         if dg:
             self.levels.append(DGLaplaceOperator(self.meshes[-1], pseq[0], mg_dtype, penalty, device))
         for l in range(1, len(self.levels)):
@@ -486,6 +532,18 @@ class Hierarchy:
                                           coeff_qp, device)
         self.mg = VCycleMultigrid(self.levels, self.transfers, self.smoothers)
 
+    def set_coefficient(self, values):
+        """New coefficient values [C, nq^3] (float64, CUDA tensor or host array) for the CG
+        matrix and every level (interpolated downwards); diagonals and smoother estimates are
+        recomputed."""
+        if hasattr(values, "is_cuda") and values.is_cuda:
+            v = values.contiguous()
+            check(lib().pmg_mg_set_coefficient(self.mg.h, self.fine64.h, _ptr(v), 1, _stream()))
+        else:
+            v = np.ascontiguousarray(values, dtype=np.float64)
+            check(lib().pmg_mg_set_coefficient(self.mg.h, self.fine64.h, v.ctypes.data_as(C.c_void_p), 0,
+                                               _stream()))
+
     def estimate(self):
         for s in self.smoothers:
             s.estimate()
@@ -495,3 +553,23 @@ class Hierarchy:
             x = self.fine64.initialize_dof_vector()
         info = solve_cg(self.fine64, x, b, self.mg, reduce, abs_tol, max_iterations)
         return x, info
+
+
+def adjoint_gradient(A: LaplaceOperator, M: LaplaceOperator, u, u_d, precond: VCycleMultigrid | None = None,
+                     reduce=1e-13, abs_tol=1e-300, max_iterations=200, lam=None, g=None):
+    """J = 1/2 (u-u_d)^T M (u-u_d), the adjoint solve A lambda = M (u - u_d) and
+    g[c, q] = dJ/dm_q = -exp(m_q) grad lambda^T G grad u.  Returns (J, g, lambda, cg info)."""
+    import torch
+    nq3 = (A.degree + 1) ** 3
+    if lam is None:
+        lam = A.initialize_dof_vector()
+    if g is None:
+        g = torch.empty(A.n_cells(), nq3, dtype=torch.float64, device=f"cuda:{A.device}")
+    J = C.c_double()
+    info = CGInfo()
+    check(lib().pmg_adjoint_gradient(A.h, M.h, precond.h if precond is not None else None, _ptr(u), _ptr(u_d),
+                                     _ptr(lam), _ptr(g), C.byref(J), reduce, abs_tol, max_iterations,
+                                     C.byref(info), _stream()))
+    return J.value, g, lam, {"iterations": info.iterations, "converged": bool(info.converged),
+                             "initial_residual": info.initial_residual,
+                             "final_residual": info.final_residual}
