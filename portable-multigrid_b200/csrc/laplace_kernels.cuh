@@ -152,6 +152,23 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return false;
 }
 
+// ---- per-thread asynchronous copies into shared memory (cp.async, completion per thread) ----
+__device__ __forceinline__ void cp_async(void *dst_smem, const void *src, int bytes, int src_bytes,
+                                         uint64_t pol) {
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2, %3;" ::"r"(smem_u32(dst_smem)),
+                 "l"(src), "r"(src_bytes), "l"(pol)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2, %3;" ::"r"(smem_u32(dst_smem)),
+                 "l"(src), "r"(src_bytes), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
 // GEOM 0: full G per quadrature point, geo = [group][N (x point p)][N (y point q)][6][LANES]
 // GEOM 1: affine, geo = [cell][8] (6 used) multiplied by the tensor Gauss weight
 // GEOM 2: affine as 1, times coef = [group][N^2][LANES] per quadrature point
@@ -208,19 +225,32 @@ template <int N, typename T> struct Unroll {
 };
 
 // Shared memory per warp of vmult_slab_kernel: 3 exchange buffers, plus (SMEM_G) the
-// group's geometry block and an mbarrier.
-template <int N, typename T, bool SMEM_G> struct SlabSmem {
+// geometry column ring and its two mbarriers, plus the gather pipeline (PIPE): 1 = one
+// group's index block, 2 = one group's gathered src values and two index blocks.
+template <int N, typename T, bool SMEM_G, int PIPE = 0> struct SlabSmem {
   static constexpr size_t XCHG = size_t(3) * Layout<N>::CPW * Stride<N>::CELL * sizeof(T);
   static constexpr size_t CHUNK = size_t(N) * 6 * Layout<N>::LANES * sizeof(T); // one x column
   static constexpr size_t GEO = SMEM_G ? 2 * CHUNK : 0;                         // two-slot ring
-  static constexpr size_t PER_WARP = ((GEO + XCHG + 15) / 16) * 16 + (SMEM_G ? 16 : 0);
+  static constexpr size_t IDXB = size_t(Layout<N>::N2) * Layout<N>::LANES * 4;   // one index block
+  static constexpr size_t SRC = PIPE == 2 ? size_t(Layout<N>::N2) * Layout<N>::LANES * sizeof(T) : 0;
+  static constexpr size_t IDX = PIPE == 0 ? 0 : (PIPE == 1 ? 1 : 2) * IDXB;
+  static constexpr size_t OFF_SRC = ((GEO + XCHG + 15) / 16) * 16;
+  static constexpr size_t OFF_IDX = OFF_SRC + ((SRC + 15) / 16) * 16;
+  static constexpr size_t PER_WARP = OFF_IDX + ((IDX + 15) / 16) * 16 + (SMEM_G ? 16 : 0);
 };
 
 // SMEM_G: the x columns of each group's geometry (contiguous chunks) stream through a
 // two-slot shared-memory ring; the copy of the next column (or of the next group's first
 // column) is issued when a column starts, so it overlaps with that column's work.
 // Launched with one warp per block.
-template <int N, typename T, int GEOM, bool SMEM_G>
+// PIPE: the dependent index -> src gather is taken off the critical path by per-thread
+// cp.async copies one group ahead (each lane copies exactly the entries it later reads, so
+// cp.async.wait_group alone orders them):
+//   1: the next group's index block is copied once the current gather has read its own;
+//   2: the next group's src values are copied (zero-filled at Dirichlet entries) right after
+//      the current group's first phase, from an index block copied a group earlier still;
+//      the scatter reads its indices from shared memory as well.
+template <int N, typename T, int GEOM, bool SMEM_G, int PIPE = 0>
 __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, T>::value))
     vmult_slab_kernel(const __grid_constant__ Tab<N, T> tab, const T *__restrict__ src, T *__restrict__ dst,
                       const uint32_t *__restrict__ idx, const T *__restrict__ geo,
@@ -230,7 +260,8 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
   constexpr int CS = Stride<N>::CELL;
   constexpr unsigned MASK = Lo::MASK;
   constexpr int UNR = SMEM_G ? N : Unroll<N, T>::value;
-  using SM = SlabSmem<N, T, SMEM_G>;
+  using SM = SlabSmem<N, T, SMEM_G, PIPE>;
+  static_assert(!(SMEM_G && PIPE == 2), "src staging is not combined with the geometry ring");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   if (lane >= LANES) return;
@@ -242,6 +273,8 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
   T *bufZ = bufW + CPW * CS;
   T *bufX = bufZ + CPW * CS;
   uint64_t *bars = reinterpret_cast<uint64_t *>(wsm + SM::PER_WARP - 16);
+  T *sbuf = reinterpret_cast<T *>(wsm + SM::OFF_SRC) + lane;               // [N2][LANES] (PIPE 2)
+  uint32_t *ibuf = reinterpret_cast<uint32_t *>(wsm + SM::OFF_IDX) + lane; // [slot][N2][LANES]
   constexpr int CHUNK_ELEMS = N * 6 * LANES;
   uint32_t chunk = 0; // columns consumed so far; slot = chunk & 1, parity = (chunk >> 1) & 1
   const int64_t warp0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -261,21 +294,69 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
   for (int r = 1; r < N; ++r)
     if (s == r) wr = tab.W[r];
 
-  for (int64_t g = warp0; g < n_groups; g += nwarps) {
+  // gather pipeline: copy the index block of group gg into slot `slot` / the src values
+  // named by slot `slot` into sbuf; every call commits exactly one cp.async group
+  auto issue_idx = [&](int64_t gg, int slot) {
+    if (gg < n_groups) {
+      const uint32_t *ip = idx + gg * (N2 * LANES) + lane;
+#pragma unroll
+      for (int a = 0; a < N2; ++a) cp_async(ibuf + (slot * N2 + a) * LANES, ip + a * LANES, 4, 4, pol_first);
+    }
+    cp_async_commit();
+  };
+  auto issue_src = [&](bool valid, int slot) {
+    if (valid) {
+#pragma unroll
+      for (int a = 0; a < N2; ++a) {
+        const uint32_t id = ibuf[(slot * N2 + a) * LANES];
+        const bool ok = id != kInvalidIdx;
+        cp_async(sbuf + a * LANES, ok ? src + id : src, (int)sizeof(T), ok ? (int)sizeof(T) : 0, pol_last);
+      }
+    }
+    cp_async_commit();
+  };
+  int it = 0; // groups done by this warp (PIPE 2: index slot of group g = it & 1)
+  if (PIPE == 1) issue_idx(warp0, 0);
+  if (PIPE == 2) {
+    issue_idx(warp0, 0);
+    cp_async_wait<0>();
+    issue_src(warp0 < n_groups, 0);
+    issue_idx(warp0 + nwarps, 1);
+  }
+
+  for (int64_t g = warp0; g < n_groups; g += nwarps, ++it) {
     if (GEOM == 0 && lane == 0 && g + nwarps < n_groups)
       prefetch_l2(geo + (g + nwarps) * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T), pol_first);
     const uint32_t *ig = idx + g * (N2 * LANES) + lane;
+    const int slot = it & 1;
 
     // ---- phase 1: gather the Y-slab y = s, u[k][i] = src at node (i, s, k) ----
     {
       T u[N][N];
+      if (PIPE == 2) {
+        cp_async_wait<1>(); // this group's src values (the next index block may be in flight)
 #pragma unroll
-      for (int k = 0; k < N; ++k)
+        for (int k = 0; k < N; ++k)
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
-          const uint32_t id = ld_stream(ig + (k * N + i) * LANES, pol_first);
-          u[k][i] = (id != kInvalidIdx) ? ld_keep(src + id, pol_last) : T(0);
-        }
+          for (int i = 0; i < N; ++i) u[k][i] = sbuf[(k * N + i) * LANES];
+      } else if (PIPE == 1) {
+        cp_async_wait<0>(); // this group's index block
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+          for (int i = 0; i < N; ++i) {
+            const uint32_t id = ibuf[(k * N + i) * LANES];
+            u[k][i] = (id != kInvalidIdx) ? ld_keep(src + id, pol_last) : T(0);
+          }
+      } else {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+          for (int i = 0; i < N; ++i) {
+            const uint32_t id = ld_stream(ig + (k * N + i) * LANES, pol_first);
+            u[k][i] = (id != kInvalidIdx) ? ld_keep(src + id, pol_last) : T(0);
+          }
+      }
 #pragma unroll UNR
       for (int p = 0; p < N; ++p) {
         T t[N], tx[N];
@@ -306,6 +387,12 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
         }
       }
     }
+    // the gather's shared-memory entries are consumed: refill them for the next group
+    if (PIPE == 1) issue_idx(g + nwarps, 0);
+    if (PIPE == 2) {
+      cp_async_wait<0>(); // the next group's index block
+      issue_src(g + nwarps < n_groups, slot ^ 1);
+    }
     __syncwarp(MASK);
 
     // ---- phase 2: Z-slab z = s, streamed over the x point p ----
@@ -331,6 +418,7 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
           }
           if (!mbar_wait_bounded(&bars[chunk & 1], (chunk >> 1) & 1, err, 1u << 24)) {
             if (lane == 0) mbar_wait_bounded(&bars[(chunk + 1) & 1], ((chunk + 1) >> 1) & 1, err, 1u << 24);
+            if (PIPE) cp_async_wait<0>();
             return; // the error flag is set; let copies in flight land before leaving
           }
           gcol = ring + (chunk & 1) * CHUNK_ELEMS;
@@ -429,12 +517,15 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
           v = fma(tab.S[k * N + r], A[r], v);
           v = fma(tab.SD[k * N + r], Cc[r], v);
         }
-        const uint32_t id = ld_stream(ig + (k * N + i) * LANES, pol_first);
+        const uint32_t id = PIPE == 2 ? ibuf[(slot * N2 + k * N + i) * LANES]
+                                      : ld_stream(ig + (k * N + i) * LANES, pol_first);
         if (id != kInvalidIdx) red_keep(dst + id, v, pol_last);
       }
     }
+    if (PIPE == 2) issue_idx(g + 2 * nwarps, slot); // this group's index slot is free
     __syncwarp(MASK); // buffers are rewritten by the next group
   }
+  if (PIPE) cp_async_wait<0>(); // no copy may land after the warp has left
 }
 
 // Diagonal of the cell operator summed into diag (atomic), same layout and slab scheme:

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -46,8 +47,8 @@ template <typename T> kern::Tab2<kN, T> make_tab2(const SlabLaunch &L) {
   return t;
 }
 
-template <typename T, bool SMEM_G> constexpr size_t vmult_smem() {
-  return size_t(SMEM_G ? 1 : kWarpsPerBlock) * kern::SlabSmem<kN, T, SMEM_G>::PER_WARP;
+template <typename T, bool SMEM_G, int PIPE> constexpr size_t vmult_smem() {
+  return size_t(SMEM_G ? 1 : kWarpsPerBlock) * kern::SlabSmem<kN, T, SMEM_G, PIPE>::PER_WARP;
 }
 template <typename T> constexpr size_t diag_smem() {
   return size_t(kWarpsPerBlock) * 3 * kern::Layout<kN>::CPW * kern::Layout<kN>::N3 * sizeof(T);
@@ -82,23 +83,75 @@ template <typename T> bool use_ring() {
   if (o == 0 || o == 1) return o == 1;
   return !((sizeof(T) == 4 && kN == 5) || (sizeof(T) == 8 && kN == 7));
 }
+// gather pipeline depth (PIPE template parameter); PMG_VMULT_PIPE=0/1/2 overrides
+inline int pipe_override() {
+  static const int v = [] {
+    const char *e = std::getenv("PMG_VMULT_PIPE");
+    return e ? std::atoi(e) : -1;
+  }();
+  return v;
+}
+// Defaults from B200 sweeps (cell kernel time, 48^3..128^3 meshes): the index pipeline for
+// the FP64 ring variant at N >= 5 (deformed cube: Q4 +3 %, Q5 +26 %); for the Q6 affine
+// kernels the index pipeline in FP32 (+10 %) and src staging in FP64 (+7 %); none elsewhere
+// (Q1-Q3 lose 3-5 %, FP32 full geometry and Q4/Q5 affine lose up to 35 %).
+template <typename T, int GEOM, bool SG> int use_pipe() {
+  const int o = pipe_override();
+  if (o >= 0 && o <= 2) return o;
+  if (SG) return (sizeof(T) == 8 && kN >= 5) ? 1 : 0;
+  if (GEOM != 0 && kN == 7) return sizeof(T) == 8 ? 2 : 1;
+  return 0;
+}
 
-template <typename T, int GEOM, bool SG> void vmult_launch(const SlabLaunch &L) {
-  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG>;
-  allow_smem(k, vmult_smem<T, SG>());
+template <typename T, int GEOM, bool SG, int PIPE> int occ_vmult_variant();
+
+template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabLaunch &L) {
+  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
+  allow_smem(k, vmult_smem<T, SG, PIPE>());
   const int wpb = SG ? 1 : kWarpsPerBlock;
   const int64_t want = (L.n_groups + wpb - 1) / wpb;
-  const int64_t resident = SG ? L.resident_warps_ring : L.resident_warps;
+  // resident warps: the operator caches the PIPE 0 figures; other depths are computed here
+  int64_t resident = SG ? L.resident_warps_ring : L.resident_warps;
+  if (PIPE != 0) {
+    int dev = 0, sms = 0;
+    PMG_CUDA(cudaGetDevice(&dev));
+    PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    static std::mutex mu;
+    static std::map<int, int> per_sm; // device -> resident warps per SM
+    int w = 0;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      auto it = per_sm.find(dev);
+      if (it == per_sm.end()) it = per_sm.emplace(dev, occ_vmult_variant<T, GEOM, SG, PIPE>()).first;
+      w = it->second;
+    }
+    resident = (int64_t)std::max(1, w) * sms;
+  }
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, resident / wpb));
-  k<<<grid, 32 * wpb, vmult_smem<T, SG>(), L.stream>>>(
+  k<<<grid, 32 * wpb, vmult_smem<T, SG, PIPE>(), L.stream>>>(
       make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
       static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err);
   PMG_LAUNCH_CHECK();
 }
 
+// The src-staging pipeline (PIPE 2) is built for the direct-load variant only: together with
+// the geometry column ring it raised "an illegal instruction was encountered" on B200
+// (Q1 FP64, deformed 4^3 mesh) for a cause not found, so that combination is not compiled.
+template <typename T, int GEOM, bool SG> void vmult_pipe(const SlabLaunch &L) {
+  const int pp = use_pipe<T, GEOM, SG>();
+  if constexpr (!SG) {
+    if (pp == 2) {
+      vmult_launch<T, GEOM, SG, 2>(L);
+      return;
+    }
+  }
+  if (pp >= 1) vmult_launch<T, GEOM, SG, 1>(L);
+  else vmult_launch<T, GEOM, SG, 0>(L);
+}
+
 template <typename T, int GEOM> void vmult_geom(const SlabLaunch &L) {
-  if (GEOM == 0 && use_ring<T>()) vmult_launch<T, GEOM, true>(L);
-  else vmult_launch<T, GEOM, false>(L);
+  if (GEOM == 0 && use_ring<T>()) vmult_pipe<T, GEOM, true>(L);
+  else vmult_pipe<T, GEOM, false>(L);
 }
 
 template <typename T, int GEOM> void diag_geom(const SlabLaunch &L) {
@@ -124,18 +177,18 @@ template <typename T> void diag_type(const SlabLaunch &L) {
   else diag_geom<T, 2>(L);
 }
 
-template <typename T, int GEOM, bool SG> int occ_vmult_variant() {
-  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG>;
-  allow_smem(k, vmult_smem<T, SG>());
+template <typename T, int GEOM, bool SG, int PIPE> int occ_vmult_variant() {
+  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
+  allow_smem(k, vmult_smem<T, SG, PIPE>());
   int nb = 0;
   PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, SG ? 32 : 32 * kWarpsPerBlock,
-                                                         vmult_smem<T, SG>()));
+                                                         vmult_smem<T, SG, PIPE>()));
   return nb * (SG ? 1 : kWarpsPerBlock); // resident warps per SM
 }
 // resident warps per SM of the direct variant (low 16 bits) and of the ring variant (high)
 template <typename T, int GEOM> int occ_vmult() {
-  const int direct = occ_vmult_variant<T, GEOM, false>();
-  const int ring = GEOM == 0 ? occ_vmult_variant<T, GEOM, true>() : direct;
+  const int direct = occ_vmult_variant<T, GEOM, false, 0>();
+  const int ring = GEOM == 0 ? occ_vmult_variant<T, GEOM, true, 0>() : direct;
   return direct | (ring << 16);
 }
 template <typename T, int GEOM> int occ_diag() {
