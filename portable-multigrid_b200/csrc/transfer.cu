@@ -6,6 +6,9 @@
 // (Dirichlet entries dropped) through the tensor product of a 1D matrix onto its fine
 // DoFs, each fine entry scaled by 1/(number of patches holding it), 0 when constrained.
 #include <algorithm>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 
 #include "pmg_internal.hpp"
 #include "transfer.hpp"
@@ -83,8 +86,160 @@ __global__ void transfer_kernel(int dir, int nc, int nf, int ppb, const T *__res
 #undef MAT
 }
 
+// Warp-per-patch form of transfer_kernel for NC, NF <= 7 (every p-transfer up to degree 6
+// and the h-transfers up to degree 3): sizes known at compile time, the patch's three
+// tensor sweeps run through per-warp shared-memory buffers with warp barriers only, the 1D
+// matrix sits in shared memory (lanes read different entries).  Same index conventions
+// and results as transfer_kernel.
+template <int NC, int NF, typename T> struct TMat {
+  T m[NC * NF]; // m[i_c * NF + j_f]
+};
+
+template <typename T, int NC, int NF, int DIR> struct PatchShape {
+  static constexpr int A = DIR == 0 ? NC : NF, B = DIR == 0 ? NF : NC;
+  static constexpr int A3 = A * A * A, B3 = B * B * B, T1 = A * A * B, T2 = A * B * B;
+  static constexpr int PER_WARP = A3 + T1 + T2; // elements of T
+};
+
+constexpr int kPatchWarps = 8;
+
+template <typename T, int NC, int NF, int DIR>
+__global__ void __launch_bounds__(32 * kPatchWarps)
+    transfer_patch_kernel(const __grid_constant__ TMat<NC, NF, T> P, const T *__restrict__ src,
+                          T *__restrict__ dst, const uint32_t *__restrict__ cidx,
+                          const uint32_t *__restrict__ fidx, const T *__restrict__ w, int64_t n_patches) {
+  using Sh = PatchShape<T, NC, NF, DIR>;
+  constexpr int A = Sh::A, B = Sh::B, NC3 = NC * NC * NC, NF3 = NF * NF * NF;
+  __shared__ T sM[NC * NF];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  for (int i = threadIdx.x; i < NC * NF; i += blockDim.x) sM[i] = P.m[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  T *in = reinterpret_cast<T *>(smem_raw) + (threadIdx.x >> 5) * Sh::PER_WARP;
+  T *t1 = in + Sh::A3;
+  T *t2 = t1 + Sh::T1;
+  const int64_t warp0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  // M(i, o): input index i, output index o
+  auto M = [&](int i, int o) -> T { return DIR == 0 ? sM[i * NF + o] : sM[o * NF + i]; };
+  for (int64_t patch = warp0; patch < n_patches; patch += nwarps) {
+    for (int l = lane; l < Sh::A3; l += 32) {
+      if (DIR == 0) {
+        const uint32_t id = __ldg(cidx + patch * NC3 + l);
+        in[l] = (id != kInvalid) ? src[id] : T(0);
+      } else {
+        in[l] = __ldg(w + patch * NF3 + l) * src[__ldg(fidx + patch * NF3 + l)];
+      }
+    }
+    __syncwarp();
+    for (int t = lane; t < Sh::T1; t += 32) { // t1[k][j][x] = sum_i M(i, x) in[k][j][i]
+      const int x = t % B, kj = t / B;
+      T s = T(0);
+#pragma unroll
+      for (int i = 0; i < A; ++i) s = fma(M(i, x), in[kj * A + i], s);
+      t1[kj * B + x] = s;
+    }
+    __syncwarp();
+    for (int t = lane; t < Sh::T2; t += 32) { // t2[k][y][x] = sum_j M(j, y) t1[k][j][x]
+      const int x = t % B, y = (t / B) % B, k = t / (B * B);
+      T s = T(0);
+#pragma unroll
+      for (int j = 0; j < A; ++j) s = fma(M(j, y), t1[(k * A + j) * B + x], s);
+      t2[(k * B + y) * B + x] = s;
+    }
+    __syncwarp();
+    for (int t = lane; t < Sh::B3; t += 32) { // z sweep and scatter
+      const int yx = t % (B * B), z = t / (B * B);
+      T s = T(0);
+#pragma unroll
+      for (int k = 0; k < A; ++k) s = fma(M(k, z), t2[k * B * B + yx], s);
+      if (DIR == 0) {
+        atomicAdd(dst + __ldg(fidx + patch * NF3 + t), __ldg(w + patch * NF3 + t) * s);
+      } else {
+        const uint32_t id = __ldg(cidx + patch * NC3 + t);
+        if (id != kInvalid) atomicAdd(dst + id, s);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// DG <-> CG at equal degree: the 1D matrix is the identity and every fine (DG) entry is
+// listed once, so the transfer is an entry-wise gather / scatter-add.
+template <typename T, int DIR>
+__global__ void transfer_identity_kernel(const T *__restrict__ src, T *__restrict__ dst,
+                                         const uint32_t *__restrict__ cidx, const uint32_t *__restrict__ fidx,
+                                         const T *__restrict__ w, int64_t n_entries) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_entries;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t id = __ldg(cidx + e);
+    if (DIR == 0) {
+      const uint32_t f = __ldg(fidx + e);
+      dst[f] += (id != kInvalid) ? __ldg(w + e) * src[id] : T(0);
+    } else if (id != kInvalid) {
+      atomicAdd(dst + id, __ldg(w + e) * src[__ldg(fidx + e)]);
+    }
+  }
+}
+
+template <typename T, int NC, int NF, int DIR>
+void patch_launch(const pmg_transfer &t, void *dst, const void *src, cudaStream_t s) {
+  using Sh = PatchShape<T, NC, NF, DIR>;
+  auto k = transfer_patch_kernel<T, NC, NF, DIR>;
+  const size_t smem = size_t(kPatchWarps) * Sh::PER_WARP * sizeof(T);
+  TMat<NC, NF, T> P;
+  for (int i = 0; i < NC * NF; ++i) P.m[i] = (T)t.P_host[i];
+  static std::mutex mu;
+  static std::map<int, int> per_sm; // device -> resident blocks per SM
+  int blocks = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = per_sm.find(t.device);
+    if (it == per_sm.end()) {
+      PMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int nb = 0;
+      PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kPatchWarps, smem));
+      it = per_sm.emplace(t.device, std::max(1, nb)).first;
+    }
+    blocks = it->second;
+  }
+  const int64_t want = (t.n_patches + kPatchWarps - 1) / kPatchWarps;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)blocks * t.sms));
+  k<<<grid, 32 * kPatchWarps, smem, s>>>(P, static_cast<const T *>(src), static_cast<T *>(dst),
+                                         t.coarse_idx.as<uint32_t>(), t.fine_idx.as<uint32_t>(),
+                                         t.weights.as<T>(), t.n_patches);
+  PMG_LAUNCH_CHECK();
+}
+
+// runtime (nc, nf) -> compiled pair; false if the pair has no compiled form
+template <typename T, int DIR, int NC, int NF> bool try_pair(const pmg_transfer &t, void *dst, const void *src,
+                                                           cudaStream_t s) {
+  if (t.nc != NC || t.nf != NF) return false;
+  patch_launch<T, NC, NF, DIR>(t, dst, src, s);
+  return true;
+}
+template <typename T, int DIR> bool patch_dispatch(const pmg_transfer &t, void *dst, const void *src, cudaStream_t s) {
+  return try_pair<T, DIR, 2, 3>(t, dst, src, s) || try_pair<T, DIR, 2, 4>(t, dst, src, s) ||
+         try_pair<T, DIR, 2, 5>(t, dst, src, s) || try_pair<T, DIR, 2, 6>(t, dst, src, s) ||
+         try_pair<T, DIR, 2, 7>(t, dst, src, s) || try_pair<T, DIR, 3, 4>(t, dst, src, s) ||
+         try_pair<T, DIR, 3, 5>(t, dst, src, s) || try_pair<T, DIR, 3, 6>(t, dst, src, s) ||
+         try_pair<T, DIR, 3, 7>(t, dst, src, s) || try_pair<T, DIR, 4, 5>(t, dst, src, s) ||
+         try_pair<T, DIR, 4, 6>(t, dst, src, s) || try_pair<T, DIR, 4, 7>(t, dst, src, s) ||
+         try_pair<T, DIR, 5, 6>(t, dst, src, s) || try_pair<T, DIR, 5, 7>(t, dst, src, s) ||
+         try_pair<T, DIR, 6, 7>(t, dst, src, s);
+}
+
 template <typename T> std::vector<T> cast(const std::vector<double> &v) {
   return std::vector<T>(v.begin(), v.end());
+}
+
+// PMG_TRANSFER_GENERIC=1 keeps every transfer on transfer_kernel (a comparison switch)
+bool patch_kernels_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("PMG_TRANSFER_GENERIC");
+    return !(e && e[0] == '1');
+  }();
+  return on;
 }
 
 bool same_box_geometry(const pmg_box &a, const pmg_box &b) {
@@ -173,6 +328,7 @@ void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_opera
     mult[i] = (fine.num.constrained[i] || mult[i] == 0.0) ? 0.0 : 1.0 / mult[i];
   std::vector<double> w(fidx.size());
   for (size_t e = 0; e < fidx.size(); ++e) w[e] = mult[fidx[e]];
+  t.P_host = P;
   if (t.dtype == PMG_F64) {
     t.P1d = upload(P);
     t.weights = upload(w);
@@ -188,6 +344,8 @@ void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_opera
   t.smem = s * (((t.nc * t.nf + 3) & ~3) + (size_t)t.ppb * 3 * nf3);
   int sms = 0;
   PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t.device));
+  t.sms = sms;
+  t.patch_kernels = patch_kernels_enabled();
   t.grid = (int)std::max<int64_t>(1, std::min<int64_t>((t.n_patches + t.ppb - 1) / t.ppb, (int64_t)sms * 8));
   if (t.dtype == PMG_F64)
     PMG_CUDA(cudaFuncSetAttribute(transfer_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
@@ -199,6 +357,37 @@ void transfer_apply(const pmg_transfer &t, int dir, void *dst, const void *src, 
   PMG_REQUIRE(dst && src, "null vector");
   if (t.n_patches == 0) return;
   prof::Scope scope(dir == 0 ? "transfer_prolongate" : "transfer_restrict", s);
+  if (t.kind == 2) {
+    const int64_t n = t.n_patches * t.nf * t.nf * t.nf;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)t.sms * 16));
+    if (t.dtype == PMG_F64) {
+      if (dir == 0)
+        transfer_identity_kernel<double, 0><<<grid, 256, 0, s>>>(static_cast<const double *>(src), static_cast<double *>(dst),
+                                                                 t.coarse_idx.as<uint32_t>(), t.fine_idx.as<uint32_t>(),
+                                                                 t.weights.as<double>(), n);
+      else
+        transfer_identity_kernel<double, 1><<<grid, 256, 0, s>>>(static_cast<const double *>(src), static_cast<double *>(dst),
+                                                                 t.coarse_idx.as<uint32_t>(), t.fine_idx.as<uint32_t>(),
+                                                                 t.weights.as<double>(), n);
+    } else {
+      if (dir == 0)
+        transfer_identity_kernel<float, 0><<<grid, 256, 0, s>>>(static_cast<const float *>(src), static_cast<float *>(dst),
+                                                                t.coarse_idx.as<uint32_t>(), t.fine_idx.as<uint32_t>(),
+                                                                t.weights.as<float>(), n);
+      else
+        transfer_identity_kernel<float, 1><<<grid, 256, 0, s>>>(static_cast<const float *>(src), static_cast<float *>(dst),
+                                                                t.coarse_idx.as<uint32_t>(), t.fine_idx.as<uint32_t>(),
+                                                                t.weights.as<float>(), n);
+    }
+    PMG_LAUNCH_CHECK();
+    return;
+  }
+  if (t.patch_kernels) {
+    bool done = false;
+    if (t.dtype == PMG_F64) done = dir == 0 ? patch_dispatch<double, 0>(t, dst, src, s) : patch_dispatch<double, 1>(t, dst, src, s);
+    else done = dir == 0 ? patch_dispatch<float, 0>(t, dst, src, s) : patch_dispatch<float, 1>(t, dst, src, s);
+    if (done) return;
+  }
   if (t.dtype == PMG_F64)
     transfer_kernel<double><<<t.grid, 128, t.smem, s>>>(dir, t.nc, t.nf, t.ppb, t.P1d.as<double>(),
                                                         static_cast<const double *>(src), static_cast<double *>(dst),

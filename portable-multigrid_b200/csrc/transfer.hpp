@@ -1,6 +1,8 @@
 // Multigrid transfer objects (transfer.cu).
 #pragma once
 
+#include <vector>
+
 #include "pmg_internal.hpp"
 
 struct pmg_transfer {
@@ -10,8 +12,11 @@ struct pmg_transfer {
   int nc = 0, nf = 0;
   int64_t n_patches = 0, n_coarse = 0, n_fine = 0;
   pmg::DeviceBuffer P1d, coarse_idx, fine_idx, weights;
+  std::vector<double> P_host; // the 1D matrix [nc][nf], passed to the kernels by value
   int ppb = 1, grid = 1;
   size_t smem = 0;
+  int sms = 0;               // SM count of the device
+  bool patch_kernels = true; // warp-per-patch kernels for the compiled (nc, nf) pairs
 };
 
 namespace pmg {
