@@ -16,6 +16,7 @@
 // basis functions are exact, so the face quadrature is applied as the 1D GLL mass matrix
 // M1 = S diag(w) S^T in each tangential direction.
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "dg.hpp"
@@ -45,15 +46,127 @@ template <int N> __device__ __forceinline__ int face_node(int d, int layer, int 
   return (k * N + j) * N + i;
 }
 
-template <int N> constexpr int dg_batch() { return (128 / (N * N)) > 0 ? 128 / (N * N) : 1; }
+// cells per block: six faces x N^2 face points per cell, about 384 threads per block
+template <int N> constexpr int dg_batch() { return (384 / (6 * N * N)) > 0 ? 384 / (6 * N * N) : 1; }
+template <int N> constexpr int dg_threads() { return ((6 * dg_batch<N>() * N * N + 31) / 32) * 32; }
+
+// One block per batch of B cells; all six faces of the batch are evaluated at once, one
+// thread per (face, cell, face point):
+//   1. per face point the flux values f1 = sigma [u] - {d_n u}, f2 = -[u]/2 from the own
+//      and the neighbour's traces (read through L1 / L2; every value is read by a few face
+//      points of the batch);
+//   2./3. the face mass matrix M1 x M1 applied along the two tangential directions, giving
+//      the value-test and normal-derivative-test coefficients of every face point;
+//   4. one thread per cell node sums what the six faces give it: the value test where the
+//      node lies on the face layer, and the normal-derivative test on every layer.
+// Three block barriers per batch, no shared-memory atomics.
+template <int N, typename T>
+__global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __grid_constant__ DGTab<N, T> tab,
+                                                                  const __grid_constant__ DGGeo geo,
+                                                                  const T *__restrict__ src,
+                                                                  T *__restrict__ dst,
+                                                                  const int32_t *__restrict__ nbr,
+                                                                  int64_t n_cells) {
+  constexpr int N2 = N * N, N3 = N2 * N, B = dg_batch<N>(), FP = 6 * B * N2;
+  __shared__ T F1[6][B][N2], F2[6][B][N2], G1[6][B][N2], G2[6][B][N2];
+  const int t = threadIdx.x;
+  // this thread's face point (phases 2-4)
+  const int f = t / (B * N2), rem = t - f * (B * N2), b = rem / N2, ab = rem - b * N2, a = ab % N, bb = ab / N;
+  const int d = f >> 1, sd = f & 1;
+  const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+  const T sgn_h = t < FP ? (sd ? T(1) : T(-1)) / (T)geo.h[d] : T(0); // n . grad = sgn_h d/dxi_d
+  const T area = t < FP ? (T)(geo.h[ta] * geo.h[tb]) : T(0);
+  const T sigma = t < FP ? (T)(geo.c_pen / geo.h[d]) : T(0);
+  const bool bc_dirichlet = t < FP && ((geo.dirichlet >> f) & 1);
+  for (int64_t base = int64_t(blockIdx.x) * B; base < n_cells; base += int64_t(gridDim.x) * B) {
+    if (t < FP) {
+      const int64_t c = base + b;
+      T f1 = T(0), f2 = T(0);
+      if (c < n_cells) {
+        const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
+        const T *dphi_nb = sd ? tab.dphi0 : tab.dphi1;
+        const int own_layer = sd ? N - 1 : 0, nb_layer = sd ? 0 : N - 1;
+        const T *uo = src + c * N3;
+        const T vo = __ldg(uo + face_node<N>(d, own_layer, a, bb));
+        T dn = T(0);
+#pragma unroll
+        for (int i = 0; i < N; ++i) dn += dphi_own[i] * __ldg(uo + face_node<N>(d, i, a, bb));
+        dn *= sgn_h;
+        const int32_t nb = nbr[c * 6 + f];
+        if (nb >= 0) {
+          const T *un = src + int64_t(nb) * N3;
+          const T vn = __ldg(un + face_node<N>(d, nb_layer, a, bb));
+          T dnn = T(0);
+#pragma unroll
+          for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * __ldg(un + face_node<N>(d, i, a, bb));
+          dnn *= sgn_h;
+          const T jump = vo - vn;
+          f1 = sigma * jump - T(0.5) * (dn + dnn);
+          f2 = T(-0.5) * jump;
+        } else if (bc_dirichlet) { // mirror: u+ = -u-, d_n u+ = d_n u-
+          f1 = sigma * T(2) * vo - dn;
+          f2 = -vo;
+        }
+      }
+      F1[f][b][ab] = f1 * area;
+      F2[f][b][ab] = f2 * area;
+    }
+    __syncthreads();
+    if (t < FP) { // face mass along a
+      T g1 = T(0), g2 = T(0);
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        g1 += tab.M1[a * N + k] * F1[f][b][bb * N + k];
+        g2 += tab.M1[a * N + k] * F2[f][b][bb * N + k];
+      }
+      G1[f][b][ab] = g1;
+      G2[f][b][ab] = g2;
+    }
+    __syncthreads();
+    if (t < FP) { // along b: value-test and normal-test coefficients (F1/F2 reused)
+      T tv = T(0), tn = T(0);
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        tv += tab.M1[bb * N + k] * G1[f][b][k * N + a];
+        tn += tab.M1[bb * N + k] * G2[f][b][k * N + a];
+      }
+      F1[f][b][ab] = tv;
+      F2[f][b][ab] = tn * sgn_h;
+    }
+    __syncthreads();
+    for (int e = t; e < B * N3; e += blockDim.x) {
+      const int cb = e / N3, l = e - cb * N3;
+      const int64_t c = base + cb;
+      if (c >= n_cells) continue;
+      const int idx[3] = {l % N, (l / N) % N, l / N2};
+      T v = T(0);
+#pragma unroll
+      for (int ff = 0; ff < 6; ++ff) {
+        const int dd = ff >> 1, ss = ff & 1;
+        const int pa = dd == 0 ? idx[1] : idx[0], pb = dd == 2 ? idx[1] : idx[2];
+        const int pab = pb * N + pa;
+        const T *dphi = ss ? tab.dphi1 : tab.dphi0;
+        v += F2[ff][cb][pab] * dphi[idx[dd]];
+        if (idx[dd] == (ss ? N - 1 : 0)) v += F1[ff][cb][pab];
+      }
+      dst[c * N3 + l] += v;
+    }
+    __syncthreads();
+  }
+}
+
+// The six faces one after another (three block barriers per face, 128 threads for a batch of
+// 128 / N^2 cells): kept as the comparison form of dg_face_kernel (PMG_DG_FACE=0).
+template <int N> constexpr int dg_batch_seq() { return (128 / (N * N)) > 0 ? 128 / (N * N) : 1; }
 
 template <int N, typename T>
-__global__ void __launch_bounds__(128) dg_face_kernel(const DGTab<N, T> tab, const DGGeo geo,
+__global__ void __launch_bounds__(128) dg_face_seq_kernel(const __grid_constant__ DGTab<N, T> tab,
+                                                          const __grid_constant__ DGGeo geo,
                                                       const T *__restrict__ src,
                                                       T *__restrict__ dst,
                                                       const int32_t *__restrict__ nbr,
                                                       int64_t n_cells) {
-  constexpr int N2 = N * N, N3 = N2 * N, B = dg_batch<N>();
+  constexpr int N2 = N * N, N3 = N2 * N, B = dg_batch_seq<N>();
   __shared__ T own[B][N3];
   __shared__ T out[B][N3];
   __shared__ T F1[B][N2], F2[B][N2], G1[B][N2], G2[B][N2];
@@ -178,6 +291,15 @@ template <typename T> __global__ void add_kernel(T *__restrict__ dst, const doub
     dst[i] += (T)src[i];
 }
 
+// PMG_DG_FACE=0 selects the face-by-face kernel (a comparison switch)
+int face_form() {
+  static const int v = [] {
+    const char *e = std::getenv("PMG_DG_FACE");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return v;
+}
+
 template <int N, typename T> DGTab<N, T> make_dg_tab(const DGHost &h) {
   DGTab<N, T> t;
   for (int a = 0; a < N * N; ++a) t.M1[a] = (T)h.M1[a];
@@ -204,11 +326,20 @@ void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, i
     dg_face_diag_kernel<N, T><<<std::max(grid, 1), 256, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
                                                                   static_cast<T *>(dst), h.nbr.as<int32_t>(), n_cells);
   } else {
-    constexpr int B = dg_batch<N>();
-    const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 16);
-    dg_face_kernel<N, T><<<std::max(grid, 1), 128, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
-                                                            static_cast<const T *>(src), static_cast<T *>(dst),
-                                                            h.nbr.as<int32_t>(), n_cells);
+    if (face_form() == 0) {
+      constexpr int B = dg_batch_seq<N>();
+      const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 16);
+      dg_face_seq_kernel<N, T><<<std::max(grid, 1), 128, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
+                                                                  static_cast<const T *>(src), static_cast<T *>(dst),
+                                                                  h.nbr.as<int32_t>(), n_cells);
+    } else {
+      constexpr int B = dg_batch<N>();
+      const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 8);
+      dg_face_kernel<N, T><<<std::max(grid, 1), dg_threads<N>(), 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
+                                                                         static_cast<const T *>(src),
+                                                                         static_cast<T *>(dst), h.nbr.as<int32_t>(),
+                                                                         n_cells);
+    }
   }
   PMG_LAUNCH_CHECK();
 }

@@ -215,13 +215,15 @@ __device__ __forceinline__ void load_g6(const T *__restrict__ geo, const T *gs,
 
 // resident blocks of 128 threads per SM the register allocation is sized for; matches the
 // shared-memory footprint (3 exchange buffers per warp) of each degree and type
-template <int N, typename T> struct MinBlocks {
-  static constexpr int value = sizeof(T) == 8 ? (N >= 6 ? 2 : 3) : 2;
+template <int N, typename T, int GEOM = 1> struct MinBlocks {
+  static constexpr int value = sizeof(T) == 8 ? (N >= 6 ? 2 : 3) : ((N == 7 && GEOM == 0) ? 3 : 2);
 };
 // outer streaming loops: runtime loops for FP64 (bounded live registers), unrolled for FP32
-// (registers are cheap at 4 bytes and unrolling keeps the tables as immediate operands)
-template <int N, typename T> struct Unroll {
-  static constexpr int value = sizeof(T) == 8 ? 1 : N;
+// (registers are cheap at 4 bytes and unrolling keeps the tables as immediate operands),
+// except FP32 Q6 with full geometry, where runtime loops at 170 registers (12 warps/SM)
+// measured 1.4x faster on B200 than the unrolled form at 255
+template <int N, typename T, int GEOM = 1> struct Unroll {
+  static constexpr int value = (sizeof(T) == 8 || (N == 7 && GEOM == 0)) ? 1 : N;
 };
 
 // Shared memory per warp of vmult_slab_kernel: 3 exchange buffers, plus (SMEM_G) the
@@ -251,7 +253,7 @@ template <int N, typename T, bool SMEM_G, int PIPE = 0> struct SlabSmem {
 //      the current group's first phase, from an index block copied a group earlier still;
 //      the scatter reads its indices from shared memory as well.
 template <int N, typename T, int GEOM, bool SMEM_G, int PIPE = 0>
-__global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, T>::value))
+__global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, T, GEOM>::value))
     vmult_slab_kernel(const __grid_constant__ Tab<N, T> tab, const T *__restrict__ src, T *__restrict__ dst,
                       const uint32_t *__restrict__ idx, const T *__restrict__ geo,
                       const T *__restrict__ coef, int64_t n_groups, unsigned int *err) {
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
   constexpr int CPW = Lo::CPW, LANES = Lo::LANES, N2 = Lo::N2;
   constexpr int CS = Stride<N>::CELL;
   constexpr unsigned MASK = Lo::MASK;
-  constexpr int UNR = SMEM_G ? N : Unroll<N, T>::value;
+  constexpr int UNR = SMEM_G ? N : Unroll<N, T, GEOM>::value;
   using SM = SlabSmem<N, T, SMEM_G, PIPE>;
   static_assert(!(SMEM_G && PIPE == 2), "src staging is not combined with the geometry ring");
   extern __shared__ __align__(16) unsigned char smem_raw[];

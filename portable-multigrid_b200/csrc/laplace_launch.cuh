@@ -47,8 +47,14 @@ template <typename T> kern::Tab2<kN, T> make_tab2(const SlabLaunch &L) {
   return t;
 }
 
+// warps per block of vmult_slab_kernel: one for the ring variant; for the direct variant four,
+// unless a warp needs more than 24 KB of shared memory (FP64 at N >= 6), where blocks of four
+// would leave most of an SM's shared memory unused (one 132-220 KB block per SM)
+template <typename T, bool SMEM_G, int PIPE> constexpr int vmult_wpb() {
+  return (SMEM_G || kern::SlabSmem<kN, T, SMEM_G, PIPE>::PER_WARP > 24 * 1024) ? 1 : kWarpsPerBlock;
+}
 template <typename T, bool SMEM_G, int PIPE> constexpr size_t vmult_smem() {
-  return size_t(SMEM_G ? 1 : kWarpsPerBlock) * kern::SlabSmem<kN, T, SMEM_G, PIPE>::PER_WARP;
+  return size_t(vmult_wpb<T, SMEM_G, PIPE>()) * kern::SlabSmem<kN, T, SMEM_G, PIPE>::PER_WARP;
 }
 template <typename T> constexpr size_t diag_smem() {
   return size_t(kWarpsPerBlock) * 3 * kern::Layout<kN>::CPW * kern::Layout<kN>::N3 * sizeof(T);
@@ -69,7 +75,8 @@ template <typename K> void allow_smem(K kernel, size_t bytes) {
 
 // Full geometry streams through the shared-memory column ring (TMA) except where direct
 // loads measured faster on B200 (deformed-cube sweeps at 64^3/128^3): FP32 degree 4, whose
-// register-heavy unrolled form already hides the latency at 8 warps/SM, and FP64 degree 6.
+// register-heavy unrolled form already hides the latency at 8 warps/SM, and degree 6 in
+// both types.
 // PMG_VMULT_STAGE=0 / 1 forces direct loads / the ring (a tuning switch; both are compiled).
 inline int stage_override() {
   static const int v = [] {
@@ -81,7 +88,7 @@ inline int stage_override() {
 template <typename T> bool use_ring() {
   const int o = stage_override();
   if (o == 0 || o == 1) return o == 1;
-  return !((sizeof(T) == 4 && kN == 5) || (sizeof(T) == 8 && kN == 7));
+  return !((sizeof(T) == 4 && kN == 5) || kN == 7);
 }
 // gather pipeline depth (PIPE template parameter); PMG_VMULT_PIPE=0/1/2 overrides
 inline int pipe_override() {
@@ -92,14 +99,14 @@ inline int pipe_override() {
   return v;
 }
 // Defaults from B200 sweeps (cell kernel time, 48^3..128^3 meshes): the index pipeline for
-// the FP64 ring variant at N >= 5 (deformed cube: Q4 +3 %, Q5 +26 %); for the Q6 affine
-// kernels the index pipeline in FP32 (+10 %) and src staging in FP64 (+7 %); none elsewhere
-// (Q1-Q3 lose 3-5 %, FP32 full geometry and Q4/Q5 affine lose up to 35 %).
+// the FP64 ring variant at N >= 5 (deformed cube: Q4 +3 %, Q5 +26 %) and for the FP32 Q6
+// affine kernel (+9 %); none elsewhere (Q1-Q3 lose 3-5 %, FP32 full geometry, Q4/Q5 affine
+// and FP64 Q6 affine lose 15-35 %).
 template <typename T, int GEOM, bool SG> int use_pipe() {
   const int o = pipe_override();
   if (o >= 0 && o <= 2) return o;
   if (SG) return (sizeof(T) == 8 && kN >= 5) ? 1 : 0;
-  if (GEOM != 0 && kN == 7) return sizeof(T) == 8 ? 2 : 1;
+  if (GEOM != 0 && kN == 7 && sizeof(T) == 4) return 1;
   return 0;
 }
 
@@ -108,7 +115,7 @@ template <typename T, int GEOM, bool SG, int PIPE> int occ_vmult_variant();
 template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabLaunch &L) {
   auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
   allow_smem(k, vmult_smem<T, SG, PIPE>());
-  const int wpb = SG ? 1 : kWarpsPerBlock;
+  constexpr int wpb = vmult_wpb<T, SG, PIPE>();
   const int64_t want = (L.n_groups + wpb - 1) / wpb;
   // resident warps: the operator caches the PIPE 0 figures; other depths are computed here
   int64_t resident = SG ? L.resident_warps_ring : L.resident_warps;
@@ -181,9 +188,9 @@ template <typename T, int GEOM, bool SG, int PIPE> int occ_vmult_variant() {
   auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
   allow_smem(k, vmult_smem<T, SG, PIPE>());
   int nb = 0;
-  PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, SG ? 32 : 32 * kWarpsPerBlock,
-                                                         vmult_smem<T, SG, PIPE>()));
-  return nb * (SG ? 1 : kWarpsPerBlock); // resident warps per SM
+  constexpr int wpb = vmult_wpb<T, SG, PIPE>();
+  PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * wpb, vmult_smem<T, SG, PIPE>()));
+  return nb * wpb; // resident warps per SM
 }
 // resident warps per SM of the direct variant (low 16 bits) and of the ring variant (high)
 template <typename T, int GEOM> int occ_vmult() {
