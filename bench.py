@@ -198,7 +198,7 @@ def time_vmults(op, dst, src, steps, torch, stream):
     pmg.profile_enable(False)
     total_ms = start.elapsed_time(stop)
     cell_ms, cell_n = pmg.profile_query("vmult_cell")
-    cons_ms, cons_n = pmg.profile_query("vmult_constrained")
+    cons_ms, cons_n = pmg.profile_query("vmult_init")
     return total_ms, cell_ms, cell_n, cons_n
 
 

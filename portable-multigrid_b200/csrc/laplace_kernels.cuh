@@ -170,7 +170,8 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
 }
 
 // GEOM 0: full G per quadrature point, geo = [group][N (x point p)][N (y point q)][6][LANES]
-// GEOM 1: affine, geo = [cell][8] (6 used) multiplied by the tensor Gauss weight
+// GEOM 1: affine, geo = [cell][8] (6 used) multiplied by the tensor Gauss weight; affine cells
+//         are axis-aligned boxes, so only rr, ss, tt are nonzero (the vmult uses those three)
 // GEOM 2: affine as 1, times coef = [group][N^2][LANES] per quadrature point
 //
 // Register budget: every phase streams over one index so that at most ~2 N^2 values are
@@ -398,6 +399,13 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
     __syncwarp(MASK);
 
     // ---- phase 2: Z-slab z = s, streamed over the x point p ----
+    T cd0 = T(0), cd3 = T(0), cd5 = T(0); // diagonal of the affine cell tensor
+    if (GEOM != 0) {
+      const T *cg = geo + (g * CPW + e) * 8;
+      cd0 = __ldg(cg);
+      cd3 = __ldg(cg + 3);
+      cd5 = __ldg(cg + 5);
+    }
     {
       T a[N][N]; // [j][i]
 #pragma unroll
@@ -443,11 +451,20 @@ __global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, 
             dy = fma(tab.SD[j * N + q], Wc[j], dy);
             dz = fma(tab.S[j * N + q], Zc[j], dz);
           }
-          T gc[6];
-          load_g6<N, T, GEOM, SMEM_G>(geo, gcol, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
-          fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
-          fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
-          bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
+          if (GEOM == 0) {
+            T gc[6];
+            load_g6<N, T, GEOM, SMEM_G>(geo, gcol, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
+            fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
+            fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
+            bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
+          } else {
+            // affine cells are axis-aligned boxes: the cell tensor is diagonal (rr, ss, tt)
+            T w = wr * tab.W[q] * tab.W[p];
+            if (GEOM == 2) w *= ld_stream(coef + g * (N2 * LANES) + (q * N + p) * LANES + lane, pol_first);
+            fx[q] = (w * cd0) * dx;
+            fy[q] = (w * cd3) * dy;
+            bufX[(s * N + q) * N + p] = (w * cd5) * dz; // fz
+          }
         }
 #pragma unroll
         for (int j = 0; j < N; ++j) {

@@ -166,6 +166,16 @@ __global__ void invert_diagonal_kernel(T *__restrict__ d, int64_t n) {
     d[i] = (d[i] != T(0)) ? T(1) / d[i] : T(1);
 }
 
+// dst_i = src_i on constrained DoFs (bit i of `bits`), 0 elsewhere
+template <typename T>
+__global__ void init_dst_kernel(T *__restrict__ dst, const T *__restrict__ src, const uint32_t *__restrict__ bits,
+                                int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = __ldg(bits + (i >> 5));
+    dst[i] = ((w >> (i & 31)) & 1u) ? src[i] : T(0);
+  }
+}
+
 template <typename T>
 __global__ void set_constrained_kernel(T *__restrict__ dst, const T *__restrict__ src,
                                        const uint32_t *__restrict__ list, int64_t n, T value) {
@@ -322,6 +332,9 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
       if (op.num.constrained[i]) list.push_back((uint32_t)i);
     op.n_constrained = (int64_t)list.size();
     op.constrained_list = upload(list);
+    std::vector<uint32_t> bits((size_t)(op.n_dofs + 31) / 32, 0u);
+    for (uint32_t i : list) bits[i >> 5] |= 1u << (i & 31);
+    op.constrained_bits = upload(bits);
   }
   // geometry (compute_G_tensors, bk3.h:456-515), computed on the device
   const size_t s = dtype_size(op.dtype);
@@ -432,7 +445,21 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
   PMG_REQUIRE(dst && src, "null vector");
   PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");
   const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
-  PMG_CUDA(cudaMemsetAsync(dst, 0, bytes, s)); // dst = 0 (bk3.h:134)
+  // dst = 0 (bk3.h:134) with the identity rows of copy_constrained_values (bk3.h:230) written
+  // in the same pass: the cell kernels never touch constrained entries (index sentinel)
+  if (op.n_constrained > 0) {
+    prof::Scope scope("vmult_init", s);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((op.n_dofs + 255) / 256, (int64_t)op.sms * 16));
+    if (op.dtype == PMG_F64)
+      init_dst_kernel<double><<<grid, 256, 0, s>>>(static_cast<double *>(dst), static_cast<const double *>(src),
+                                                   op.constrained_bits.as<uint32_t>(), op.n_dofs);
+    else
+      init_dst_kernel<float><<<grid, 256, 0, s>>>(static_cast<float *>(dst), static_cast<const float *>(src),
+                                                  op.constrained_bits.as<uint32_t>(), op.n_dofs);
+    PMG_LAUNCH_CHECK();
+  } else {
+    PMG_CUDA(cudaMemsetAsync(dst, 0, bytes, s));
+  }
   if (compute && op.n_cells > 0 && op.kind == PMG_OP_MASS) {
     prof::Scope scope("vmult_mass", s);
     mass_vmult_cells(op, src, dst, s);
@@ -451,17 +478,6 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
       prof::Scope scope("vmult_dg_faces", s);
       dg_apply_faces(*op.dg, op.degree, op.dtype, src, dst, op.n_cells, op.sms, s);
     }
-  }
-  if (op.n_constrained > 0) {
-    prof::Scope scope("vmult_constrained", s);
-    const int grid = (int)std::min<int64_t>(1024, (op.n_constrained + 255) / 256);
-    if (op.dtype == PMG_F64)
-      set_constrained_kernel<double><<<grid, 256, 0, s>>>(static_cast<double *>(dst), static_cast<const double *>(src),
-                                                          op.constrained_list.as<uint32_t>(), op.n_constrained, 0.0);
-    else
-      set_constrained_kernel<float><<<grid, 256, 0, s>>>(static_cast<float *>(dst), static_cast<const float *>(src),
-                                                         op.constrained_list.as<uint32_t>(), op.n_constrained, 0.0f);
-    PMG_LAUNCH_CHECK();
   }
 }
 

@@ -197,6 +197,7 @@ struct pmg_operator {
   pmg::DeviceBuffer cell_xyz;       // [C][3] int32 lattice coordinates of the cells
   pmg::DeviceBuffer cell_lut;       // lattice (x fastest) -> cell, int32 (built on demand)
   pmg::DeviceBuffer constrained_list; // uint32 [n_constrained]
+  pmg::DeviceBuffer constrained_bits; // uint32 [(N + 31) / 32], bit i set: DoF i constrained
   int64_t n_constrained = 0;
   pmg::DeviceBuffer inv_diag;       // [N] dtype
   bool has_diag = false;
