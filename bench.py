@@ -61,6 +61,23 @@ def dist_env():
     return rank, world, local
 
 
+def slowest_rank_ms(times_ms, device):
+    """Each of the local device times (ms) as the maximum over all ranks of the default process
+    group (the job is as slow as its slowest replica); unchanged without a process group."""
+    import torch
+    t = torch.tensor([float(v) for v in times_ms], dtype=torch.float64, device=device)
+    dist = torch.distributed
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def replica_rate(n_dofs, world, steps, ms):
+    """Whole-job GDoF/s of `world` replicas that each applied the operator `steps` times to
+    n_dofs DoFs in `ms` milliseconds (the slowest rank's time)."""
+    return n_dofs * world * steps / (ms * 1e-3) / 1e9
+
+
 def box_for(cells):
     refine = int(round(np.log2(cells)))
     assert 1 << refine == cells, "--cells must be a power of two"
@@ -418,22 +435,16 @@ def gpu_arm(args):
     torch.cuda.synchronize()
     barrier()
     # slowest rank
-    t_local = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
-    if world > 1:
-        torch.distributed.all_reduce(t_local, op=torch.distributed.ReduceOp.MAX)
-    t_max = float(t_local.item())
+    t_max = slowest_rank_ms([total_ms], f"cuda:{dev}")[0]
     ms_per_step = t_max / args.steps
-    value = N * world * args.steps / (t_max * 1e-3) / 1e9
+    value = replica_rate(N, world, args.steps, t_max)
 
     # end to end through the same C-ABI call, host buffers, copies inside the timed region
     e2e_steps = max(3, min(args.steps // 10, 20))
     e2e_ms, e2e_serial_ms = e2e_vmults(op, src_host, e2e_steps, torch, dev, barrier)
-    if world > 1:
-        t = torch.tensor([e2e_ms, e2e_serial_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms, e2e_serial_ms = float(t[0]), float(t[1])
-    e2e_value = N * world * e2e_steps / (e2e_ms * 1e-3) / 1e9
-    e2e_serial = N * world * e2e_steps / (e2e_serial_ms * 1e-3) / 1e9
+    e2e_ms, e2e_serial_ms = slowest_rank_ms([e2e_ms, e2e_serial_ms], f"cuda:{dev}")
+    e2e_value = replica_rate(N, world, e2e_steps, e2e_ms)
+    e2e_serial = replica_rate(N, world, e2e_steps, e2e_serial_ms)
     bytes_elem = 8 if dt == pmg.F64 else 4
 
     # roofline of the cell kernel: algorithmic bytes per launch over its event-timed duration
