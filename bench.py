@@ -323,6 +323,49 @@ def time_to_solution(torch, pmg, dev, refine=4, repeats=3):
     return res
 
 
+def reference_problem(torch, pmg, dev, cycle=20, repeats=3):
+    """The reference's own logged solve: Q4, f = 1, homogeneous Dirichlet on the "doubling" mesh
+    of cycle 20 (2 x 2 x 1 coarse cells refined 6 times, 67,634,433 DoFs), ph-multigrid with
+    p 4 -> 3 -> 2 -> 1 and Q1 h-levels, Chebyshev(5), CG to a reduction of 1e-9, all-FP64 and with
+    the FP32 V-cycle; setup (hierarchy, right-hand side, eigenvalue estimates) and solve times
+    next to the GH200 figures the reference logged for the same problem
+    (tests/poisson_cube_bk3_fp64/results/single-gpu-batched.out:1172-1184 and
+    tests/poisson_cube_bk3/results/signle-gpu-batched-mixed-precision.out:1262-1281)."""
+    box = pmg.doubling_box(cycle)
+    res = {}
+    for name, dt in (("fp64_mg", pmg.F64), ("fp32_mg", pmg.F32)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = pmg.Hierarchy(box, [4, 3, 2, 1], mg_dtype=dt, cheb_degree=5, device=dev)
+        b = h.fine64.assemble_rhs(0)
+        h.estimate()
+        torch.cuda.synchronize()
+        setup = time.perf_counter() - t0
+        h.solve(b)
+        times, info = [], None
+        for _ in range(repeats):
+            x = h.fine64.initialize_dof_vector()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            x, info = h.solve(b, x=x)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) * 1e-3)
+        res[name] = {"seconds": float(np.median(times)), "iterations": info["iterations"],
+                     "reduction_per_step": info["reduction_per_step"], "setup_seconds": setup}
+        n = h.fine64.m()
+        del h, b, x
+        torch.cuda.empty_cache()
+    res["n_dofs"] = n
+    res["reference_gh200"] = {"fp64_mg_seconds": 0.5695, "fp32_mg_seconds": 0.4902, "iterations": 5,
+                              "fp64_mg_setup_seconds": 129.87, "fp32_mg_setup_seconds": 194.33}
+    res["speedup_vs_reference"] = {"fp64_mg": 0.5695 / res["fp64_mg"]["seconds"],
+                                   "fp32_mg": 0.4902 / res["fp32_mg"]["seconds"]}
+    res["config"] = "Q4 doubling mesh cycle 20, p 4-3-2-1 + Q1 h-levels, Chebyshev(5), CG to 1e-9"
+    return res
+
+
 def dg_time_to_solution(torch, pmg, dev, refine=6, repeats=3):
     """DG-SIPG Q3 on 64^3 Cartesian cells (16,777,216 DoFs), penalty 2 (p+1)^2 / h,
     u = exp(x) sin(pi y) cos(pi z) with the Dirichlet data imposed weakly; multigrid
@@ -472,6 +515,7 @@ def gpu_arm(args):
         torch.cuda.empty_cache()
         tts = time_to_solution(torch, pmg, dev)
         extra["dg_time_to_1e-10"] = dg_time_to_solution(torch, pmg, dev)
+        extra["reference_problem"] = reference_problem(torch, pmg, dev)
         extra["adjoint_gradient"] = adjoint_check(torch, pmg, dev)
 
     cpu = None
