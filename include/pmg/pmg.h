@@ -170,6 +170,14 @@ pmg_status pmg_operator_set_coefficient(pmg_operator *op, const double *coeff_qp
  * src refined at least as often; log(coefficient) is interpolated by the tensor Lagrange
  * polynomial through src's Gauss points of the containing cell, so values stay positive. */
 pmg_status pmg_operator_interpolate_coefficient(pmg_operator *dst, pmg_operator *src, void *stream);
+/* ||u_h - u||_{L2(Omega)} of the FE function with DoF values u (the operator's dtype, every DoF
+ * counted, Dirichlet ones included) against the exact solution of the manufactured problems of
+ * pmg_operator_assemble_rhs: exact_kind 1: u = sin(pi x) sin(pi y) sin(pi z) (f_kind 1),
+ * exact_kind 2: u = exp(x) sin(pi y) cos(pi z) (f_kind 2); an nq-point Gauss rule per direction
+ * (nq <= 0: degree + 2), evaluated on the GPU with a deterministic sum.  Replaces the host
+ * FEValues error loop of tests/poisson_cube_bk3/program.cc.  Synchronises. */
+pmg_status pmg_operator_l2_error(const pmg_operator *op, const void *u, int32_t exact_kind, int32_t nq,
+                                 double *error, void *stream);
 /* Quadrature points of the operator's Gauss rule, device array xq[C][nq^3][3] (FP64). */
 pmg_status pmg_operator_quadrature_points(const pmg_operator *op, double *xq, void *stream);
 /* out[c][q] = alpha * grad u(x_q)^T kappa_q |det J| w_q J^{-1} J^{-T} grad v(x_q) in reference

@@ -284,6 +284,16 @@ pmg_status pmg_operator_interpolate_coefficient(pmg_operator *dst, pmg_operator 
   });
 }
 
+pmg_status pmg_operator_l2_error(const pmg_operator *op, const void *u, int32_t exact_kind, int32_t nq,
+                                 double *error, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(u);
+    NEED(error);
+    *error = pmg::operator_l2_error(*op, u, exact_kind, nq, as_stream(stream));
+  });
+}
+
 pmg_status pmg_operator_quadrature_points(const pmg_operator *op, double *xq, void *stream) {
   return guarded(__func__, [&] {
     NEED(op);

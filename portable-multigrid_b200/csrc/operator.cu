@@ -6,6 +6,7 @@
 #include "laplace_kernels.cuh"
 #include "dg.hpp"
 #include "fields.hpp"
+#include "vector_ops.hpp"
 #include "pmg_internal.hpp"
 
 namespace pmg {
@@ -49,14 +50,18 @@ __device__ __forceinline__ double coefficient(int kind, const double x[3]) {
 // mode 1: write coef * (per-point factor) into the affine coefficient layout;
 // mode 2: right-hand side, b_i += sum_q phi_i(x_q) f(x_q) |det J| w_q (atomic);
 // mode 3: the quadrature points, out[cell][q][3];
-// mode 4: coef * |det J| w_q into the affine coefficient layout (mass-matrix weights).
+// mode 4: coef * |det J| w_q into the affine coefficient layout (mass-matrix weights);
+// mode 5: out[cell] = (sum_q (u_h(x_q) - u(x_q))^2 |det J| w_q)^(1/2) for the exact solution
+//         u of f_kind 1 (sin(pi x) sin(pi y) sin(pi z)) or 2 (exp(x) sin(pi y) cos(pi z)).
 template <typename T>
 __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restrict__ cell_xyz,
                                      int64_t n_cells, int mode, int coeff_kind,
                                      const double *__restrict__ coef_values,
                                      T *__restrict__ out, const uint32_t *__restrict__ idx_perm,
-                                     int f_kind) {
+                                     int f_kind, const void *__restrict__ uvec = nullptr,
+                                     const uint32_t *__restrict__ plain = nullptr, int u_f32 = 0) {
   __shared__ double X[3][kMaxNm * kMaxNm * kMaxNm];
+  __shared__ double U[kMaxNm * kMaxNm * kMaxNm]; // mode 5: the cell's nodal values
   __shared__ double fq[kMaxNq * kMaxNq * kMaxNq];
   const int nm = g.nm, nq = g.nq, nm3 = nm * nm * nm, nq3 = nq * nq * nq;
   for (int64_t c = blockIdx.x; c < n_cells; c += gridDim.x) {
@@ -70,11 +75,15 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
       X[0][l] = xp[0];
       X[1][l] = xp[1];
       X[2][l] = xp[2];
+      if (mode == 5) {
+        const uint32_t d = plain[c * nm3 + l];
+        U[l] = u_f32 ? (double)static_cast<const float *>(uvec)[d] : static_cast<const double *>(uvec)[d];
+      }
     }
     __syncthreads();
     for (int q = threadIdx.x; q < nq3; q += blockDim.x) {
       const int q0 = q % nq, q1 = (q / nq) % nq, q2 = q / (nq * nq);
-      double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, xq[3] = {0, 0, 0};
+      double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, xq[3] = {0, 0, 0}, uh = 0.0;
       for (int k = 0; k < nm; ++k)
         for (int j = 0; j < nm; ++j) {
           const double sj = g.S[j * nq + q1], dj = g.SD[j * nq + q1];
@@ -83,6 +92,7 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
             const int l = (k * nm + j) * nm + i;
             const double si = g.S[i * nq + q0], di = g.SD[i * nq + q0];
             const double v = si * sj * sk, g0 = di * sj * sk, g1 = si * dj * sk, g2 = si * sj * dk;
+            if (mode == 5) uh += U[l] * v;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
               const double xv = X[d][l];
@@ -130,6 +140,11 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
         for (int d = 0; d < 3; ++d) out[(c * nq3 + q) * 3 + d] = (T)xq[d];
       } else if (mode == 4) {
         out[(grp * (g.N * g.N) + m_row) * g.lanes + lane] = (T)(fabs(det) * wq * kap);
+      } else if (mode == 5) {
+        double ex = 0.0;
+        if (f_kind == 1) ex = sin(M_PI * xq[0]) * sin(M_PI * xq[1]) * sin(M_PI * xq[2]);
+        if (f_kind == 2) ex = exp(xq[0]) * sin(M_PI * xq[1]) * cos(M_PI * xq[2]);
+        fq[q] = (uh - ex) * (uh - ex) * fabs(det) * wq;
       } else {
         double f = 1.0;
         if (f_kind == 1) f = 3.0 * M_PI * M_PI * sin(M_PI * xq[0]) * sin(M_PI * xq[1]) * sin(M_PI * xq[2]);
@@ -138,6 +153,11 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
       }
     }
     __syncthreads();
+    if (mode == 5 && threadIdx.x == 0) { // fixed summation order: deterministic
+      double e = 0.0;
+      for (int q = 0; q < nq3; ++q) e += fq[q];
+      out[c] = (T)sqrt(e);
+    }
     if (mode == 2) {
       for (int l = threadIdx.x; l < nm3; l += blockDim.x) {
         const int i = l % nm, j = (l / nm) % nm, k = l / (nm * nm);
@@ -639,6 +659,27 @@ void operator_qp_form(const pmg_operator &op, const void *u, const void *v, doub
   if (op.n_cells == 0) return;
   prof::Scope scope("qp_form", s);
   qp_form_cells(op, u, v, alpha, out, s);
+}
+
+// ||u_h - u||_{L2} with an nq-point Gauss rule per direction; every DoF's value counts,
+// Dirichlet ones included (the plain index map is uploaded for the call).
+double operator_l2_error(const pmg_operator &op, const void *u, int exact_kind, int nq, cudaStream_t s) {
+  PMG_REQUIRE(u, "null vector");
+  PMG_REQUIRE(exact_kind == 1 || exact_kind == 2, "exact_kind must be 1 (sine) or 2 (exp-sine-cosine)");
+  if (nq <= 0) nq = op.nq + 1;
+  PMG_REQUIRE(nq >= 1 && nq <= kMaxNq, "nq must be in [1,8]");
+  PMG_CUDA(cudaSetDevice(op.device));
+  if (op.n_cells == 0) return 0.0;
+  DeviceBuffer plain = upload(op.num.plain);
+  DeviceBuffer cell_err(sizeof(double) * op.n_cells);
+  const GeoParams gp = make_geo_params(op, nq);
+  const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)op.sms * 16);
+  cell_geometry_kernel<double><<<grid, 128, 0, s>>>(gp, op.cell_xyz.as<int32_t>(), op.n_cells, 5, 0, nullptr,
+                                                    cell_err.as<double>(), nullptr, exact_kind, u,
+                                                    plain.as<uint32_t>(), op.dtype == PMG_F32 ? 1 : 0);
+  PMG_LAUNCH_CHECK();
+  const double e2 = vec::dot(cell_err.get(), cell_err.get(), PMG_F64, op.n_cells, s); // synchronises
+  return std::sqrt(e2);
 }
 
 } // namespace pmg

@@ -156,6 +156,7 @@ def _declare(L):
         "pmg_operator_set_coefficient": ([vp, vp, i32, vp], i32),
         "pmg_operator_interpolate_coefficient": ([vp, vp, vp], i32),
         "pmg_operator_quadrature_points": ([vp, vp, vp], i32),
+        "pmg_operator_l2_error": ([vp, vp, i32, i32, P(d), vp], i32),
         "pmg_operator_qp_form": ([vp, vp, vp, d, vp, vp], i32),
         "pmg_mg_set_coefficient": ([vp, vp, vp, i32, vp], i32),
         "pmg_adjoint_gradient": ([vp, vp, vp, vp, vp, vp, vp, P(d), d, d, i32, P(CGInfo), vp], i32),
@@ -363,6 +364,12 @@ class LaplaceOperator:
     def interpolate_coefficient(self, src: "LaplaceOperator"):
         """This operator's coefficient := src's coefficient field at this operator's points."""
         check(lib().pmg_operator_interpolate_coefficient(self.h, src.h, _stream()))
+
+    def l2_error(self, u, exact_kind, nq=0):
+        """||u_h - u||_L2 against the manufactured solution exact_kind (1: sine, 2: exp-sine-cosine)."""
+        e = C.c_double()
+        check(lib().pmg_operator_l2_error(self.h, _ptr(u), exact_kind, nq, C.byref(e), _stream()))
+        return e.value
 
     def quadrature_points(self):
         """Gauss points of every cell, float64 CUDA tensor [C, nq^3, 3]."""

@@ -113,3 +113,18 @@ def test_dg_multigrid_solve_matches_oracle(oracle, mg_dtype):
     assert abs(info["iterations"] - info_o.iterations) <= (0 if mg_dtype == pmg.F64 else 1)
     assert rel_err(x.cpu().numpy(), x_o) < 1e-7
     assert abs(oracle.dg_l2_error(ob, p, p + 2, x.cpu().numpy()) / info_o.l2_error - 1) < 1e-6
+
+
+@pytest.mark.parametrize("p", [1, 3, 4])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+def test_dg_l2_error_matches_oracle(oracle, p, dtype):
+    """||u_h - exp(x) sin(pi y) cos(pi z)||_L2 of a DG function on the GPU against the oracle."""
+    box = pmg.Box.make(coarse=(3, 2, 1), refine=1, hi=(3.0, 2.0, 0.5))
+    ob = obox(oracle, box)
+    op = pmg.DGLaplaceOperator(pmg.Mesh(box), p, dtype)
+    u = np.random.default_rng(3).uniform(-1, 1, op.m())
+    ut = torch.tensor(u, dtype=torch.float64 if dtype == pmg.F64 else torch.float32, device="cuda")
+    u_used = ut.double().cpu().numpy()
+    got = op.l2_error(ut, 2, p + 2)
+    want = oracle.dg_l2_error(ob, p, p + 2, u_used)
+    assert abs(got - want) <= 1e-12 * want

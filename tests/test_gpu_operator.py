@@ -165,3 +165,22 @@ def test_invalid_arguments_raise():
     v = op.initialize_dof_vector()
     with pytest.raises(pmg.PmgError):
         op.vmult(v, v)  # aliasing is rejected
+
+
+@pytest.mark.parametrize("degree", [1, 2, 4, 6])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+@pytest.mark.parametrize("boxname", ["unit_r2", "deformed_r2", "ragged_3x2x1"])
+def test_l2_error_matches_oracle(oracle, degree, dtype, boxname):
+    """||u_h - sin sin sin||_L2 on the GPU against the oracle's host loop, every DoF's value
+    counted (Dirichlet ones included)."""
+    box = pmg.Box.make(**BOXES[boxname])
+    ob = obox(oracle, box)
+    op = pmg.LaplaceOperator(pmg.Mesh(box), degree, dtype)
+    plain, cons, idx = oracle.dofs(ob, degree)
+    u = random_src(op.m(), 7)
+    ut = torch.tensor(u, dtype=tdtype(dtype), device="cuda")
+    u_used = ut.double().cpu().numpy()  # the values the GPU sees (rounded in FP32)
+    for nq in (degree + 1, degree + 2):
+        got = op.l2_error(ut, 1, nq)
+        want = oracle.l2_error_sine(ob, degree, nq, plain, u_used)
+        assert abs(got - want) <= 1e-12 * want
