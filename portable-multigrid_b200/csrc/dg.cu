@@ -46,6 +46,39 @@ template <int N> __device__ __forceinline__ int face_node(int d, int layer, int 
   return (k * N + j) * N + i;
 }
 
+// flux values of face F (compile time, so the node indexing folds to constants) at face point
+// (a, bb) of cell c: f1 = sigma [u] - {d_n u}, f2 = -[u]/2 (Dirichlet: mirror u+ = -u-)
+template <int N, typename T, int F>
+__device__ __forceinline__ void face_flux(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ src,
+                                          const int32_t *__restrict__ nbr, int64_t c, int a, int bb, T sgn_h,
+                                          T sigma, T &f1, T &f2) {
+  constexpr int N3 = N * N * N, d = F >> 1, sd = F & 1;
+  constexpr int own_layer = sd ? N - 1 : 0, nb_layer = sd ? 0 : N - 1;
+  const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
+  const T *dphi_nb = sd ? tab.dphi0 : tab.dphi1;
+  const T *uo = src + c * N3;
+  const T vo = __ldg(uo + face_node<N>(d, own_layer, a, bb));
+  T dn = T(0);
+#pragma unroll
+  for (int i = 0; i < N; ++i) dn += dphi_own[i] * __ldg(uo + face_node<N>(d, i, a, bb));
+  dn *= sgn_h;
+  const int32_t nb = __ldg(nbr + c * 6 + F);
+  if (nb >= 0) {
+    const T *un = src + int64_t(nb) * N3;
+    const T vn = __ldg(un + face_node<N>(d, nb_layer, a, bb));
+    T dnn = T(0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * __ldg(un + face_node<N>(d, i, a, bb));
+    dnn *= sgn_h;
+    const T jump = vo - vn;
+    f1 = sigma * jump - T(0.5) * (dn + dnn);
+    f2 = T(-0.5) * jump;
+  } else if ((geo.dirichlet >> F) & 1) {
+    f1 = sigma * T(2) * vo - dn;
+    f2 = -vo;
+  }
+}
+
 // cells per block: six faces x N^2 face points per cell, about 384 threads per block
 template <int N> constexpr int dg_batch() { return (384 / (6 * N * N)) > 0 ? 384 / (6 * N * N) : 1; }
 template <int N> constexpr int dg_threads() { return ((6 * dg_batch<N>() * N * N + 31) / 32) * 32; }
@@ -77,35 +110,20 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
   const T sgn_h = t < FP ? (sd ? T(1) : T(-1)) / (T)geo.h[d] : T(0); // n . grad = sgn_h d/dxi_d
   const T area = t < FP ? (T)(geo.h[ta] * geo.h[tb]) : T(0);
   const T sigma = t < FP ? (T)(geo.c_pen / geo.h[d]) : T(0);
-  const bool bc_dirichlet = t < FP && ((geo.dirichlet >> f) & 1);
   for (int64_t base = int64_t(blockIdx.x) * B; base < n_cells; base += int64_t(gridDim.x) * B) {
     if (t < FP) {
       const int64_t c = base + b;
       T f1 = T(0), f2 = T(0);
       if (c < n_cells) {
-        const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
-        const T *dphi_nb = sd ? tab.dphi0 : tab.dphi1;
-        const int own_layer = sd ? N - 1 : 0, nb_layer = sd ? 0 : N - 1;
-        const T *uo = src + c * N3;
-        const T vo = __ldg(uo + face_node<N>(d, own_layer, a, bb));
-        T dn = T(0);
-#pragma unroll
-        for (int i = 0; i < N; ++i) dn += dphi_own[i] * __ldg(uo + face_node<N>(d, i, a, bb));
-        dn *= sgn_h;
-        const int32_t nb = nbr[c * 6 + f];
-        if (nb >= 0) {
-          const T *un = src + int64_t(nb) * N3;
-          const T vn = __ldg(un + face_node<N>(d, nb_layer, a, bb));
-          T dnn = T(0);
-#pragma unroll
-          for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * __ldg(un + face_node<N>(d, i, a, bb));
-          dnn *= sgn_h;
-          const T jump = vo - vn;
-          f1 = sigma * jump - T(0.5) * (dn + dnn);
-          f2 = T(-0.5) * jump;
-        } else if (bc_dirichlet) { // mirror: u+ = -u-, d_n u+ = d_n u-
-          f1 = sigma * T(2) * vo - dn;
-          f2 = -vo;
+        // f is uniform over a warp where B * N^2 is a multiple of 32 (N = 2, 4); elsewhere a
+        // warp can span two faces and takes both branches
+        switch (f) {
+        case 0: face_flux<N, T, 0>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 1: face_flux<N, T, 1>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 2: face_flux<N, T, 2>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 3: face_flux<N, T, 3>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 4: face_flux<N, T, 4>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        default: face_flux<N, T, 5>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
         }
       }
       F1[f][b][ab] = f1 * area;
