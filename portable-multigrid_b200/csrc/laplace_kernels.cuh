@@ -245,7 +245,7 @@ template <int N, typename T, bool SMEM_G, int PIPE = 0> struct SlabSmem {
 // SMEM_G: the x columns of each group's geometry (contiguous chunks) stream through a
 // two-slot shared-memory ring; the copy of the next column (or of the next group's first
 // column) is issued when a column starts, so it overlaps with that column's work.
-// Launched with one warp per block.
+// Warps share nothing (each has its own ring, barriers and buffers): any warps per block.
 // PIPE: the dependent index -> src gather is taken off the critical path by per-thread
 // cp.async copies one group ahead (each lane copies exactly the entries it later reads, so
 // cp.async.wait_group alone orders them):
@@ -254,7 +254,7 @@ template <int N, typename T, bool SMEM_G, int PIPE = 0> struct SlabSmem {
 //      the current group's first phase, from an index block copied a group earlier still;
 //      the scatter reads its indices from shared memory as well.
 template <int N, typename T, int GEOM, bool SMEM_G, int PIPE = 0>
-__global__ void __launch_bounds__(SMEM_G ? 32 : 128, (SMEM_G ? 8 : MinBlocks<N, T, GEOM>::value))
+__global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N, T, GEOM>::value))
     vmult_slab_kernel(const __grid_constant__ Tab<N, T> tab, const T *__restrict__ src, T *__restrict__ dst,
                       const uint32_t *__restrict__ idx, const T *__restrict__ geo,
                       const T *__restrict__ coef, int64_t n_groups, unsigned int *err) {

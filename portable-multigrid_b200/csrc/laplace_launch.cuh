@@ -110,32 +110,72 @@ template <typename T, int GEOM, bool SG> int use_pipe() {
   return 0;
 }
 
-template <typename T, int GEOM, bool SG, int PIPE> int occ_vmult_variant();
+
+// Block shape of a vmult variant on the current device: warps per block and resident warps
+// per SM.  The direct variant keeps vmult_wpb(); the ring variant, whose warps share nothing,
+// takes the block size (1..8 warps) that fits the most warps per SM -- the per-block
+// shared-memory reservation can leave room for one more warp in one large block than in
+// one-warp blocks (Q4 FP64: 7 against 6).  PMG_RING_WPB=1..8 fixes it (a tuning switch).
+struct VmultShape {
+  int wpb = 1, warps_per_sm = 1;
+};
+inline int ring_wpb_override() {
+  static const int v = [] {
+    const char *e = std::getenv("PMG_RING_WPB");
+    return e ? std::atoi(e) : 0;
+  }();
+  return v;
+}
+template <typename T, int GEOM, bool SG, int PIPE> VmultShape vmult_shape() {
+  static std::mutex mu;
+  static std::map<int, VmultShape> cache; // device -> shape
+  int dev = 0;
+  PMG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
+  constexpr size_t per_warp = kern::SlabSmem<kN, T, SG, PIPE>::PER_WARP;
+  VmultShape best;
+  if (!SG) {
+    best.wpb = vmult_wpb<T, SG, PIPE>();
+    PMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(best.wpb * per_warp)));
+    int nb = 0;
+    PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * best.wpb, best.wpb * per_warp));
+    best.warps_per_sm = std::max(1, nb * best.wpb);
+  } else {
+    int max_smem = 0;
+    PMG_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const int hi = (int)std::min<size_t>(8, std::max<size_t>(1, (size_t)max_smem / per_warp));
+    PMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(hi * per_warp)));
+    const int o = ring_wpb_override();
+    best.warps_per_sm = 0;
+    for (int w = 1; w <= hi; ++w) {
+      if (o >= 1 && o <= hi && w != o) continue;
+      int nb = 0;
+      PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * w, w * per_warp));
+      if (nb * w > best.warps_per_sm) {
+        best.wpb = w;
+        best.warps_per_sm = nb * w;
+      }
+    }
+    best.warps_per_sm = std::max(1, best.warps_per_sm);
+  }
+  cache.emplace(dev, best);
+  return best;
+}
 
 template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabLaunch &L) {
   auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
-  allow_smem(k, vmult_smem<T, SG, PIPE>());
-  constexpr int wpb = vmult_wpb<T, SG, PIPE>();
-  const int64_t want = (L.n_groups + wpb - 1) / wpb;
-  // resident warps: the operator caches the PIPE 0 figures; other depths are computed here
-  int64_t resident = SG ? L.resident_warps_ring : L.resident_warps;
-  if (PIPE != 0) {
-    int dev = 0, sms = 0;
-    PMG_CUDA(cudaGetDevice(&dev));
-    PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    static std::mutex mu;
-    static std::map<int, int> per_sm; // device -> resident warps per SM
-    int w = 0;
-    {
-      std::lock_guard<std::mutex> lock(mu);
-      auto it = per_sm.find(dev);
-      if (it == per_sm.end()) it = per_sm.emplace(dev, occ_vmult_variant<T, GEOM, SG, PIPE>()).first;
-      w = it->second;
-    }
-    resident = (int64_t)std::max(1, w) * sms;
-  }
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, resident / wpb));
-  k<<<grid, 32 * wpb, vmult_smem<T, SG, PIPE>(), L.stream>>>(
+  const VmultShape sh = vmult_shape<T, GEOM, SG, PIPE>();
+  int sms = 0, dev = 0;
+  PMG_CUDA(cudaGetDevice(&dev));
+  PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int64_t want = (L.n_groups + sh.wpb - 1) / sh.wpb;
+  const int64_t resident_blocks = (int64_t)sh.warps_per_sm * sms / sh.wpb;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, resident_blocks));
+  const size_t smem = (size_t)sh.wpb * kern::SlabSmem<kN, T, SG, PIPE>::PER_WARP;
+  k<<<grid, 32 * sh.wpb, smem, L.stream>>>(
       make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
       static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err);
   PMG_LAUNCH_CHECK();
@@ -185,12 +225,7 @@ template <typename T> void diag_type(const SlabLaunch &L) {
 }
 
 template <typename T, int GEOM, bool SG, int PIPE> int occ_vmult_variant() {
-  auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
-  allow_smem(k, vmult_smem<T, SG, PIPE>());
-  int nb = 0;
-  constexpr int wpb = vmult_wpb<T, SG, PIPE>();
-  PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * wpb, vmult_smem<T, SG, PIPE>()));
-  return nb * wpb; // resident warps per SM
+  return vmult_shape<T, GEOM, SG, PIPE>().warps_per_sm; // resident warps per SM
 }
 // resident warps per SM of the direct variant (low 16 bits) and of the ring variant (high)
 template <typename T, int GEOM> int occ_vmult() {
