@@ -78,7 +78,15 @@ void chebyshev_estimate(pmg_chebyshev &c, cudaStream_t s) {
   const int dt = op.dtype;
   const int64_t N = op.n_dofs;
   const size_t bytes = dtype_size(dt) * N;
-  DeviceBuffer x(bytes), r(bytes), z(bytes), p(bytes), v(bytes);
+  // work vectors: temporary for a first estimate; a smoother that is estimated again (new
+  // coefficients) keeps them, so repeated estimates allocate nothing
+  std::vector<DeviceBuffer> tmp;
+  std::vector<DeviceBuffer> &w = c.generation > 0 ? c.est_work : tmp;
+  if (w.size() != 5 || w[0].bytes() != bytes) {
+    w.clear();
+    for (int i = 0; i < 5; ++i) w.emplace_back(bytes);
+  }
+  DeviceBuffer &x = w[0], &r = w[1], &z = w[2], &p = w[3], &v = w[4];
   PMG_CUDA(cudaMemsetAsync(x.get(), 0, bytes, s));
   vec::fill_mod11(r.get(), dt, N, s);
   std::vector<double> diag, offd;

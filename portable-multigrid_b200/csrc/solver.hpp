@@ -16,6 +16,7 @@ struct pmg_chebyshev {
   double theta = 1, delta = 0, min_ev = 1, max_ev = 1;
   int cg_its = 0;
   pmg::DeviceBuffer xo, Ax;
+  std::vector<pmg::DeviceBuffer> est_work; // eigenvalue-estimate vectors kept once re-estimated
 };
 
 struct pmg_mg {
