@@ -73,10 +73,10 @@ template <typename K> void allow_smem(K kernel, size_t bytes) {
   done.insert(key);
 }
 
-// Full geometry streams through the shared-memory column ring (TMA) except where direct
-// loads measured faster on B200 (deformed-cube sweeps at 64^3/128^3): FP32 degree 4, whose
-// register-heavy unrolled form already hides the latency at 8 warps/SM, and degree 6 in
-// both types.
+// Full geometry streams through the shared-memory column ring (TMA) where that measured faster
+// on B200 (deformed-cube sweeps at 64^3/128^3): FP64 degrees 1-5 and FP32 degrees 2-3; FP32
+// degrees 1, 4, 5, 6 (whose register-heavy unrolled forms hide the latency at 8 warps/SM) and
+// FP64 degree 6 load it directly.
 // PMG_VMULT_STAGE=0 / 1 forces direct loads / the ring (a tuning switch; both are compiled).
 inline int stage_override() {
   static const int v = [] {
@@ -88,7 +88,7 @@ inline int stage_override() {
 template <typename T> bool use_ring() {
   const int o = stage_override();
   if (o == 0 || o == 1) return o == 1;
-  return !((sizeof(T) == 4 && kN == 5) || kN == 7);
+  return sizeof(T) == 8 ? kN != 7 : (kN == 3 || kN == 4);
 }
 // gather pipeline depth (PIPE template parameter); PMG_VMULT_PIPE=0/1/2 overrides
 inline int pipe_override() {
