@@ -22,6 +22,7 @@ template <int N, typename T> kern::Tab<N, T> tab_of(const Tables1D &t) {
     k.D[a] = (T)t.D[a];
   }
   for (int a = 0; a < N; ++a) k.W[a] = (T)t.W[a];
+  kern::fill_even_odd(k, t.S.data(), t.SD.data());
   return k;
 }
 

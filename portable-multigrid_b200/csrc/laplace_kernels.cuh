@@ -36,12 +36,78 @@ namespace kern {
 
 constexpr uint32_t kInvalidIdx = 0xFFFFFFFFu;
 
+// Even/odd form of a 1D apply out_q = sum_i M(i, q) in_i for a matrix with the mirror
+// symmetry M(N-1-i, N-1-q) = SIG M(i, q) (SIG = +1: S and its transpose; -1: SD and its
+// transpose, from the symmetric GLL nodes and Gauss points): with e_i = in_i + in_{N-1-i},
+// o_i = in_i - in_{N-1-i} (i < H = N/2) and E_q = sum_i A(i,q) e_i + C(q) in_H (odd N),
+// O_q = sum_i B(i,q) o_i, out_q = E_q + O_q and out_{N-1-q} = SIG (E_q - O_q): about half
+// the multiply-adds of the plain product.  A = (M(i,q) + M(N-1-i,q))/2, B = (M(i,q) -
+// M(N-1-i,q))/2, C(q) = M(H,q), for q < Q = (N+1)/2.
+template <int N, typename T> struct EvenOdd {
+  static constexpr int H = N / 2, Q = (N + 1) / 2;
+  T A[H * Q > 0 ? H * Q : 1], B[H * Q > 0 ? H * Q : 1], C[Q];
+};
+
 template <int N, typename T> struct Tab {
   T S[N * N];  // S[i*N+q]  = phi_i(g_q)
   T SD[N * N]; // SD[i*N+q] = phi_i'(g_q)
   T D[N * N];  // D[n*N+q]  = l_n'(g_q) on the Gauss points
   T W[N];      // Gauss weights
+  EvenOdd<N, T> eS, eSD;   // S and SD (input node i, output point q)
+  EvenOdd<N, T> eST, eSDT; // their transposes (input point q, output node i)
 };
+
+// fill the even/odd tables of `tab` from the row-major N x N tables S and SD (host)
+template <int N, typename T> inline void fill_even_odd(Tab<N, T> &tab, const double *S, const double *SD) {
+  constexpr int H = N / 2, Q = (N + 1) / 2;
+  auto fill = [&](EvenOdd<N, T> &e, auto M) {
+    for (int i = 0; i < H; ++i)
+      for (int q = 0; q < Q; ++q) {
+        e.A[i * Q + q] = (T)(0.5 * (M(i, q) + M(N - 1 - i, q)));
+        e.B[i * Q + q] = (T)(0.5 * (M(i, q) - M(N - 1 - i, q)));
+      }
+    for (int q = 0; q < Q; ++q) e.C[q] = (N & 1) ? (T)M(H, q) : T(0);
+  };
+  fill(tab.eS, [&](int i, int q) { return S[i * N + q]; });
+  fill(tab.eSD, [&](int i, int q) { return SD[i * N + q]; });
+  fill(tab.eST, [&](int r, int k) { return S[k * N + r]; });
+  fill(tab.eSDT, [&](int r, int k) { return SD[k * N + r]; });
+}
+
+// out_q = sum_i M(i, q) in_i by the even/odd form; f(q, out_q) is called once for every q
+template <int N, typename T, int SIG, typename F>
+__device__ __forceinline__ void eo_apply(const EvenOdd<N, T> &m, const T (&in)[N], F &&f) {
+  constexpr int H = N / 2, Q = (N + 1) / 2;
+  T e[H > 0 ? H : 1], o[H > 0 ? H : 1];
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    e[i] = in[i] + in[N - 1 - i];
+    o[i] = in[i] - in[N - 1 - i];
+  }
+#pragma unroll
+  for (int q = 0; q < H; ++q) {
+    T E = (N & 1) ? m.C[q] * in[H] : T(0), O = T(0);
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      E = fma(m.A[i * Q + q], e[i], E);
+      O = fma(m.B[i * Q + q], o[i], O);
+    }
+    f(q, E + O);
+    f(N - 1 - q, SIG > 0 ? E - O : O - E);
+  }
+  if (N & 1) {
+    T v = T(0);
+    if (SIG > 0) {
+      v = m.C[H] * in[H];
+#pragma unroll
+      for (int i = 0; i < H; ++i) v = fma(m.A[i * Q + H], e[i], v);
+    } else {
+#pragma unroll
+      for (int i = 0; i < H; ++i) v = fma(m.B[i * Q + H], o[i], v);
+    }
+    f(H, v);
+  }
+}
 
 // squared tables for the diagonal: S2 = S*S, SS = S*SD, D2 = SD*SD (elementwise)
 template <int N, typename T> struct Tab2 {
@@ -263,6 +329,12 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   constexpr int CS = Stride<N>::CELL;
   constexpr unsigned MASK = Lo::MASK;
   constexpr int UNR = SMEM_G ? N : Unroll<N, T, GEOM>::value;
+  // even/odd contractions in phases 1 and 3 where they measured faster on B200: the ring
+  // variants and the FP32 direct variants other than N = 6 and N = 7 full geometry (FP64 Q5
+  // ring +17 %, Q4 ring +3 %, FP32 Q6 affine +4 %); the FP64 runtime-loop variants spill with
+  // them (FP64 Q6 direct -25..40 %); N = 2 gains nothing
+  constexpr bool EO =
+      N >= 3 && (SMEM_G || (sizeof(T) == 4 && N != 6 && !(N == 7 && GEOM == 0)));
   using SM = SlabSmem<N, T, SMEM_G, PIPE>;
   static_assert(!(SMEM_G && PIPE == 2), "src staging is not combined with the geometry ring");
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -374,19 +446,26 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
           t[k] = a;
           tx[k] = b;
         }
+        // z contraction: w = Sz t, wz = SDz t, wx = Sz tx at (z = r, y = s, x = p)
+        if constexpr (EO) {
+          eo_apply<N, T, 1>(tab.eS, t, [&](int r, T v) { bufW[(r * N + s) * N + p] = v; });
+          eo_apply<N, T, -1>(tab.eSD, t, [&](int r, T v) { bufZ[(r * N + s) * N + p] = v; });
+          eo_apply<N, T, 1>(tab.eS, tx, [&](int r, T v) { bufX[(r * N + s) * N + p] = v; });
+        } else {
 #pragma unroll
-        for (int r = 0; r < N; ++r) {
-          T w = T(0), wz = T(0), wx = T(0);
+          for (int r = 0; r < N; ++r) {
+            T w = T(0), wz = T(0), wx = T(0);
 #pragma unroll
-          for (int k = 0; k < N; ++k) {
-            w = fma(tab.S[k * N + r], t[k], w);
-            wz = fma(tab.SD[k * N + r], t[k], wz);
-            wx = fma(tab.S[k * N + r], tx[k], wx);
+            for (int k = 0; k < N; ++k) {
+              w = fma(tab.S[k * N + r], t[k], w);
+              wz = fma(tab.SD[k * N + r], t[k], wz);
+              wx = fma(tab.S[k * N + r], tx[k], wx);
+            }
+            const int o = (r * N + s) * N + p;
+            bufW[o] = w;
+            bufZ[o] = wz;
+            bufX[o] = wx;
           }
-          const int o = (r * N + s) * N + p;
-          bufW[o] = w;
-          bufZ[o] = wz;
-          bufX[o] = wx;
         }
       }
     }
@@ -528,17 +607,27 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
         A[r] = bufW[(r * N + s) * N + i];
         Cc[r] = bufZ[(r * N + s) * N + i];
       }
+      // out = Sz^T a + SDz^T c
+      T v[N];
+      if constexpr (EO) {
+        eo_apply<N, T, 1>(tab.eST, A, [&](int k, T x) { v[k] = x; });
+        eo_apply<N, T, -1>(tab.eSDT, Cc, [&](int k, T x) { v[k] += x; });
+      } else {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          v[k] = T(0);
+#pragma unroll
+          for (int r = 0; r < N; ++r) {
+            v[k] = fma(tab.S[k * N + r], A[r], v[k]);
+            v[k] = fma(tab.SD[k * N + r], Cc[r], v[k]);
+          }
+        }
+      }
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        T v = T(0);
-#pragma unroll
-        for (int r = 0; r < N; ++r) {
-          v = fma(tab.S[k * N + r], A[r], v);
-          v = fma(tab.SD[k * N + r], Cc[r], v);
-        }
         const uint32_t id = PIPE == 2 ? ibuf[(slot * N2 + k * N + i) * LANES]
                                       : ld_stream(ig + (k * N + i) * LANES, pol_first);
-        if (id != kInvalidIdx) red_keep(dst + id, v, pol_last);
+        if (id != kInvalidIdx) red_keep(dst + id, v[k], pol_last);
       }
     }
     if (PIPE == 2) issue_idx(g + 2 * nwarps, slot); // this group's index slot is free

@@ -33,6 +33,7 @@ template <typename T> kern::Tab<kN, T> make_tab(const SlabLaunch &L) {
     t.D[a] = (T)L.D[a];
   }
   for (int a = 0; a < kN; ++a) t.W[a] = (T)L.W[a];
+  kern::fill_even_odd(t, L.S, L.SD);
   return t;
 }
 
