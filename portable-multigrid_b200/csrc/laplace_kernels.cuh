@@ -250,6 +250,13 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
 //   phase 3 (Y-slab), per x node i:        out = Sz^T a + SDz^T c, scatter
 // Each lane overwrites only its own slab's region of the buffers between the two
 // exchanges, so only the two exchanges (and the end of a group) need a __syncwarp.
+// compile-time overrides of the even/odd choices below (-1: the tuned default, 0: off, 1: on)
+#ifndef PMG_VMULT_EO_PHASE2
+#define PMG_VMULT_EO_PHASE2 -1
+#endif
+#ifndef PMG_VMULT_EO_PHASE1X
+#define PMG_VMULT_EO_PHASE1X -1
+#endif
 template <int N> struct Stride {
   // per-cell stride of the exchange buffers, padded where that lowers bank conflicts of
   // the two exchange patterns (offsets N*s and N*N*s within a cell)
@@ -329,12 +336,22 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   constexpr int CS = Stride<N>::CELL;
   constexpr unsigned MASK = Lo::MASK;
   constexpr int UNR = SMEM_G ? N : Unroll<N, T, GEOM>::value;
-  // even/odd contractions in phases 1 and 3 where they measured faster on B200: the ring
-  // variants and the FP32 direct variants other than N = 6 and N = 7 full geometry (FP64 Q5
-  // ring +17 %, Q4 ring +3 %, FP32 Q6 affine +4 %); the FP64 runtime-loop variants spill with
-  // them (FP64 Q6 direct -25..40 %); N = 2 gains nothing
+  // even/odd contractions where they measured faster on B200 (the FP64 runtime-loop
+  // variants spill with the extra live values; N = 2 gains nothing):
+  //  EO   z contractions of phases 1 and 3: the ring variants and the FP32 direct variants
+  //       other than N = 6 and N = 7 full geometry
+  //  EO2  phase 2 (the y contractions of the columns, the x contraction of fz): the ring
+  //       variants, FP32 N <= 5 and FP64 N = 7 full geometry
+  //  EO1X x contractions of phase 1 by mirrored pairs of points (the point loop unrolled):
+  //       with EO except at N = 6
   constexpr bool EO =
       N >= 3 && (SMEM_G || (sizeof(T) == 4 && N != 6 && !(N == 7 && GEOM == 0)));
+  constexpr bool EO2 =
+      PMG_VMULT_EO_PHASE2 >= 0
+          ? (PMG_VMULT_EO_PHASE2 == 1 && N >= 3)
+          : N >= 3 && (SMEM_G || (sizeof(T) == 4 && N <= 5) || (sizeof(T) == 8 && N == 7 && GEOM == 0));
+  constexpr bool EO1X = PMG_VMULT_EO_PHASE1X >= 0 ? (PMG_VMULT_EO_PHASE1X == 1 && EO && UNR == N)
+                                                  : (EO && UNR == N && N != 6);
   using SM = SlabSmem<N, T, SMEM_G, PIPE>;
   static_assert(!(SMEM_G && PIPE == 2), "src staging is not combined with the geometry ring");
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -432,39 +449,97 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
             u[k][i] = (id != kInvalidIdx) ? ld_keep(src + id, pol_last) : T(0);
           }
       }
-#pragma unroll UNR
-      for (int p = 0; p < N; ++p) {
-        T t[N], tx[N];
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-          T a = T(0), b = T(0);
-#pragma unroll
-          for (int i = 0; i < N; ++i) {
-            a = fma(tab.S[i * N + p], u[k][i], a);
-            b = fma(tab.SD[i * N + p], u[k][i], b);
-          }
-          t[k] = a;
-          tx[k] = b;
-        }
-        // z contraction: w = Sz t, wz = SDz t, wx = Sz tx at (z = r, y = s, x = p)
-        if constexpr (EO) {
+      if constexpr (EO1X) {
+        // x contractions t = Sx u, tx = SDx u by mirrored pairs of points (p, N-1-p): the
+        // sums and differences of mirrored nodes replace u in place (u[k][i] = e_i and
+        // u[k][N-1-i] = o_i for i < H)
+        constexpr int H = N / 2, Q = (N + 1) / 2;
+        // z contraction of one x point p in even/odd form: w = Sz t, wz = SDz t, wx = Sz tx
+        auto zstore = [&](int p, const T(&t)[N], const T(&tx)[N]) {
           eo_apply<N, T, 1>(tab.eS, t, [&](int r, T v) { bufW[(r * N + s) * N + p] = v; });
           eo_apply<N, T, -1>(tab.eSD, t, [&](int r, T v) { bufZ[(r * N + s) * N + p] = v; });
           eo_apply<N, T, 1>(tab.eS, tx, [&](int r, T v) { bufX[(r * N + s) * N + p] = v; });
-        } else {
+        };
 #pragma unroll
-          for (int r = 0; r < N; ++r) {
-            T w = T(0), wz = T(0), wx = T(0);
+        for (int k = 0; k < N; ++k)
 #pragma unroll
-            for (int k = 0; k < N; ++k) {
-              w = fma(tab.S[k * N + r], t[k], w);
-              wz = fma(tab.SD[k * N + r], t[k], wz);
-              wx = fma(tab.S[k * N + r], tx[k], wx);
+          for (int i = 0; i < H; ++i) {
+            const T a = u[k][i], b = u[k][N - 1 - i];
+            u[k][i] = a + b;
+            u[k][N - 1 - i] = a - b;
+          }
+#pragma unroll
+        for (int p = 0; p < H; ++p) {
+          T tp[N], tm[N], xp[N], xm[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            T es = (N & 1) ? tab.eS.C[p] * u[k][H] : T(0), os = T(0);
+            T ed = (N & 1) ? tab.eSD.C[p] * u[k][H] : T(0), od = T(0);
+#pragma unroll
+            for (int i = 0; i < H; ++i) {
+              es = fma(tab.eS.A[i * Q + p], u[k][i], es);
+              os = fma(tab.eS.B[i * Q + p], u[k][N - 1 - i], os);
+              ed = fma(tab.eSD.A[i * Q + p], u[k][i], ed);
+              od = fma(tab.eSD.B[i * Q + p], u[k][N - 1 - i], od);
             }
-            const int o = (r * N + s) * N + p;
-            bufW[o] = w;
-            bufZ[o] = wz;
-            bufX[o] = wx;
+            tp[k] = es + os;
+            tm[k] = es - os;
+            xp[k] = ed + od;
+            xm[k] = od - ed;
+          }
+          zstore(p, tp, xp);
+          zstore(N - 1 - p, tm, xm);
+        }
+        if (N & 1) {
+          T t[N], tx[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            T a = tab.eS.C[H] * u[k][H], b = T(0);
+#pragma unroll
+            for (int i = 0; i < H; ++i) {
+              a = fma(tab.eS.A[i * Q + H], u[k][i], a);
+              b = fma(tab.eSD.B[i * Q + H], u[k][N - 1 - i], b);
+            }
+            t[k] = a;
+            tx[k] = b;
+          }
+          zstore(H, t, tx);
+        }
+      } else {
+#pragma unroll UNR
+        for (int p = 0; p < N; ++p) {
+          T t[N], tx[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            T a = T(0), b = T(0);
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+              a = fma(tab.S[i * N + p], u[k][i], a);
+              b = fma(tab.SD[i * N + p], u[k][i], b);
+            }
+            t[k] = a;
+            tx[k] = b;
+          }
+          // z contraction: w = Sz t, wz = SDz t, wx = Sz tx at (z = r, y = s, x = p)
+          if constexpr (EO) {
+            eo_apply<N, T, 1>(tab.eS, t, [&](int r, T v) { bufW[(r * N + s) * N + p] = v; });
+            eo_apply<N, T, -1>(tab.eSD, t, [&](int r, T v) { bufZ[(r * N + s) * N + p] = v; });
+            eo_apply<N, T, 1>(tab.eS, tx, [&](int r, T v) { bufX[(r * N + s) * N + p] = v; });
+          } else {
+#pragma unroll
+            for (int r = 0; r < N; ++r) {
+              T w = T(0), wz = T(0), wx = T(0);
+#pragma unroll
+              for (int k = 0; k < N; ++k) {
+                w = fma(tab.S[k * N + r], t[k], w);
+                wz = fma(tab.SD[k * N + r], t[k], wz);
+                wx = fma(tab.S[k * N + r], tx[k], wx);
+              }
+              const int o = (r * N + s) * N + p;
+              bufW[o] = w;
+              bufZ[o] = wz;
+              bufX[o] = wx;
+            }
           }
         }
       }
@@ -521,42 +596,78 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
           Xc[j] = bufX[o];
         }
         T fx[N], fy[N];
+        if constexpr (EO2) {
+          // f = G grad u at the point (p, q) of this slab: fx, fy kept, fz -> own bufX region
+          auto point = [&](int q, T dx, T dy, T dz) {
+            if (GEOM == 0) {
+              T gc[6];
+              load_g6<N, T, GEOM, SMEM_G>(geo, gcol, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
+              fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
+              fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
+              bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
+            } else {
+              // affine cells are axis-aligned boxes: the cell tensor is diagonal (rr, ss, tt)
+              T w = wr * tab.W[q] * tab.W[p];
+              if (GEOM == 2) w *= ld_stream(coef + g * (N2 * LANES) + (q * N + p) * LANES + lane, pol_first);
+              fx[q] = (w * cd0) * dx;
+              fy[q] = (w * cd3) * dy;
+              bufX[(s * N + q) * N + p] = (w * cd5) * dz; // fz
+            }
+          };
+          // dx = Sy wx, dy = SDy w, dz = Sy wz along the column; y1 = Sy^T fx, y2 = SDy^T fy
+          T dxv[N], dyv[N], dzv[N], y1v[N], y2v[N];
+          eo_apply<N, T, 1>(tab.eS, Xc, [&](int q, T v) { dxv[q] = v; });
+          eo_apply<N, T, -1>(tab.eSD, Wc, [&](int q, T v) { dyv[q] = v; });
+          eo_apply<N, T, 1>(tab.eS, Zc, [&](int q, T v) { dzv[q] = v; });
 #pragma unroll
-        for (int q = 0; q < N; ++q) {
-          T dx = T(0), dy = T(0), dz = T(0);
+          for (int q = 0; q < N; ++q) point(q, dxv[q], dyv[q], dzv[q]);
+          eo_apply<N, T, 1>(tab.eST, fx, [&](int j, T v) { y1v[j] = v; });
+          eo_apply<N, T, -1>(tab.eSDT, fy, [&](int j, T v) { y2v[j] = v; });
 #pragma unroll
-          for (int j = 0; j < N; ++j) {
-            dx = fma(tab.S[j * N + q], Xc[j], dx);
-            dy = fma(tab.SD[j * N + q], Wc[j], dy);
-            dz = fma(tab.S[j * N + q], Zc[j], dz);
-          }
-          if (GEOM == 0) {
-            T gc[6];
-            load_g6<N, T, GEOM, SMEM_G>(geo, gcol, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
-            fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
-            fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
-            bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
-          } else {
-            // affine cells are axis-aligned boxes: the cell tensor is diagonal (rr, ss, tt)
-            T w = wr * tab.W[q] * tab.W[p];
-            if (GEOM == 2) w *= ld_stream(coef + g * (N2 * LANES) + (q * N + p) * LANES + lane, pol_first);
-            fx[q] = (w * cd0) * dx;
-            fy[q] = (w * cd3) * dy;
-            bufX[(s * N + q) * N + p] = (w * cd5) * dz; // fz
-          }
-        }
+          for (int j = 0; j < N; ++j)
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
-          T y1 = T(0), y2 = T(0);
+            for (int i = 0; i < N; ++i) {
+              a[j][i] = fma(tab.SD[i * N + p], y1v[j], a[j][i]);
+              a[j][i] = fma(tab.S[i * N + p], y2v[j], a[j][i]);
+            }
+        } else {
 #pragma unroll
           for (int q = 0; q < N; ++q) {
-            y1 = fma(tab.S[j * N + q], fx[q], y1);
-            y2 = fma(tab.SD[j * N + q], fy[q], y2);
+            T dx = T(0), dy = T(0), dz = T(0);
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+              dx = fma(tab.S[j * N + q], Xc[j], dx);
+              dy = fma(tab.SD[j * N + q], Wc[j], dy);
+              dz = fma(tab.S[j * N + q], Zc[j], dz);
+            }
+            // f = G grad u at the point (p, q) of this slab: fx, fy kept, fz -> own bufX region
+            if (GEOM == 0) {
+              T gc[6];
+              load_g6<N, T, GEOM, SMEM_G>(geo, gcol, coef, tab, g, lane, e, q, p, wr, pol_first, gc);
+              fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
+              fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
+              bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
+            } else {
+              T w = wr * tab.W[q] * tab.W[p];
+              if (GEOM == 2) w *= ld_stream(coef + g * (N2 * LANES) + (q * N + p) * LANES + lane, pol_first);
+              fx[q] = (w * cd0) * dx;
+              fy[q] = (w * cd3) * dy;
+              bufX[(s * N + q) * N + p] = (w * cd5) * dz; // fz
+            }
           }
 #pragma unroll
-          for (int i = 0; i < N; ++i) {
-            a[j][i] = fma(tab.SD[i * N + p], y1, a[j][i]);
-            a[j][i] = fma(tab.S[i * N + p], y2, a[j][i]);
+          for (int j = 0; j < N; ++j) {
+            T y1 = T(0), y2 = T(0);
+#pragma unroll
+            for (int q = 0; q < N; ++q) {
+              y1 = fma(tab.S[j * N + q], fx[q], y1);
+              y2 = fma(tab.SD[j * N + q], fy[q], y2);
+            }
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+              a[j][i] = fma(tab.SD[i * N + p], y1, a[j][i]);
+              a[j][i] = fma(tab.S[i * N + p], y2, a[j][i]);
+            }
           }
         }
         if (SMEM_G && GEOM == 0) {
@@ -582,13 +693,22 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
         T fz[N];
 #pragma unroll
         for (int p = 0; p < N; ++p) fz[p] = bufX[(s * N + q) * N + p];
+        if constexpr (EO2) {
+          T x3v[N]; // x3 = Sx^T fz along this row
+          eo_apply<N, T, 1>(tab.eST, fz, [&](int i, T v) { x3v[i] = v; });
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
-          T x3 = T(0);
+          for (int i = 0; i < N; ++i)
 #pragma unroll
-          for (int p = 0; p < N; ++p) x3 = fma(tab.S[i * N + p], fz[p], x3);
+            for (int j = 0; j < N; ++j) c[j][i] = fma(tab.S[j * N + q], x3v[i], c[j][i]);
+        } else {
 #pragma unroll
-          for (int j = 0; j < N; ++j) c[j][i] = fma(tab.S[j * N + q], x3, c[j][i]);
+          for (int i = 0; i < N; ++i) {
+            T x3 = T(0);
+#pragma unroll
+            for (int p = 0; p < N; ++p) x3 = fma(tab.S[i * N + p], fz[p], x3);
+#pragma unroll
+            for (int j = 0; j < N; ++j) c[j][i] = fma(tab.S[j * N + q], x3, c[j][i]);
+          }
         }
       }
 #pragma unroll
