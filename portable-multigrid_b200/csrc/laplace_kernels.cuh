@@ -254,6 +254,9 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
 #ifndef PMG_VMULT_EO_PHASE2
 #define PMG_VMULT_EO_PHASE2 -1
 #endif
+#ifndef PMG_VMULT_DEFER
+#define PMG_VMULT_DEFER -1
+#endif
 #ifndef PMG_VMULT_EO_PHASE1X
 #define PMG_VMULT_EO_PHASE1X -1
 #endif
@@ -296,6 +299,8 @@ template <int N, typename T, int GEOM = 1> struct MinBlocks {
 // (registers are cheap at 4 bytes and unrolling keeps the tables as immediate operands),
 // except FP32 Q6 with full geometry, where runtime loops at 170 registers (12 warps/SM)
 // measured 1.4x faster on B200 than the unrolled form at 255
+// (FP32 Q6 affine in runtime loops at 142 registers, 12 warps/SM, measured no faster than the
+// unrolled form at 8 warps/SM)
 template <int N, typename T, int GEOM = 1> struct Unroll {
   static constexpr int value = (sizeof(T) == 8 || (N == 7 && GEOM == 0)) ? 1 : N;
 };
@@ -341,15 +346,20 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   //  EO   z contractions of phases 1 and 3: the ring variants and the FP32 direct variants
   //       other than N = 6 and N = 7 full geometry
   //  EO2  phase 2 (the y contractions of the columns, the x contraction of fz): the ring
-  //       variants, FP32 N <= 5 and FP64 N = 7 full geometry
+  //       variants, FP32 N <= 5 and every N = 7 variant
   //  EO1X x contractions of phase 1 by mirrored pairs of points (the point loop unrolled):
   //       with EO except at N = 6
+  //  DEFER (below) phase 2 without register accumulators, at N = 7
   constexpr bool EO =
       N >= 3 && (SMEM_G || (sizeof(T) == 4 && N != 6 && !(N == 7 && GEOM == 0)));
   constexpr bool EO2 =
       PMG_VMULT_EO_PHASE2 >= 0
           ? (PMG_VMULT_EO_PHASE2 == 1 && N >= 3)
-          : N >= 3 && (SMEM_G || (sizeof(T) == 4 && N <= 5) || (sizeof(T) == 8 && N == 7 && GEOM == 0));
+          : N >= 3 && (SMEM_G || (sizeof(T) == 4 && N <= 5) || N == 7);
+  // DEFER: phase 2 keeps no accumulators; y1, y2 and x3 are parked in the lane's own plane and
+  // contracted along x (and y) afterwards in even/odd form (N = 7: 8-35 % faster on B200,
+  // the runtime-loop FP64 variants lose their spills; slower at N <= 6)
+  constexpr bool DEFER = EO2 && (PMG_VMULT_DEFER >= 0 ? PMG_VMULT_DEFER == 1 : N == 7);
   constexpr bool EO1X = PMG_VMULT_EO_PHASE1X >= 0 ? (PMG_VMULT_EO_PHASE1X == 1 && EO && UNR == N)
                                                   : (EO && UNR == N && N != 6);
   using SM = SlabSmem<N, T, SMEM_G, PIPE>;
@@ -623,13 +633,22 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
           for (int q = 0; q < N; ++q) point(q, dxv[q], dyv[q], dzv[q]);
           eo_apply<N, T, 1>(tab.eST, fx, [&](int j, T v) { y1v[j] = v; });
           eo_apply<N, T, -1>(tab.eSDT, fy, [&](int j, T v) { y2v[j] = v; });
+          if constexpr (DEFER) {
+            // park y1, y2 over the consumed column p of this lane's plane (bufW, bufZ)
 #pragma unroll
-          for (int j = 0; j < N; ++j)
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-              a[j][i] = fma(tab.SD[i * N + p], y1v[j], a[j][i]);
-              a[j][i] = fma(tab.S[i * N + p], y2v[j], a[j][i]);
+            for (int j = 0; j < N; ++j) {
+              bufW[(s * N + j) * N + p] = y1v[j];
+              bufZ[(s * N + j) * N + p] = y2v[j];
             }
+          } else {
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+#pragma unroll
+              for (int i = 0; i < N; ++i) {
+                a[j][i] = fma(tab.SD[i * N + p], y1v[j], a[j][i]);
+                a[j][i] = fma(tab.S[i * N + p], y2v[j], a[j][i]);
+              }
+          }
         } else {
 #pragma unroll
           for (int q = 0; q < N; ++q) {
@@ -675,13 +694,47 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
           ++chunk;
         }
       }
-      // a -> own slab region of bufW (all of this lane's reads of it are done)
+      if constexpr (DEFER) {
+        // a(j, .) = SDx^T y1(j, .) + Sx^T y2(j, .), row by row in place over y1 (bufW)
+#pragma unroll UNR
+        for (int j = 0; j < N; ++j) {
+          T y1[N], y2[N], v[N];
 #pragma unroll
-      for (int j = 0; j < N; ++j)
+          for (int p = 0; p < N; ++p) {
+            y1[p] = bufW[(s * N + j) * N + p];
+            y2[p] = bufZ[(s * N + j) * N + p];
+          }
+          eo_apply<N, T, -1>(tab.eSDT, y1, [&](int i, T x) { v[i] = x; });
+          eo_apply<N, T, 1>(tab.eST, y2, [&](int i, T x) { v[i] += x; });
 #pragma unroll
-        for (int i = 0; i < N; ++i) bufW[(s * N + j) * N + i] = a[j][i];
+          for (int i = 0; i < N; ++i) bufW[(s * N + j) * N + i] = v[i];
+        }
+      } else {
+        // a -> own slab region of bufW (all of this lane's reads of it are done)
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+#pragma unroll
+          for (int i = 0; i < N; ++i) bufW[(s * N + j) * N + i] = a[j][i];
+      }
     }
-    {
+    if constexpr (DEFER) {
+      // c = Sy^T Sx^T fz: x3 = Sx^T fz row by row in place (bufX), then Sy^T by columns into
+      // this lane's region of bufZ (whose y2 values the pass above consumed)
+#pragma unroll UNR
+      for (int q = 0; q < N; ++q) {
+        T fz[N];
+#pragma unroll
+        for (int p = 0; p < N; ++p) fz[p] = bufX[(s * N + q) * N + p];
+        eo_apply<N, T, 1>(tab.eST, fz, [&](int i, T x) { bufX[(s * N + q) * N + i] = x; });
+      }
+#pragma unroll UNR
+      for (int i = 0; i < N; ++i) {
+        T x3[N];
+#pragma unroll
+        for (int q = 0; q < N; ++q) x3[q] = bufX[(s * N + q) * N + i];
+        eo_apply<N, T, 1>(tab.eST, x3, [&](int j, T x) { bufZ[(s * N + j) * N + i] = x; });
+      }
+    } else {
       // c = Sy^T Sx^T fz from this lane's fz region, into its own region of bufZ
       T c[N][N];
 #pragma unroll
