@@ -141,28 +141,49 @@ void chebyshev_estimate(pmg_chebyshev &c, cudaStream_t s) {
 }
 
 // Chebyshev iteration of the first kind: vmult from x = 0 (degree-1 products), step from dst
-// (degree products); x_{k+1} = x_k + f1 (x_k - x_{k-1}) + f2 D^{-1}(b - A x_k).
+// (degree products); x_{k+1} = x_k + f1 (x_k - x_{k-1}) + f2 D^{-1}(b - A x_k).  The iterates
+// alternate between dst and the work vector xo, each update written over the previous
+// iterate (one vector written per step); the first iterate goes where the parity of the
+// remaining steps puts the last one into dst.  Per element the arithmetic is that of the
+// two-vector form, so results are bit-identical to it.
 void chebyshev_apply(pmg_chebyshev &c, void *dst, const void *src, bool from_zero, cudaStream_t s) {
   if (!c.estimated) chebyshev_estimate(c, s);
   pmg_operator &op = *c.op;
   const int dt = op.dtype;
   const int64_t N = op.n_dofs;
+  const bool more = !(c.degree < 2 || std::fabs(c.delta) < 1e-40);
+  const int d = more ? c.degree : 1; // iterates after x_0
+  void *const A = dst, *const B = c.xo.get();
+  void *cur = nullptr, *prev = nullptr; // x_k and x_{k-1} (null: x_{k-1} = 0)
   if (from_zero) {
-    vec::cheb_init(dst, c.xo.get(), src, op.inv_diag.get(), 1.0 / c.theta, dt, N, s);
+    cur = ((d - 1) % 2 == 0) ? A : B;
+    vec::cheb_init(cur, nullptr, src, op.inv_diag.get(), 1.0 / c.theta, dt, N, s);
   } else {
     operator_vmult(op, c.Ax.get(), dst, s);
-    vec::cheb_first_step(dst, c.xo.get(), src, c.Ax.get(), op.inv_diag.get(), 1.0 / c.theta, dt, N, s);
+    if (d % 2 == 0) { // x_1 into xo, x_0 stays in dst as the previous iterate
+      vec::cheb_first_step_into(B, A, src, c.Ax.get(), op.inv_diag.get(), 1.0 / c.theta, dt, N, s);
+      cur = B;
+      prev = A;
+    } else { // x_0 moved to xo, x_1 in dst
+      vec::cheb_first_step(A, B, src, c.Ax.get(), op.inv_diag.get(), 1.0 / c.theta, dt, N, s);
+      cur = A;
+      prev = B;
+    }
   }
-  if (c.degree < 2 || std::fabs(c.delta) < 1e-40) return;
+  if (!more) return;
   double rhok = c.delta / c.theta;
   const double sigma = c.theta / c.delta;
-  for (int k = 1; k < c.degree; ++k) {
-    operator_vmult(op, c.Ax.get(), dst, s);
+  for (int k = 1; k < d; ++k) {
+    operator_vmult(op, c.Ax.get(), cur, s);
     const double rhokp = 1.0 / (2.0 * sigma - rhok);
     const double f1 = rhokp * rhok, f2 = 2.0 * rhokp / c.delta;
     rhok = rhokp;
-    vec::cheb_update(dst, c.xo.get(), src, c.Ax.get(), op.inv_diag.get(), f1, f2, dt, N, s);
+    void *out = prev ? prev : (cur == A ? B : A);
+    vec::cheb_update_into(out, cur, prev, src, c.Ax.get(), op.inv_diag.get(), f1, f2, dt, N, s);
+    prev = cur;
+    cur = out;
   }
+  PMG_REQUIRE(cur == A, "Chebyshev: the last iterate is not in dst");
 }
 
 void mg_setup(pmg_mg &mg, int n_levels, pmg_operator *const *levels, pmg_transfer *const *transfers,

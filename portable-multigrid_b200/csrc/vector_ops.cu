@@ -33,7 +33,7 @@ template <typename T>
 __global__ void cheb_init_k(T *dst, T *xo, const T *src, const T *invd, T scale, int64_t n) {
   GRID_STRIDE(i, n) {
     dst[i] = scale * invd[i] * src[i];
-    xo[i] = T(0);
+    if (xo) xo[i] = T(0);
   }
 }
 
@@ -47,13 +47,24 @@ __global__ void cheb_first_step_k(T *dst, T *xo, const T *src, const T *Ax, cons
   }
 }
 
+// the same first step into another vector: x0 is kept as the previous iterate
 template <typename T>
-__global__ void cheb_update_k(T *dst, T *xo, const T *src, const T *Ax, const T *invd, T f1, T f2,
-                              int64_t n) {
+__global__ void cheb_first_step_into_k(T *out, const T *x0, const T *src, const T *Ax, const T *invd,
+                                       T scale, int64_t n) {
   GRID_STRIDE(i, n) {
-    const T x = dst[i];
-    dst[i] = x + f1 * (x - xo[i]) + f2 * invd[i] * (src[i] - Ax[i]);
-    xo[i] = x;
+    const T x = x0[i];
+    out[i] = x + scale * invd[i] * (src[i] - Ax[i]);
+  }
+}
+
+// the update written over the previous iterate (out == prev allowed; prev == nullptr: zero)
+template <typename T>
+__global__ void cheb_update_into_k(T *out, const T *cur, const T *prev, const T *src, const T *Ax,
+                                   const T *invd, T f1, T f2, int64_t n) {
+  GRID_STRIDE(i, n) {
+    const T x = cur[i];
+    const T xo = prev ? prev[i] : T(0);
+    out[i] = x + f1 * (x - xo) + f2 * invd[i] * (src[i] - Ax[i]);
   }
 }
 
@@ -211,12 +222,22 @@ void cheb_first_step(void *dst, void *xo, const void *src, const void *Ax, const
   PMG_LAUNCH_CHECK();
 }
 
-void cheb_update(void *dst, void *xo, const void *src, const void *Ax, const void *invd, double f1,
-                 double f2, int dtype, int64_t n, cudaStream_t s) {
+void cheb_first_step_into(void *out, const void *x0, const void *src, const void *Ax, const void *invd,
+                          double scale, int dtype, int64_t n, cudaStream_t s) {
   prof::Scope scope_("vector_update", s);
-  DISPATCH(dtype, cheb_update_k<T><<<grid_for(n), kBlock, 0, s>>>(
-                      static_cast<T *>(dst), static_cast<T *>(xo), static_cast<const T *>(src),
-                      static_cast<const T *>(Ax), static_cast<const T *>(invd), (T)f1, (T)f2, n));
+  DISPATCH(dtype, cheb_first_step_into_k<T><<<grid_for(n), kBlock, 0, s>>>(
+                      static_cast<T *>(out), static_cast<const T *>(x0), static_cast<const T *>(src),
+                      static_cast<const T *>(Ax), static_cast<const T *>(invd), (T)scale, n));
+  PMG_LAUNCH_CHECK();
+}
+
+void cheb_update_into(void *out, const void *cur, const void *prev, const void *src, const void *Ax,
+                      const void *invd, double f1, double f2, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
+  DISPATCH(dtype, cheb_update_into_k<T><<<grid_for(n), kBlock, 0, s>>>(
+                      static_cast<T *>(out), static_cast<const T *>(cur), static_cast<const T *>(prev),
+                      static_cast<const T *>(src), static_cast<const T *>(Ax), static_cast<const T *>(invd),
+                      (T)f1, (T)f2, n));
   PMG_LAUNCH_CHECK();
 }
 

@@ -11,12 +11,18 @@ namespace vec {
 
 void fill_mod11(void *x, int dtype, int64_t n, cudaStream_t s);
 void convert(void *dst, int dt_dst, const void *src, int dt_src, int64_t n, cudaStream_t s);
+// Chebyshev vector steps (x_{k+1} = x_k + f1 (x_k - x_{k-1}) + f2 D^{-1} (b - A x_k)):
+// cheb_init: dst = scale D^{-1} src, xo = 0 unless xo is null; cheb_first_step: xo = dst,
+// dst += scale D^{-1} (src - Ax); cheb_first_step_into: out = x0 + scale D^{-1} (src - Ax);
+// cheb_update_into: out = the update from cur and prev (null: zero), out == prev allowed
 void cheb_init(void *dst, void *xo, const void *src, const void *invd, double scale, int dtype,
                int64_t n, cudaStream_t s);
 void cheb_first_step(void *dst, void *xo, const void *src, const void *Ax, const void *invd,
                      double scale, int dtype, int64_t n, cudaStream_t s);
-void cheb_update(void *dst, void *xo, const void *src, const void *Ax, const void *invd, double f1,
-                 double f2, int dtype, int64_t n, cudaStream_t s);
+void cheb_first_step_into(void *out, const void *x0, const void *src, const void *Ax, const void *invd,
+                          double scale, int dtype, int64_t n, cudaStream_t s);
+void cheb_update_into(void *out, const void *cur, const void *prev, const void *src, const void *Ax,
+                      const void *invd, double f1, double f2, int dtype, int64_t n, cudaStream_t s);
 void residual(void *t, const void *def, int dtype, int64_t n, cudaStream_t s);
 void jacobi(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s);
 void xpay(void *p, const void *z, double beta, int dtype, int64_t n, cudaStream_t s);
