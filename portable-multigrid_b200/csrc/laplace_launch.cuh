@@ -100,13 +100,14 @@ inline int pipe_override() {
   return v;
 }
 // Defaults from B200 sweeps (cell kernel time, 48^3..128^3 meshes): the index pipeline for
-// the FP64 ring variant at N >= 5 (deformed cube: Q4 +3 %, Q5 +26 %) and for the FP32 Q6
+// the FP64 ring variant at N >= 6 (deformed cube: Q5 +18 %; at Q4 its 3 KB index block
+// costs the seventh warp per SM, and Q4 runs 3.5 % faster without it) and for the FP32 Q6
 // affine kernel (+9 %); none elsewhere (Q1-Q3 lose 3-5 %, FP32 full geometry, Q4/Q5 affine
 // and FP64 Q6 affine lose 15-35 %).
 template <typename T, int GEOM, bool SG> int use_pipe() {
   const int o = pipe_override();
   if (o >= 0 && o <= 2) return o;
-  if (SG) return (sizeof(T) == 8 && kN >= 5) ? 1 : 0;
+  if (SG) return (sizeof(T) == 8 && kN >= 6) ? 1 : 0;
   if (GEOM != 0 && kN == 7 && sizeof(T) == 4) return 1;
   return 0;
 }
