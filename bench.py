@@ -323,6 +323,44 @@ def time_to_solution(torch, pmg, dev, refine=4, repeats=3):
     return res
 
 
+def q6_kernel_rates(torch, pmg, dev, peaks, refine=4, launches=20):
+    """The Q6 affine + kappa cell kernels of the config-3 fine level (48^3 cells) alone, FP32
+    and FP64: event-timed duration per launch and the algorithmic FLOP rate against the
+    same-run FMA peak.  Algorithmic FLOPs per cell: 24 N^4 (twelve 1D passes of N^4
+    multiply-adds: interpolation and derivative in three directions, forward and transposed)
+    + 6 N^3 (the diagonal cell tensor times weight and coefficient at each point), N = 7.  The
+    even/odd form executes about half the passes' multiply-adds, so the rate is an
+    algorithmic one, not an instruction count."""
+    box = pmg.Box.make(coarse=(3, 3, 3), refine=refine)
+    mesh = pmg.Mesh(box)
+    N = 7
+    flops = mesh.n_cells() * (24 * N ** 4 + 6 * N ** 3)
+    res = {"algorithmic_flops_per_launch": flops}
+    for name, dt, tdt, peak_key in (("fp32", pmg.F32, torch.float32, "fp32_fma_tflops"),
+                                    ("fp64", pmg.F64, torch.float64, "fp64_fma_tflops")):
+        op = pmg.LaplaceOperator(mesh, 6, dt, pmg.GEOMETRY_AFFINE, pmg.COEFF_KAPPA, device=dev)
+        src = torch.rand(op.m(), dtype=tdt, device=f"cuda:{dev}")
+        dst = torch.empty_like(src)
+        for _ in range(3):
+            op.vmult(dst, src)
+        torch.cuda.synchronize()
+        pmg.profile_reset()
+        pmg.profile_enable(True)
+        for _ in range(launches):
+            op.vmult(dst, src)
+        torch.cuda.synchronize()
+        pmg.profile_enable(False)
+        ms, n = pmg.profile_query("vmult_cell")
+        t = ms / max(n, 1) * 1e-3
+        tflops = flops / t / 1e12
+        res[name] = {"cell_kernel_us": t * 1e6, "algorithmic_tflops": tflops,
+                     "frac_of_same_run_fma": tflops / peaks[peak_key] if peaks else None}
+        del op, src, dst
+    del mesh
+    torch.cuda.empty_cache()
+    return res
+
+
 def reference_problem(torch, pmg, dev, cycle=20, repeats=3):
     """The reference's own logged solve: Q4, f = 1, homogeneous Dirichlet on the "doubling" mesh
     of cycle 20 (2 x 2 x 1 coarse cells refined 6 times, 67,634,433 DoFs), ph-multigrid with
@@ -447,6 +485,8 @@ def gpu_arm(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
+    # same-run peaks (copy bandwidth, FMA rates) before anything else holds device memory
+    peaks = pmg.measure_peaks(dev, 1 << 30) if rank == 0 else None
     dt = pmg.F64 if args.dtype == "f64" else pmg.F32
     tdt = torch.float64 if dt == pmg.F64 else torch.float32
     refine = box_for(args.cells)
@@ -514,6 +554,7 @@ def gpu_arm(args):
         del op, src, dst
         torch.cuda.empty_cache()
         tts = time_to_solution(torch, pmg, dev)
+        tts["q6_cell_kernels"] = q6_kernel_rates(torch, pmg, dev, peaks)
         extra["dg_time_to_1e-10"] = dg_time_to_solution(torch, pmg, dev)
         extra["reference_problem"] = reference_problem(torch, pmg, dev)
         extra["adjoint_gradient"] = adjoint_check(torch, pmg, dev)
@@ -540,6 +581,7 @@ def gpu_arm(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": ("measured MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
                                          else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"),
+                         "frac_of_same_run_copy": achieved / peaks["copy_gbs"] if peaks else None,
                          "kernel": "vmult_slab_kernel<5,double,0>",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "kernel_ms_avg": cell_avg_s * 1e3},
@@ -554,6 +596,7 @@ def gpu_arm(args):
             "time_to_1e-10": tts,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "peaks_same_run": peaks,
         }
         line.update(extra)
         print(json.dumps(line), flush=True)

@@ -335,6 +335,19 @@ pmg_status pmg_profile_reset(void);
  * number of launches since the last reset. */
 pmg_status pmg_profile_query(const char *kernel, double *total_ms, int64_t *launches);
 
+/* Same-run peaks for roofline fractions (no reference counterpart): a device-to-device copy
+ * over two buffers of copy_bytes each (256 MiB .. 16 GiB, larger than L2; copy_gbs counts
+ * bytes read plus written) and FP64 / FP32 FMA throughput (2 flops per FMA, no memory
+ * traffic).  Allocates 2 x copy_bytes for the duration of the call and synchronises. */
+typedef struct pmg_peaks {
+  double copy_gbs;
+  double fp64_fma_tflops;
+  double fp32_fma_tflops;
+  int64_t copy_bytes;
+  int32_t sm_count;
+} pmg_peaks;
+pmg_status pmg_measure_peaks(int32_t device, int64_t copy_bytes, pmg_peaks *out);
+
 #ifdef __cplusplus
 }
 #endif

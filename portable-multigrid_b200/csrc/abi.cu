@@ -41,7 +41,8 @@ inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
 
 namespace pmg {
 void vector_dot_noalloc(const void *a, const void *b, int dtype, int64_t n, double *result,
-                        cudaStream_t s); // noalloc.cu
+                        cudaStream_t s);                                 // noalloc.cu
+void measure_peaks(int device, int64_t copy_bytes, pmg_peaks *out); // peaks.cu
 }
 
 extern "C" {
@@ -537,6 +538,16 @@ pmg_status pmg_profile_enable(int32_t on) {
 
 pmg_status pmg_profile_reset(void) {
   return guarded(__func__, [&] { pmg::prof::reset(); });
+}
+
+pmg_status pmg_measure_peaks(int32_t device, int64_t copy_bytes, pmg_peaks *out) {
+  return guarded(__func__, [&] {
+    NEED(out);
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) pmg::fail(PMG_ENODEV, "no CUDA device available");
+    PMG_REQUIRE(device >= 0 && device < n, "device out of range");
+    pmg::measure_peaks(device, copy_bytes, out);
+  });
 }
 
 pmg_status pmg_profile_query(const char *kernel, double *total_ms, int64_t *launches) {

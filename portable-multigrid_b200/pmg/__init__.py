@@ -97,6 +97,11 @@ class CGInfo(C.Structure):
                 ("reduction_per_step", C.c_double)]
 
 
+class Peaks(C.Structure):
+    _fields_ = [("copy_gbs", C.c_double), ("fp64_fma_tflops", C.c_double), ("fp32_fma_tflops", C.c_double),
+                ("copy_bytes", C.c_int64), ("sm_count", C.c_int32)]
+
+
 _lib = None
 
 
@@ -179,6 +184,7 @@ def _declare(L):
         "pmg_profile_enable": ([i32], i32),
         "pmg_profile_reset": ([], i32),
         "pmg_profile_query": ([C.c_char_p, P(d), P(i64)], i32),
+        "pmg_measure_peaks": ([i32, i64, P(Peaks)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -236,6 +242,15 @@ def profile_query(kernel):
     ms, n = C.c_double(), C.c_int64()
     check(lib().pmg_profile_query(kernel.encode(), C.byref(ms), C.byref(n)))
     return ms.value, n.value
+
+
+def measure_peaks(device: int = 0, copy_bytes: int = 1 << 30):
+    """Same-run peaks on `device`: STREAM-style copy GB/s (read + write bytes) over two buffers
+    of `copy_bytes`, and FP64 / FP32 FMA TFLOP/s (pmg_measure_peaks)."""
+    p = Peaks()
+    check(lib().pmg_measure_peaks(device, copy_bytes, C.byref(p)))
+    return {"copy_gbs": p.copy_gbs, "fp64_fma_tflops": p.fp64_fma_tflops,
+            "fp32_fma_tflops": p.fp32_fma_tflops, "copy_bytes": p.copy_bytes, "sm_count": p.sm_count}
 
 
 class Mesh:
