@@ -254,6 +254,9 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
 #ifndef PMG_VMULT_EO_PHASE2
 #define PMG_VMULT_EO_PHASE2 -1
 #endif
+#ifndef PMG_VMULT_ROLL_TAIL
+#define PMG_VMULT_ROLL_TAIL -1
+#endif
 #ifndef PMG_VMULT_DEFER
 #define PMG_VMULT_DEFER -1
 #endif
@@ -360,6 +363,12 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   // contracted along x (and y) afterwards in even/odd form (N = 7: 8-35 % faster on B200,
   // the runtime-loop FP64 variants lose their spills; slower at N <= 6)
   constexpr bool DEFER = EO2 && (PMG_VMULT_DEFER >= 0 ? PMG_VMULT_DEFER == 1 : N == 7);
+  // the deferred passes and phase 3 index the tables by their inner loops only, so their
+  // outer loops can stay rolled (smaller code) at no table-load cost: FP32 Q4 affine falls
+  // from ~205 to 128 registers and runs 21 % faster on B200; every other variant measured
+  // 1-15 % slower rolled
+  constexpr int TUNR = PMG_VMULT_ROLL_TAIL >= 0 ? (PMG_VMULT_ROLL_TAIL == 1 ? 1 : UNR)
+                                                : ((sizeof(T) == 4 && N == 5 && GEOM != 0) ? 1 : UNR);
   constexpr bool EO1X = PMG_VMULT_EO_PHASE1X >= 0 ? (PMG_VMULT_EO_PHASE1X == 1 && EO && UNR == N)
                                                   : (EO && UNR == N && N != 6);
   using SM = SlabSmem<N, T, SMEM_G, PIPE>;
@@ -696,7 +705,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
       }
       if constexpr (DEFER) {
         // a(j, .) = SDx^T y1(j, .) + Sx^T y2(j, .), row by row in place over y1 (bufW)
-#pragma unroll UNR
+#pragma unroll TUNR
         for (int j = 0; j < N; ++j) {
           T y1[N], y2[N], v[N];
 #pragma unroll
@@ -720,14 +729,14 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     if constexpr (DEFER) {
       // c = Sy^T Sx^T fz: x3 = Sx^T fz row by row in place (bufX), then Sy^T by columns into
       // this lane's region of bufZ (whose y2 values the pass above consumed)
-#pragma unroll UNR
+#pragma unroll TUNR
       for (int q = 0; q < N; ++q) {
         T fz[N];
 #pragma unroll
         for (int p = 0; p < N; ++p) fz[p] = bufX[(s * N + q) * N + p];
         eo_apply<N, T, 1>(tab.eST, fz, [&](int i, T x) { bufX[(s * N + q) * N + i] = x; });
       }
-#pragma unroll UNR
+#pragma unroll TUNR
       for (int i = 0; i < N; ++i) {
         T x3[N];
 #pragma unroll
@@ -772,7 +781,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     __syncwarp(MASK);
 
     // ---- phase 3: Y-slab y = s, out = Sz^T a + SDz^T c, scatter ----
-#pragma unroll UNR
+#pragma unroll TUNR
     for (int i = 0; i < N; ++i) {
       T A[N], Cc[N];
 #pragma unroll
