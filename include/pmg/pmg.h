@@ -84,6 +84,11 @@ pmg_status pmg_mesh_n_cells(const pmg_mesh *mesh, int64_t *n_cells);
 #define PMG_GEOMETRY_AUTO 0   /* per-cell constants on undeformed boxes, else per point */
 #define PMG_GEOMETRY_FULL 1   /* symmetric tensor G per quadrature point, 6*nq^3/cell   */
 #define PMG_GEOMETRY_AFFINE 2 /* 6 constants per cell, times w_q and the coefficient   */
+/* J^{-1} (9 values) and JxW per quadrature point, 10*nq^3/cell: the deal.II-style
+ * formulation of include/operators/portable_laplace_operator.h:136-245 with
+ * include/kernels/portable_local_laplace_operator.h:329-347 (inverse Jacobian applied twice
+ * per point); any box, PMG_COEFF_NONE / _KAPPA / _VALUES folded into JxW */
+#define PMG_GEOMETRY_INVJAC 3
 
 #define PMG_COEFF_NONE 0   /* -lap u                                                   */
 #define PMG_COEFF_KAPPA 1  /* kappa = 1 + 0.9 sin(2 pi x) sin(2 pi y) sin(2 pi z)      */

@@ -119,6 +119,7 @@ void qp_form_geom(const pmg_operator &op, const void *u, const void *v, double a
 template <int N, typename T>
 void qp_form_launch(const pmg_operator &op, const void *u, const void *v, double alpha, double *out,
                     cudaStream_t s) {
+  PMG_REQUIRE(op.geometry != PMG_GEOMETRY_INVJAC, "the per-point form needs the G or affine geometry layout");
   if (op.geometry == PMG_GEOMETRY_FULL) qp_form_geom<N, T, 0>(op, u, v, alpha, out, s);
   else if (op.has_coeff_values) qp_form_geom<N, T, 2>(op, u, v, alpha, out, s);
   else qp_form_geom<N, T, 1>(op, u, v, alpha, out, s);

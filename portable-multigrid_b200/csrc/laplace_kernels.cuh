@@ -269,6 +269,25 @@ template <int N> struct Stride {
   static constexpr int CELL = N * N * N + ((N == 3 || N == 5) ? 0 : 1);
 };
 
+// Inverse-Jacobian formulation (geo = [group][x point p][y point q][10][LANES]: J^{-1} row by
+// row, then JxW): the physical gradient J^{-T} grad_ref, times JxW, and back with J^{-1}
+// (include/kernels/portable_local_laplace_operator.h:329-347).
+template <int N, typename T>
+__device__ __forceinline__ void invjac_flux(const T *__restrict__ geo, int64_t g, int lane, int q, int p,
+                                            uint64_t pol, T dx, T dy, T dz, T (&f)[3]) {
+  constexpr int LANES = Layout<N>::LANES, N2 = Layout<N>::N2;
+  const T *gp = geo + g * (N2 * 10 * LANES) + (p * N + q) * 10 * LANES + lane;
+  T iv[9];
+#pragma unroll
+  for (int m = 0; m < 9; ++m) iv[m] = ld_stream(gp + m * LANES, pol);
+  const T jw = ld_stream(gp + 9 * LANES, pol);
+  T gx[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) gx[k] = jw * (iv[k] * dx + iv[3 + k] * dy + iv[6 + k] * dz);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) f[d] = iv[3 * d] * gx[0] + iv[3 * d + 1] * gx[1] + iv[3 * d + 2] * gx[2];
+}
+
 template <int N, typename T, int GEOM, bool SMEM_G>
 __device__ __forceinline__ void load_g6(const T *__restrict__ geo, const T *gs,
                                         const T *__restrict__ coef, const Tab<N, T> &tab,
@@ -296,7 +315,8 @@ __device__ __forceinline__ void load_g6(const T *__restrict__ geo, const T *gs,
 // resident blocks of 128 threads per SM the register allocation is sized for; matches the
 // shared-memory footprint (3 exchange buffers per warp) of each degree and type
 template <int N, typename T, int GEOM = 1> struct MinBlocks {
-  static constexpr int value = sizeof(T) == 8 ? (N >= 6 ? 2 : 3) : ((N == 7 && GEOM == 0) ? 3 : 2);
+  static constexpr int value =
+      sizeof(T) == 8 ? (N >= 6 ? 2 : 3) : ((N == 7 && (GEOM == 0 || GEOM == 3)) ? 3 : 2);
 };
 // outer streaming loops: runtime loops for FP64 (bounded live registers), unrolled for FP32
 // (registers are cheap at 4 bytes and unrolling keeps the tables as immediate operands),
@@ -305,7 +325,7 @@ template <int N, typename T, int GEOM = 1> struct MinBlocks {
 // (FP32 Q6 affine in runtime loops at 142 registers, 12 warps/SM, measured no faster than the
 // unrolled form at 8 warps/SM)
 template <int N, typename T, int GEOM = 1> struct Unroll {
-  static constexpr int value = (sizeof(T) == 8 || (N == 7 && GEOM == 0)) ? 1 : N;
+  static constexpr int value = (sizeof(T) == 8 || (N == 7 && (GEOM == 0 || GEOM == 3))) ? 1 : N;
 };
 
 // Shared memory per warp of vmult_slab_kernel: 3 exchange buffers, plus (SMEM_G) the
@@ -354,7 +374,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   //       with EO except at N = 6
   //  DEFER (below) phase 2 without register accumulators, at N = 7
   constexpr bool EO =
-      N >= 3 && (SMEM_G || (sizeof(T) == 4 && N != 6 && !(N == 7 && GEOM == 0)));
+      N >= 3 && (SMEM_G || (sizeof(T) == 4 && N != 6 && !(N == 7 && (GEOM == 0 || GEOM == 3))));
   constexpr bool EO2 =
       PMG_VMULT_EO_PHASE2 >= 0
           ? (PMG_VMULT_EO_PHASE2 == 1 && N >= 3)
@@ -368,11 +388,12 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   // from ~205 to 128 registers and runs 21 % faster on B200; every other variant measured
   // 1-15 % slower rolled
   constexpr int TUNR = PMG_VMULT_ROLL_TAIL >= 0 ? (PMG_VMULT_ROLL_TAIL == 1 ? 1 : UNR)
-                                                : ((sizeof(T) == 4 && N == 5 && GEOM != 0) ? 1 : UNR);
+                                                : ((sizeof(T) == 4 && N == 5 && (GEOM == 1 || GEOM == 2)) ? 1 : UNR);
   constexpr bool EO1X = PMG_VMULT_EO_PHASE1X >= 0 ? (PMG_VMULT_EO_PHASE1X == 1 && EO && UNR == N)
                                                   : (EO && UNR == N && N != 6);
   using SM = SlabSmem<N, T, SMEM_G, PIPE>;
   static_assert(!(SMEM_G && PIPE == 2), "src staging is not combined with the geometry ring");
+  constexpr int NCOMP = GEOM == 3 ? 10 : 6; // geometry values per quadrature point
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   if (lane >= LANES) return;
@@ -436,8 +457,8 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   }
 
   for (int64_t g = warp0; g < n_groups; g += nwarps, ++it) {
-    if (GEOM == 0 && lane == 0 && g + nwarps < n_groups)
-      prefetch_l2(geo + (g + nwarps) * (N2 * 6 * LANES), N2 * 6 * LANES * sizeof(T), pol_first);
+    if ((GEOM == 0 || GEOM == 3) && lane == 0 && g + nwarps < n_groups)
+      prefetch_l2(geo + (g + nwarps) * (N2 * NCOMP * LANES), N2 * NCOMP * LANES * sizeof(T), pol_first);
     const uint32_t *ig = idx + g * (N2 * LANES) + lane;
     const int slot = it & 1;
 
@@ -573,7 +594,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
 
     // ---- phase 2: Z-slab z = s, streamed over the x point p ----
     T cd0 = T(0), cd3 = T(0), cd5 = T(0); // diagonal of the affine cell tensor
-    if (GEOM != 0) {
+    if (GEOM == 1 || GEOM == 2) {
       const T *cg = geo + (g * CPW + e) * 8;
       cd0 = __ldg(cg);
       cd3 = __ldg(cg + 3);
@@ -624,6 +645,12 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
               fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
               fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
               bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
+            } else if (GEOM == 3) {
+              T f3[3];
+              invjac_flux<N, T>(geo, g, lane, q, p, pol_first, dx, dy, dz, f3);
+              fx[q] = f3[0];
+              fy[q] = f3[1];
+              bufX[(s * N + q) * N + p] = f3[2]; // fz
             } else {
               // affine cells are axis-aligned boxes: the cell tensor is diagonal (rr, ss, tt)
               T w = wr * tab.W[q] * tab.W[p];
@@ -675,6 +702,12 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
               fx[q] = gc[0] * dx + gc[1] * dy + gc[2] * dz;
               fy[q] = gc[1] * dx + gc[3] * dy + gc[4] * dz;
               bufX[(s * N + q) * N + p] = gc[2] * dx + gc[4] * dy + gc[5] * dz; // fz
+            } else if (GEOM == 3) {
+              T f3[3];
+              invjac_flux<N, T>(geo, g, lane, q, p, pol_first, dx, dy, dz, f3);
+              fx[q] = f3[0];
+              fy[q] = f3[1];
+              bufX[(s * N + q) * N + p] = f3[2]; // fz
             } else {
               T w = wr * tab.W[q] * tab.W[p];
               if (GEOM == 2) w *= ld_stream(coef + g * (N2 * LANES) + (q * N + p) * LANES + lane, pol_first);
@@ -858,6 +891,19 @@ __global__ void __launch_bounds__(128) diag_slab_kernel(const Tab2<N, T> tab,
           const T *gp = geo + g * (N2 * 6 * LANES) + (p * N + q) * 6 * LANES + lane;
 #pragma unroll
           for (int m = 0; m < 6; ++m) c[m] = __ldg(gp + m * LANES);
+        } else if (GEOM == 3) {
+          // G = JxW J^{-1} J^{-T} from the inverse-Jacobian layout, in the order of G
+          const T *gp = geo + g * (N2 * 10 * LANES) + (p * N + q) * 10 * LANES + lane;
+          T iv[9];
+#pragma unroll
+          for (int m = 0; m < 9; ++m) iv[m] = __ldg(gp + m * LANES);
+          const T jw = __ldg(gp + 9 * LANES);
+          int m = 0;
+#pragma unroll
+          for (int d1 = 0; d1 < 3; ++d1)
+#pragma unroll
+            for (int d2 = d1; d2 < 3; ++d2)
+              c[m++] = jw * (iv[3 * d1] * iv[3 * d2] + iv[3 * d1 + 1] * iv[3 * d2 + 1] + iv[3 * d1 + 2] * iv[3 * d2 + 2]);
         } else {
           const T *cg = geo + (g * CPW + e) * 8;
           T w = wr * tab.W[q] * tab.W[p];

@@ -108,7 +108,7 @@ template <typename T, int GEOM, bool SG> int use_pipe() {
   const int o = pipe_override();
   if (o >= 0 && o <= 2) return o;
   if (SG) return (sizeof(T) == 8 && kN >= 6) ? 1 : 0;
-  if (GEOM != 0 && kN == 7 && sizeof(T) == 4) return 1;
+  if ((GEOM == 1 || GEOM == 2) && kN == 7 && sizeof(T) == 4) return 1;
   return 0;
 }
 
@@ -199,8 +199,13 @@ template <typename T, int GEOM, bool SG> void vmult_pipe(const SlabLaunch &L) {
 }
 
 template <typename T, int GEOM> void vmult_geom(const SlabLaunch &L) {
-  if (GEOM == 0 && use_ring<T>()) vmult_pipe<T, GEOM, true>(L);
-  else vmult_pipe<T, GEOM, false>(L);
+  if constexpr (GEOM == 0) {
+    if (use_ring<T>()) {
+      vmult_pipe<T, GEOM, true>(L);
+      return;
+    }
+  }
+  vmult_pipe<T, GEOM, false>(L);
 }
 
 template <typename T, int GEOM> void diag_geom(const SlabLaunch &L) {
@@ -217,12 +222,14 @@ template <typename T, int GEOM> void diag_geom(const SlabLaunch &L) {
 template <typename T> void vmult_type(const SlabLaunch &L) {
   if (L.geom == 0) vmult_geom<T, 0>(L);
   else if (L.geom == 1) vmult_geom<T, 1>(L);
+  else if (L.geom == 3) vmult_geom<T, 3>(L);
   else vmult_geom<T, 2>(L);
 }
 
 template <typename T> void diag_type(const SlabLaunch &L) {
   if (L.geom == 0) diag_geom<T, 0>(L);
   else if (L.geom == 1) diag_geom<T, 1>(L);
+  else if (L.geom == 3) diag_geom<T, 3>(L);
   else diag_geom<T, 2>(L);
 }
 
@@ -232,7 +239,8 @@ template <typename T, int GEOM, bool SG, int PIPE> int occ_vmult_variant() {
 // resident warps per SM of the direct variant (low 16 bits) and of the ring variant (high)
 template <typename T, int GEOM> int occ_vmult() {
   const int direct = occ_vmult_variant<T, GEOM, false, 0>();
-  const int ring = GEOM == 0 ? occ_vmult_variant<T, GEOM, true, 0>() : direct;
+  int ring = direct;
+  if constexpr (GEOM == 0) ring = occ_vmult_variant<T, GEOM, true, 0>();
   return direct | (ring << 16);
 }
 template <typename T, int GEOM> int occ_diag() {
@@ -241,6 +249,23 @@ template <typename T, int GEOM> int occ_diag() {
   int nb = 0;
   PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kWarpsPerBlock, diag_smem<T>()));
   return nb * kWarpsPerBlock; // resident warps per SM
+}
+
+template <typename T> int occ_vmult_geom(int geom) {
+  switch (geom) {
+  case 0: return occ_vmult<T, 0>();
+  case 1: return occ_vmult<T, 1>();
+  case 3: return occ_vmult<T, 3>();
+  default: return occ_vmult<T, 2>();
+  }
+}
+template <typename T> int occ_diag_geom(int geom) {
+  switch (geom) {
+  case 0: return occ_diag<T, 0>();
+  case 1: return occ_diag<T, 1>();
+  case 3: return occ_diag<T, 3>();
+  default: return occ_diag<T, 2>();
+  }
 }
 
 } // namespace
@@ -256,15 +281,11 @@ void PMG_CAT(launch_diag_p, PMG_DEGREE)(const SlabLaunch &L) {
 }
 
 int PMG_CAT(occupancy_vmult_p, PMG_DEGREE)(int dtype, int geom) {
-  if (dtype == PMG_F64)
-    return geom == 0 ? occ_vmult<double, 0>() : geom == 1 ? occ_vmult<double, 1>() : occ_vmult<double, 2>();
-  return geom == 0 ? occ_vmult<float, 0>() : geom == 1 ? occ_vmult<float, 1>() : occ_vmult<float, 2>();
+  return dtype == PMG_F64 ? occ_vmult_geom<double>(geom) : occ_vmult_geom<float>(geom);
 }
 
 int PMG_CAT(occupancy_diag_p, PMG_DEGREE)(int dtype, int geom) {
-  if (dtype == PMG_F64)
-    return geom == 0 ? occ_diag<double, 0>() : geom == 1 ? occ_diag<double, 1>() : occ_diag<double, 2>();
-  return geom == 0 ? occ_diag<float, 0>() : geom == 1 ? occ_diag<float, 1>() : occ_diag<float, 2>();
+  return dtype == PMG_F64 ? occ_diag_geom<double>(geom) : occ_diag_geom<float>(geom);
 }
 
 } // namespace pmg

@@ -52,7 +52,9 @@ __device__ __forceinline__ double coefficient(int kind, const double x[3]) {
 // mode 3: the quadrature points, out[cell][q][3];
 // mode 4: coef * |det J| w_q into the affine coefficient layout (mass-matrix weights);
 // mode 5: out[cell] = (sum_q (u_h(x_q) - u(x_q))^2 |det J| w_q)^(1/2) for the exact solution
-//         u of f_kind 1 (sin(pi x) sin(pi y) sin(pi z)) or 2 (exp(x) sin(pi y) cos(pi z)).
+//         u of f_kind 1 (sin(pi x) sin(pi y) sin(pi z)) or 2 (exp(x) sin(pi y) cos(pi z));
+// mode 6: write J^{-1} (9 entries, row d = d xi_d / dx) and coef * |det J| w_q into the slab
+//         layout of the inverse-Jacobian formulation, [group][x point][y point][10][lane].
 template <typename T>
 __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restrict__ cell_xyz,
                                      int64_t n_cells, int mode, int coeff_kind,
@@ -134,6 +136,10 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
             out[((grp * (g.N * g.N) + m) * 6 + comp) * g.lanes + lane] = (T)(f * s);
             ++comp;
           }
+      } else if (mode == 6) {
+        for (int comp = 0; comp < 9; ++comp)
+          out[((grp * (g.N * g.N) + m) * 10 + comp) * g.lanes + lane] = (T)inv[comp];
+        out[((grp * (g.N * g.N) + m) * 10 + 9) * g.lanes + lane] = (T)(fabs(det) * wq * kap);
       } else if (mode == 1) {
         out[(grp * (g.N * g.N) + m_row) * g.lanes + lane] = (T)kap;
       } else if (mode == 3) {
@@ -258,6 +264,7 @@ int occupancy(bool diag, int degree, int dtype, int geom) {
 
 int geom_code(const pmg_operator &op) {
   if (op.geometry == PMG_GEOMETRY_FULL) return 0;
+  if (op.geometry == PMG_GEOMETRY_INVJAC) return 3;
   return op.has_coeff_values ? 2 : 1;
 }
 
@@ -307,7 +314,8 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   int geometry = prm.geometry;
   if (geometry == PMG_GEOMETRY_AUTO || op.kind == PMG_OP_DG_SIPG)
     geometry = mesh.m.box.deform ? PMG_GEOMETRY_FULL : PMG_GEOMETRY_AFFINE;
-  PMG_REQUIRE(geometry == PMG_GEOMETRY_FULL || geometry == PMG_GEOMETRY_AFFINE, "bad geometry");
+  PMG_REQUIRE(geometry == PMG_GEOMETRY_FULL || geometry == PMG_GEOMETRY_AFFINE || geometry == PMG_GEOMETRY_INVJAC,
+              "bad geometry");
   PMG_REQUIRE(!(geometry == PMG_GEOMETRY_AFFINE && mesh.m.box.deform), "affine geometry needs an undeformed box");
   op.geometry = geometry;
   op.has_coeff_values = (geometry == PMG_GEOMETRY_AFFINE && prm.coeff_kind != PMG_COEFF_NONE);
@@ -405,14 +413,15 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
                                                    coef_in, op.coef.as<float>(), nullptr, 0);
       PMG_LAUNCH_CHECK();
     }
-  } else if (geometry == PMG_GEOMETRY_FULL) {
-    op.geo.allocate(s * op.n_groups * N2 * 6 * op.lanes);
+  } else if (geometry == PMG_GEOMETRY_FULL || geometry == PMG_GEOMETRY_INVJAC) {
+    const bool ij = geometry == PMG_GEOMETRY_INVJAC;
+    op.geo.allocate(s * op.n_groups * N2 * (ij ? 10 : 6) * op.lanes);
     PMG_CUDA(cudaMemset(op.geo.get(), 0, op.geo.bytes()));
     if (op.dtype == PMG_F64)
-      cell_geometry_kernel<double><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 0, prm.coeff_kind,
+      cell_geometry_kernel<double><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, ij ? 6 : 0, prm.coeff_kind,
                                                   coef_in, op.geo.as<double>(), nullptr, 0);
     else
-      cell_geometry_kernel<float><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, 0, prm.coeff_kind,
+      cell_geometry_kernel<float><<<grid, 128>>>(gp, xyz.as<int32_t>(), op.n_cells, ij ? 6 : 0, prm.coeff_kind,
                                                  coef_in, op.geo.as<float>(), nullptr, 0);
     PMG_LAUNCH_CHECK();
   } else {
@@ -582,6 +591,7 @@ int64_t operator_bytes(const pmg_operator &op) {
   int64_t g = 0;
   if (op.kind == PMG_OP_MASS) g = op.mass_geom == 1 ? 1 : nq3;
   else if (op.geometry == PMG_GEOMETRY_FULL) g = 6 * nq3;
+  else if (op.geometry == PMG_GEOMETRY_INVJAC) g = 10 * nq3;
   else g = 6 + (op.has_coeff_values ? nq3 : 0);
   return 2 * s * op.n_dofs + 4 * nm3 * op.n_cells + g * s * op.n_cells;
 }
@@ -605,8 +615,8 @@ void operator_set_coefficient(pmg_operator &op, const double *values, bool on_de
   if (op.kind == PMG_OP_MASS) {
     mode = 4;
     out = op.coef.get();
-  } else if (op.geometry == PMG_GEOMETRY_FULL) {
-    mode = 0;
+  } else if (op.geometry == PMG_GEOMETRY_FULL || op.geometry == PMG_GEOMETRY_INVJAC) {
+    mode = op.geometry == PMG_GEOMETRY_INVJAC ? 6 : 0;
     out = op.geo.get();
   } else {
     mode = 1;

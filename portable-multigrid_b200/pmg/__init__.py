@@ -31,7 +31,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "libpmg_b200.so")
 HEADER_PATH = os.path.join(REPO_ROOT, "include", "pmg", "pmg.h")
 
 F64, F32 = 0, 1
-GEOMETRY_AUTO, GEOMETRY_FULL, GEOMETRY_AFFINE = 0, 1, 2
+GEOMETRY_AUTO, GEOMETRY_FULL, GEOMETRY_AFFINE, GEOMETRY_INVJAC = 0, 1, 2, 3
 COEFF_NONE, COEFF_KAPPA, COEFF_VALUES = 0, 1, 2
 OP_LAPLACE, OP_DG_SIPG, OP_MASS = 0, 1, 2
 INVALID = 0xFFFFFFFF

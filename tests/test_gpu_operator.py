@@ -184,3 +184,65 @@ def test_l2_error_matches_oracle(oracle, degree, dtype, boxname):
         got = op.l2_error(ut, 1, nq)
         want = oracle.l2_error_sine(ob, degree, nq, plain, u_used)
         assert abs(got - want) <= 1e-12 * want
+
+
+# ---- the deal.II-style formulation (PMG_GEOMETRY_INVJAC: J^{-1} and JxW per point) ----
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+@pytest.mark.parametrize("boxname,kind", [("deformed_r2", pmg.COEFF_NONE), ("ragged_3x2x1", pmg.COEFF_NONE),
+                                          ("deformed_r2", pmg.COEFF_KAPPA), ("single_cell", pmg.COEFF_NONE)])
+def test_invjac_vmult_matches_oracle_invjac(oracle, degree, dtype, boxname, kind):
+    """The inverse-Jacobian formulation on the GPU against the oracle's restatement of
+    portable_local_laplace_operator.h:329-347 (orc_vmult_invjac)."""
+    box = pmg.Box.make(**BOXES[boxname])
+    ob = obox(oracle, box)
+    op = pmg.LaplaceOperator(pmg.Mesh(box), degree, dtype, pmg.GEOMETRY_INVJAC, kind)
+    plain, cons, idx = oracle.dofs(ob, degree)
+    iJ, jxw = oracle.invjac(ob, degree, coeff_kind=kind)
+    src = random_src(op.m(), 11)
+    ref = oracle.vmult_invjac(degree, idx, iJ, jxw, cons, src)
+    s = torch.tensor(src, dtype=tdtype(dtype), device="cuda")
+    d = op.initialize_dof_vector()
+    op.vmult(d, s)
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype]
+    # the same operator as the G formulation
+    ref_g = oracle.vmult(degree, idx, oracle.geometry_G(ob, degree, coeff_kind=kind), cons, src)
+    assert rel_err(d.double().cpu().numpy(), ref_g) < TOL[dtype]
+
+
+@pytest.mark.parametrize("degree", [2, 4, 6])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+def test_invjac_diagonal_matches_oracle(oracle, degree, dtype):
+    box = pmg.Box.make(coarse=(2, 1, 1), refine=1, hi=(2.0, 1.0, 1.0), deform=1)
+    ob = obox(oracle, box)
+    op = pmg.LaplaceOperator(pmg.Mesh(box), degree, dtype, pmg.GEOMETRY_INVJAC)
+    plain, cons, idx = oracle.dofs(ob, degree)
+    ref = oracle.diagonal(degree, idx, oracle.geometry_G(ob, degree), cons)
+    op.compute_diagonal()
+    inv = op.get_matrix_diagonal_inverse()
+    torch.cuda.synchronize()
+    assert rel_err(1.0 / inv.double().cpu().numpy(), ref) < TOL[dtype] * 10
+
+
+def test_invjac_multigrid_solve_matches_g_formulation():
+    """A Q4 ph-multigrid CG solve on the deformed cube with every level in the inverse-Jacobian
+    formulation takes the iterations of the G formulation and reaches the same solution."""
+    box = pmg.Box.make(refine=3, deform=1)
+    res = {}
+    for geom in (pmg.GEOMETRY_FULL, pmg.GEOMETRY_INVJAC):
+        h = pmg.Hierarchy(box, [4, 2, 1], mg_dtype=pmg.F32, cheb_degree=4, geometry=geom)
+        b = h.fine64.assemble_rhs(1)
+        h.estimate()
+        x, info = h.solve(b, reduce=1e-10)
+        res[geom] = (x.cpu().numpy(), info["iterations"])
+    assert res[pmg.GEOMETRY_INVJAC][1] == res[pmg.GEOMETRY_FULL][1]
+    assert rel_err(res[pmg.GEOMETRY_INVJAC][0], res[pmg.GEOMETRY_FULL][0]) < 1e-9
+
+
+def test_invjac_rejects_the_per_point_form():
+    op = pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(refine=1)), 2, pmg.F64, pmg.GEOMETRY_INVJAC)
+    u = torch.zeros(op.m(), dtype=torch.float64, device="cuda")
+    with pytest.raises(pmg.PmgError):
+        op.qp_form(u, u, 1.0)
