@@ -57,18 +57,25 @@ __device__ __forceinline__ void face_flux(const DGTab<N, T> &tab, const DGGeo &g
   const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
   const T *dphi_nb = sd ? tab.dphi0 : tab.dphi1;
   const T *uo = src + c * N3;
-  const T vo = __ldg(uo + face_node<N>(d, own_layer, a, bb));
-  T dn = T(0);
+  // the N values along the normal: the face value is one of them
+  T vo = T(0), dn = T(0);
 #pragma unroll
-  for (int i = 0; i < N; ++i) dn += dphi_own[i] * __ldg(uo + face_node<N>(d, i, a, bb));
+  for (int i = 0; i < N; ++i) {
+    const T x = __ldg(uo + face_node<N>(d, i, a, bb));
+    if (i == own_layer) vo = x;
+    dn += dphi_own[i] * x;
+  }
   dn *= sgn_h;
   const int32_t nb = __ldg(nbr + c * 6 + F);
   if (nb >= 0) {
     const T *un = src + int64_t(nb) * N3;
-    const T vn = __ldg(un + face_node<N>(d, nb_layer, a, bb));
-    T dnn = T(0);
+    T vn = T(0), dnn = T(0);
 #pragma unroll
-    for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * __ldg(un + face_node<N>(d, i, a, bb));
+    for (int i = 0; i < N; ++i) {
+      const T x = __ldg(un + face_node<N>(d, i, a, bb));
+      if (i == nb_layer) vn = x;
+      dnn += dphi_nb[i] * x;
+    }
     dnn *= sgn_h;
     const T jump = vo - vn;
     f1 = sigma * jump - T(0.5) * (dn + dnn);
@@ -92,7 +99,9 @@ template <int N> constexpr int dg_threads() { return ((6 * dg_batch<N>() * N * N
 //      the value-test and normal-derivative-test coefficients of every face point;
 //   4. one thread per cell node sums what the six faces give it: the value test where the
 //      node lies on the face layer, and the normal-derivative test on every layer.
-// Three block barriers per batch, no shared-memory atomics.
+// Phases 1-3 exchange data only among the N^2 threads of one face of one cell; where N^2
+// divides 32 (N = 2, 4) those threads lie in one warp and a warp barrier orders them, so a
+// batch takes two block barriers instead of four.  No shared-memory atomics.
 template <int N, typename T>
 __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __grid_constant__ DGTab<N, T> tab,
                                                                   const __grid_constant__ DGGeo geo,
@@ -110,6 +119,11 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
   const T sgn_h = t < FP ? (sd ? T(1) : T(-1)) / (T)geo.h[d] : T(0); // n . grad = sgn_h d/dxi_d
   const T area = t < FP ? (T)(geo.h[ta] * geo.h[tb]) : T(0);
   const T sigma = t < FP ? (T)(geo.c_pen / geo.h[d]) : T(0);
+  // a face's N^2 threads share a warp when N^2 divides 32 (blockDim is a multiple of 32)
+  auto face_sync = [] {
+    if constexpr (32 % (N * N) == 0) __syncwarp();
+    else __syncthreads();
+  };
   for (int64_t base = int64_t(blockIdx.x) * B; base < n_cells; base += int64_t(gridDim.x) * B) {
     if (t < FP) {
       const int64_t c = base + b;
@@ -129,7 +143,7 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
       F1[f][b][ab] = f1 * area;
       F2[f][b][ab] = f2 * area;
     }
-    __syncthreads();
+    face_sync();
     if (t < FP) { // face mass along a
       T g1 = T(0), g2 = T(0);
 #pragma unroll
@@ -140,7 +154,7 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
       G1[f][b][ab] = g1;
       G2[f][b][ab] = g2;
     }
-    __syncthreads();
+    face_sync();
     if (t < FP) { // along b: value-test and normal-test coefficients (F1/F2 reused)
       T tv = T(0), tn = T(0);
 #pragma unroll
