@@ -183,6 +183,13 @@ pmg_status pmg_operator_interpolate_coefficient(pmg_operator *dst, pmg_operator 
  * FEValues error loop of tests/poisson_cube_bk3/program.cc.  Synchronises. */
 pmg_status pmg_operator_l2_error(const pmg_operator *op, const void *u, int32_t exact_kind, int32_t nq,
                                  double *error, void *stream);
+/* Support point of every DoF, device array xyz[n_dofs][3] (FP64): where Dirichlet data is
+ * evaluated, as deal.II's VectorTools::interpolate_boundary_values does for the constraints
+ * (source/plain_solver/program.cc:125-131, homogeneous there).  With it inhomogeneous data is
+ * imposed by lifting: u_D = g at the Dirichlet DoFs (0 elsewhere), b0 = b - A0 u_D on the free
+ * rows (A0 the operator of the same mesh without Dirichlet DoFs), solve A u0 = b0, u = u0 + u_D.
+ * Synchronises. */
+pmg_status pmg_operator_dof_coordinates(const pmg_operator *op, double *xyz, void *stream);
 /* Quadrature points of the operator's Gauss rule, device array xq[C][nq^3][3] (FP64). */
 pmg_status pmg_operator_quadrature_points(const pmg_operator *op, double *xq, void *stream);
 /* out[c][q] = alpha * grad u(x_q)^T kappa_q |det J| w_q J^{-1} J^{-T} grad v(x_q) in reference

@@ -295,6 +295,14 @@ pmg_status pmg_operator_l2_error(const pmg_operator *op, const void *u, int32_t 
   });
 }
 
+pmg_status pmg_operator_dof_coordinates(const pmg_operator *op, double *xyz, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(xyz);
+    pmg::operator_dof_coordinates(*op, xyz, as_stream(stream));
+  });
+}
+
 pmg_status pmg_operator_quadrature_points(const pmg_operator *op, double *xq, void *stream) {
   return guarded(__func__, [&] {
     NEED(op);

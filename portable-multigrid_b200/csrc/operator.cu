@@ -54,7 +54,9 @@ __device__ __forceinline__ double coefficient(int kind, const double x[3]) {
 // mode 5: out[cell] = (sum_q (u_h(x_q) - u(x_q))^2 |det J| w_q)^(1/2) for the exact solution
 //         u of f_kind 1 (sin(pi x) sin(pi y) sin(pi z)) or 2 (exp(x) sin(pi y) cos(pi z));
 // mode 6: write J^{-1} (9 entries, row d = d xi_d / dx) and coef * |det J| w_q into the slab
-//         layout of the inverse-Jacobian formulation, [group][x point][y point][10][lane].
+//         layout of the inverse-Jacobian formulation, [group][x point][y point][10][lane];
+// mode 7: out[dof][3] = the mapped position of every node (DoFs shared by cells receive the
+//         same value from each of them).
 template <typename T>
 __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restrict__ cell_xyz,
                                      int64_t n_cells, int mode, int coeff_kind,
@@ -74,6 +76,13 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
                             g.lo[2] + (cz + g.xl[k]) * g.h[2]};
       double xp[3];
       map_point(g, xr, xp);
+      if (mode == 7) {
+        const uint32_t d = plain[c * nm3 + l];
+        out[3 * int64_t(d)] = (T)xp[0];
+        out[3 * int64_t(d) + 1] = (T)xp[1];
+        out[3 * int64_t(d) + 2] = (T)xp[2];
+        continue;
+      }
       X[0][l] = xp[0];
       X[1][l] = xp[1];
       X[2][l] = xp[2];
@@ -82,6 +91,7 @@ __global__ void cell_geometry_kernel(const GeoParams g, const int32_t *__restric
         U[l] = u_f32 ? (double)static_cast<const float *>(uvec)[d] : static_cast<const double *>(uvec)[d];
       }
     }
+    if (mode == 7) continue; // uniform over the block: no shared memory was written
     __syncthreads();
     for (int q = threadIdx.x; q < nq3; q += blockDim.x) {
       const int q0 = q % nq, q1 = (q / nq) % nq, q2 = q / (nq * nq);
@@ -673,6 +683,22 @@ void operator_qp_form(const pmg_operator &op, const void *u, const void *v, doub
 
 // ||u_h - u||_{L2} with an nq-point Gauss rule per direction; every DoF's value counts,
 // Dirichlet ones included (the plain index map is uploaded for the call).
+// xyz[dof][3] (device, FP64) = the mapped support point of every DoF, for boundary data
+// (the points at which deal.II's VectorTools::interpolate_boundary_values evaluates the
+// Dirichlet function, source/plain_solver/program.cc:125-131)
+void operator_dof_coordinates(const pmg_operator &op, double *xyz, cudaStream_t s) {
+  PMG_REQUIRE(xyz, "null output");
+  PMG_CUDA(cudaSetDevice(op.device));
+  if (op.n_cells == 0) return;
+  DeviceBuffer plain = upload(op.num.plain);
+  const GeoParams gp = make_geo_params(op, op.nq);
+  const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)op.sms * 16);
+  cell_geometry_kernel<double><<<grid, 128, 0, s>>>(gp, op.cell_xyz.as<int32_t>(), op.n_cells, 7, 0, nullptr, xyz,
+                                                    nullptr, 0, nullptr, plain.as<uint32_t>(), 0);
+  PMG_LAUNCH_CHECK();
+  PMG_CUDA(cudaStreamSynchronize(s)); // the plain index map is freed on return
+}
+
 double operator_l2_error(const pmg_operator &op, const void *u, int exact_kind, int nq, cudaStream_t s) {
   PMG_REQUIRE(u, "null vector");
   PMG_REQUIRE(exact_kind == 1 || exact_kind == 2, "exact_kind must be 1 (sine) or 2 (exp-sine-cosine)");

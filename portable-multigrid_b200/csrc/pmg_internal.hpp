@@ -222,6 +222,7 @@ void operator_set_coefficient(pmg_operator &op, const double *values, bool on_de
 void operator_interpolate_coefficient(pmg_operator &dst, pmg_operator &src, cudaStream_t s);
 void operator_quadrature_points(const pmg_operator &op, double *xq, cudaStream_t s);
 double operator_l2_error(const pmg_operator &op, const void *u, int exact_kind, int nq, cudaStream_t s);
+void operator_dof_coordinates(const pmg_operator &op, double *xyz, cudaStream_t s);
 void operator_qp_form(const pmg_operator &op, const void *u, const void *v, double alpha, double *out,
                       cudaStream_t s);
 } // namespace pmg

@@ -162,6 +162,7 @@ def _declare(L):
         "pmg_operator_interpolate_coefficient": ([vp, vp, vp], i32),
         "pmg_operator_quadrature_points": ([vp, vp, vp], i32),
         "pmg_operator_l2_error": ([vp, vp, i32, i32, P(d), vp], i32),
+        "pmg_operator_dof_coordinates": ([vp, vp, vp], i32),
         "pmg_operator_qp_form": ([vp, vp, vp, d, vp, vp], i32),
         "pmg_mg_set_coefficient": ([vp, vp, vp, i32, vp], i32),
         "pmg_adjoint_gradient": ([vp, vp, vp, vp, vp, vp, vp, P(d), d, d, i32, P(CGInfo), vp], i32),
@@ -386,6 +387,13 @@ class LaplaceOperator:
         check(lib().pmg_operator_l2_error(self.h, _ptr(u), exact_kind, nq, C.byref(e), _stream()))
         return e.value
 
+    def dof_coordinates(self):
+        """Support point of every DoF, float64 CUDA tensor [m, 3]."""
+        import torch
+        xyz = torch.empty((self.m(), 3), dtype=torch.float64, device=f"cuda:{self.device}")
+        check(lib().pmg_operator_dof_coordinates(self.h, _ptr(xyz), _stream()))
+        return xyz
+
     def quadrature_points(self):
         """Gauss points of every cell, float64 CUDA tensor [C, nq^3, 3]."""
         import torch
@@ -553,6 +561,8 @@ class Hierarchy:
             self.fine64 = LaplaceOperator(self.meshes[-1], pseq[0], F64, geometry, coeff_kind,
                                           coeff_qp, device)
         self.mg = VCycleMultigrid(self.levels, self.transfers, self.smoothers)
+        self._fine_args = (pseq[0], geometry, coeff_kind, coeff_qp, device, dg)
+        self._lift_op = None
 
     def set_coefficient(self, values):
         """New coefficient values [C, nq^3] (float64, CUDA tensor or host array) for the CG
@@ -575,6 +585,34 @@ class Hierarchy:
             x = self.fine64.initialize_dof_vector()
         info = solve_cg(self.fine64, x, b, self.mg, reduce, abs_tol, max_iterations)
         return x, info
+
+    def solve_dirichlet(self, b, g, reduce=1e-9, abs_tol=1e-16, max_iterations=100):
+        """Solve with inhomogeneous Dirichlet data by lifting (the reference imposes
+        homogeneous data only).  g maps the DoF support points (float64 CUDA tensor [m, 3]) to
+        the boundary values; b is the right-hand side of pmg_operator_assemble_rhs (zero on
+        the Dirichlet rows).  u_D = g at the Dirichlet DoFs and 0 elsewhere; b0 = b - A0 u_D on
+        the free rows, with A0 the same operator on the same mesh without Dirichlet DoFs (the
+        numbering does not depend on them); u = u0 + u_D with A u0 = b0.  Returns (u, info)."""
+        import torch
+        degree, geometry, coeff_kind, coeff_qp, device, dg = self._fine_args
+        if dg:
+            raise ValueError("DG operators take Dirichlet data weakly (pmg_operator_assemble_rhs)")
+        A = self.fine64
+        if self._lift_op is None:
+            b0x = self.box
+            free_box = Box.make(tuple(b0x.coarse), b0x.refine, tuple(b0x.lo), tuple(b0x.hi), b0x.deform,
+                                b0x.amp, 0)
+            self._lift_mesh = Mesh(free_box)
+            self._lift_op = LaplaceOperator(self._lift_mesh, degree, F64, geometry, coeff_kind, coeff_qp, device)
+            self._lift_cons = torch.as_tensor(A.constrained().astype(bool), device=f"cuda:{device}")
+        cons = self._lift_cons
+        xyz = A.dof_coordinates()
+        u_d = torch.where(cons, g(xyz).to(torch.float64), torch.zeros((), dtype=torch.float64, device=xyz.device))
+        r = torch.empty_like(u_d)
+        self._lift_op.vmult(r, u_d)
+        b0 = torch.where(cons, torch.zeros((), dtype=torch.float64, device=xyz.device), b - r)
+        u0, info = self.solve(b0, reduce=reduce, abs_tol=abs_tol, max_iterations=max_iterations)
+        return u0 + u_d, info
 
 
 def adjoint_gradient(A: LaplaceOperator, M: LaplaceOperator, u, u_d, precond: VCycleMultigrid | None = None,
