@@ -246,3 +246,28 @@ def test_invjac_rejects_the_per_point_form():
     u = torch.zeros(op.m(), dtype=torch.float64, device="cuda")
     with pytest.raises(pmg.PmgError):
         op.qp_form(u, u, 1.0)
+
+
+@pytest.mark.parametrize("degree", [3, 5])
+def test_invjac_coefficient_values_and_update_match_g(degree):
+    """Per-point coefficient values folded into JxW (and replaced later) give the operator of
+    the G formulation with the same values."""
+    box = pmg.Box.make(refine=2, deform=1)
+    mesh = pmg.Mesh(box)
+    nq3 = (degree + 1) ** 3
+    rng = np.random.default_rng(degree)
+    k1 = np.exp(rng.uniform(-0.5, 0.5, (mesh.n_cells(), nq3)))
+    k2 = np.exp(rng.uniform(-0.5, 0.5, (mesh.n_cells(), nq3)))
+    ops = [pmg.LaplaceOperator(mesh, degree, pmg.F64, g, pmg.COEFF_VALUES, k1)
+           for g in (pmg.GEOMETRY_FULL, pmg.GEOMETRY_INVJAC)]
+    s = torch.tensor(random_src(ops[0].m(), 5), dtype=torch.float64, device="cuda")
+    for values in (None, k2):
+        out = []
+        for op in ops:
+            if values is not None:
+                op.set_coefficient(values)
+            d = op.initialize_dof_vector()
+            op.vmult(d, s)
+            out.append(d.cpu().numpy())
+        torch.cuda.synchronize()
+        assert rel_err(out[1], out[0]) < 1e-12
