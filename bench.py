@@ -361,14 +361,27 @@ def q6_kernel_rates(torch, pmg, dev, peaks, refine=4, launches=20):
     return res
 
 
+# the reference's logged GH200 figures for the doubling-mesh solve (seconds, CG iterations)
+REFERENCE_LOGS = {
+    # one GH200: tests/poisson_cube_bk3_fp64/results/single-gpu-batched.out:1172-1184 and
+    # tests/poisson_cube_bk3/results/signle-gpu-batched-mixed-precision.out:1262-1281
+    20: {"gpus": 1, "fp64_mg_seconds": 0.5695, "fp32_mg_seconds": 0.4902, "iterations": 5,
+         "fp64_mg_setup_seconds": 129.87, "fp32_mg_setup_seconds": 194.33},
+    # four GH200 (MPI): tests/poisson_cube_bk3_fp64/results/1-node-batched.out:1388,1417,1463 and
+    # tests/poisson_cube_bk3/results/1-node-batched-mixed-precision.out:1485,1514,1560
+    22: {"gpus": 4, "fp64_mg_seconds": 0.77931, "fp32_mg_seconds": 0.61183, "iterations": 5,
+         "fp64_mg_setup_seconds": 136.41, "fp32_mg_setup_seconds": 206.83},
+}
+
+
 def reference_problem(torch, pmg, dev, cycle=20, repeats=3):
     """The reference's own logged solve: Q4, f = 1, homogeneous Dirichlet on the "doubling" mesh
-    of cycle 20 (2 x 2 x 1 coarse cells refined 6 times, 67,634,433 DoFs), ph-multigrid with
-    p 4 -> 3 -> 2 -> 1 and Q1 h-levels, Chebyshev(5), CG to a reduction of 1e-9, all-FP64 and with
-    the FP32 V-cycle; setup (hierarchy, right-hand side, eigenvalue estimates) and solve times
-    next to the GH200 figures the reference logged for the same problem
-    (tests/poisson_cube_bk3_fp64/results/single-gpu-batched.out:1172-1184 and
-    tests/poisson_cube_bk3/results/signle-gpu-batched-mixed-precision.out:1262-1281)."""
+    of `cycle` (cycle 20: 2 x 2 x 1 coarse cells refined 6 times, 67,634,433 DoFs; cycle 22:
+    269,748,225 DoFs), ph-multigrid with p 4 -> 3 -> 2 -> 1 and Q1 h-levels, Chebyshev(5), CG to
+    a reduction of 1e-9, all-FP64 and with the FP32 V-cycle; setup (hierarchy, right-hand side,
+    eigenvalue estimates) and solve times on this one GPU next to the GH200 figures the
+    reference logged for the same problem (REFERENCE_LOGS: one GH200 at cycle 20, four at
+    cycle 22)."""
     box = pmg.doubling_box(cycle)
     res = {}
     for name, dt in (("fp64_mg", pmg.F64), ("fp32_mg", pmg.F32)):
@@ -396,11 +409,12 @@ def reference_problem(torch, pmg, dev, cycle=20, repeats=3):
         del h, b, x
         torch.cuda.empty_cache()
     res["n_dofs"] = n
-    res["reference_gh200"] = {"fp64_mg_seconds": 0.5695, "fp32_mg_seconds": 0.4902, "iterations": 5,
-                              "fp64_mg_setup_seconds": 129.87, "fp32_mg_setup_seconds": 194.33}
-    res["speedup_vs_reference"] = {"fp64_mg": 0.5695 / res["fp64_mg"]["seconds"],
-                                   "fp32_mg": 0.4902 / res["fp32_mg"]["seconds"]}
-    res["config"] = "Q4 doubling mesh cycle 20, p 4-3-2-1 + Q1 h-levels, Chebyshev(5), CG to 1e-9"
+    ref = REFERENCE_LOGS[cycle]
+    res["reference_gh200"] = ref
+    res["speedup_vs_reference"] = {"fp64_mg": ref["fp64_mg_seconds"] / res["fp64_mg"]["seconds"],
+                                   "fp32_mg": ref["fp32_mg_seconds"] / res["fp32_mg"]["seconds"]}
+    res["config"] = (f"Q4 doubling mesh cycle {cycle}, p 4-3-2-1 + Q1 h-levels, Chebyshev(5), CG to 1e-9; "
+                     f"one B200 against {ref['gpus']} GH200")
     return res
 
 
@@ -550,13 +564,14 @@ def gpu_arm(args):
         del op32
 
     tts = None
-    if not args.skip_solve:
+    if not args.skip_solve and world == 1:  # the solver figures are single-GPU measurements
         del op, src, dst
         torch.cuda.empty_cache()
         tts = time_to_solution(torch, pmg, dev)
         tts["q6_cell_kernels"] = q6_kernel_rates(torch, pmg, dev, peaks)
         extra["dg_time_to_1e-10"] = dg_time_to_solution(torch, pmg, dev)
         extra["reference_problem"] = reference_problem(torch, pmg, dev)
+        extra["reference_problem_4gpu"] = reference_problem(torch, pmg, dev, cycle=22, repeats=2)
         extra["adjoint_gradient"] = adjoint_check(torch, pmg, dev)
 
     cpu = None
