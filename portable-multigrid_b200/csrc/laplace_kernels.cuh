@@ -314,9 +314,20 @@ __device__ __forceinline__ void load_g6(const T *__restrict__ geo, const T *gs,
 
 // resident blocks of 128 threads per SM the register allocation is sized for; matches the
 // shared-memory footprint (3 exchange buffers per warp) of each degree and type
+// FP64 affine kernels at 3 <= N <= 5: 0 plain runtime loops, 1 with even/odd z contractions,
+// 2 (default) unrolled with every even/odd form at up to 255 registers, which measured fastest
+// on B200 despite some spills (64^3 / 48^3 with kappa: Q4 217 -> 174 us, Q3 205 -> 200 us,
+// Q2 74 -> 67 us; mode 1: 210, 199, 72 us)
+#ifndef PMG_VMULT_F64_AFFINE_MODE
+#define PMG_VMULT_F64_AFFINE_MODE 2
+#endif
+template <int N, typename T, int GEOM> constexpr int f64_affine_mode_v =
+    (sizeof(T) == 8 && N <= 5 && N >= 3 && (GEOM == 1 || GEOM == 2)) ? PMG_VMULT_F64_AFFINE_MODE : 0;
 template <int N, typename T, int GEOM = 1> struct MinBlocks {
   static constexpr int value =
-      sizeof(T) == 8 ? (N >= 6 ? 2 : 3) : ((N == 7 && (GEOM == 0 || GEOM == 3)) ? 3 : 2);
+      f64_affine_mode_v<N, T, GEOM> == 2
+          ? 2
+          : (sizeof(T) == 8 ? (N >= 6 ? 2 : 3) : ((N == 7 && (GEOM == 0 || GEOM == 3)) ? 3 : 2));
 };
 // outer streaming loops: runtime loops for FP64 (bounded live registers), unrolled for FP32
 // (registers are cheap at 4 bytes and unrolling keeps the tables as immediate operands),
@@ -325,7 +336,9 @@ template <int N, typename T, int GEOM = 1> struct MinBlocks {
 // (FP32 Q6 affine in runtime loops at 142 registers, 12 warps/SM, measured no faster than the
 // unrolled form at 8 warps/SM)
 template <int N, typename T, int GEOM = 1> struct Unroll {
-  static constexpr int value = (sizeof(T) == 8 || (N == 7 && (GEOM == 0 || GEOM == 3))) ? 1 : N;
+  static constexpr int value = f64_affine_mode_v<N, T, GEOM> == 2
+                                   ? N
+                                   : ((sizeof(T) == 8 || (N == 7 && (GEOM == 0 || GEOM == 3))) ? 1 : N);
 };
 
 // Shared memory per warp of vmult_slab_kernel: 3 exchange buffers, plus (SMEM_G) the
@@ -366,19 +379,20 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   constexpr int UNR = SMEM_G ? N : Unroll<N, T, GEOM>::value;
   // even/odd contractions where they measured faster on B200 (the FP64 runtime-loop
   // variants spill with the extra live values; N = 2 gains nothing):
-  //  EO   z contractions of phases 1 and 3: the ring variants and the FP32 direct variants
-  //       other than N = 6 and N = 7 full geometry
+  //  EO   z contractions of phases 1 and 3: the ring variants, the FP32 direct variants
+  //       other than N = 6 and N = 7 full geometry, and the FP64 affine kernels at N <= 5
   //  EO2  phase 2 (the y contractions of the columns, the x contraction of fz): the ring
-  //       variants, FP32 N <= 5 and every N = 7 variant
+  //       variants, FP32 N <= 5, every N = 7 variant and the unrolled FP64 affine kernels
   //  EO1X x contractions of phase 1 by mirrored pairs of points (the point loop unrolled):
   //       with EO except at N = 6
   //  DEFER (below) phase 2 without register accumulators, at N = 7
   constexpr bool EO =
-      N >= 3 && (SMEM_G || (sizeof(T) == 4 && N != 6 && !(N == 7 && (GEOM == 0 || GEOM == 3))));
+      N >= 3 && (SMEM_G || (sizeof(T) == 4 && N != 6 && !(N == 7 && (GEOM == 0 || GEOM == 3))) ||
+                 f64_affine_mode_v<N, T, GEOM> >= 1);
   constexpr bool EO2 =
       PMG_VMULT_EO_PHASE2 >= 0
           ? (PMG_VMULT_EO_PHASE2 == 1 && N >= 3)
-          : N >= 3 && (SMEM_G || (sizeof(T) == 4 && N <= 5) || N == 7);
+          : N >= 3 && (SMEM_G || (sizeof(T) == 4 && N <= 5) || N == 7 || f64_affine_mode_v<N, T, GEOM> == 2);
   // DEFER: phase 2 keeps no accumulators; y1, y2 and x3 are parked in the lane's own plane and
   // contracted along x (and y) afterwards in even/odd form (N = 7: 8-35 % faster on B200,
   // the runtime-loop FP64 variants lose their spills; slower at N <= 6)
