@@ -318,11 +318,15 @@ __device__ __forceinline__ void load_g6(const T *__restrict__ geo, const T *gs,
 // 2 (default) unrolled with every even/odd form at up to 255 registers, which measured fastest
 // on B200 despite some spills (64^3 / 48^3 with kappa: Q4 217 -> 174 us, Q3 205 -> 200 us,
 // Q2 74 -> 67 us; mode 1: 210, 199, 72 us)
+// (at N = 6 and 7 the unrolled FP64 form spills 0.5-1.4 KB and measured 1.6-2.1x slower)
+#ifndef PMG_VMULT_F64_AFFINE_NMAX
+#define PMG_VMULT_F64_AFFINE_NMAX 5
+#endif
 #ifndef PMG_VMULT_F64_AFFINE_MODE
 #define PMG_VMULT_F64_AFFINE_MODE 2
 #endif
 template <int N, typename T, int GEOM> constexpr int f64_affine_mode_v =
-    (sizeof(T) == 8 && N <= 5 && N >= 3 && (GEOM == 1 || GEOM == 2)) ? PMG_VMULT_F64_AFFINE_MODE : 0;
+    (sizeof(T) == 8 && N <= PMG_VMULT_F64_AFFINE_NMAX && N >= 3 && (GEOM == 1 || GEOM == 2)) ? PMG_VMULT_F64_AFFINE_MODE : 0;
 template <int N, typename T, int GEOM = 1> struct MinBlocks {
   static constexpr int value =
       f64_affine_mode_v<N, T, GEOM> == 2
