@@ -13,6 +13,9 @@ ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
 LOGS = {
     "fp64": "tests/poisson_cube_bk3_fp64/results/single-gpu-batched.out",
     "mixed": "tests/poisson_cube_bk3/results/signle-gpu-batched-mixed-precision.out",
+    # one node, four GPUs over MPI
+    "fp64_4gpu": "tests/poisson_cube_bk3_fp64/results/1-node-batched.out",
+    "mixed_4gpu": "tests/poisson_cube_bk3/results/1-node-batched-mixed-precision.out",
 }
 
 
@@ -37,12 +40,29 @@ def parse(rel):
     return rows
 
 
+def parse_setup(rel):
+    """{cycle: {"seconds": total setup time, "source": file:line}} (the first 'Total setup
+    time' after each 'Cycle N' line)."""
+    out, cycle = {}, None
+    with open(os.path.join(ROOT, rel)) as f:
+        for j, line in enumerate(f):
+            m = re.match(r"^Cycle (\d+)", line)
+            if m:
+                cycle = int(m.group(1))
+                continue
+            m = re.search(r"Total setup time: (\S+)", line)
+            if m and cycle is not None and str(cycle) not in out:
+                out[str(cycle)] = {"seconds": float(m.group(1)), "source": f"{rel}:{j + 1}"}
+    return out
+
+
 def main():
     out = {
         "what": "Q4 ph-multigrid CG on the doubling mesh, f=1, Chebyshev degree 5, range 15, "
                 "10 eigenvalue iterations, ReductionControl(100,1e-16,1e-9); logged by the "
-                "reference (1 GPU).",
+                "reference (1 GPU; the *_4gpu tables: one node, 4 GPUs over MPI).",
         "tables": {k: parse(v) for k, v in LOGS.items()},
+        "setup": {k: parse_setup(v) for k, v in LOGS.items()},
     }
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_logs.json")
     with open(dst, "w") as f:
