@@ -48,7 +48,25 @@ template <int N> __device__ __forceinline__ int face_node(int d, int layer, int 
 
 // flux values of face F (compile time, so the node indexing folds to constants) at face point
 // (a, bb) of cell c: f1 = sigma [u] - {d_n u}, f2 = -[u]/2 (Dirichlet: mirror u+ = -u-)
-template <int N, typename T, int F>
+// the N values of cell u along the normal of face direction d at face point (a, b): for d = 0
+// they are contiguous and, with VEC (src 16-byte aligned, N * sizeof(T) a multiple of 16), read
+// as 16-byte vectors
+template <int N, typename T, int d, bool VEC>
+__device__ __forceinline__ void normal_line(const T *__restrict__ u, int a, int bb, T (&line)[N]) {
+  if constexpr (d == 0 && VEC) {
+    const float4 *p = reinterpret_cast<const float4 *>(u + face_node<N>(0, 0, a, bb));
+#pragma unroll
+    for (int v = 0; v < N * (int)sizeof(T) / 16; ++v) {
+      const float4 w = __ldg(p + v);
+      memcpy(line + v * (16 / (int)sizeof(T)), &w, 16);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) line[i] = __ldg(u + face_node<N>(d, i, a, bb));
+  }
+}
+
+template <int N, typename T, int F, bool VEC>
 __device__ __forceinline__ void face_flux(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ src,
                                           const int32_t *__restrict__ nbr, int64_t c, int a, int bb, T sgn_h,
                                           T sigma, T &f1, T &f2) {
@@ -58,24 +76,21 @@ __device__ __forceinline__ void face_flux(const DGTab<N, T> &tab, const DGGeo &g
   const T *dphi_nb = sd ? tab.dphi0 : tab.dphi1;
   const T *uo = src + c * N3;
   // the N values along the normal: the face value is one of them
-  T vo = T(0), dn = T(0);
+  T line[N];
+  normal_line<N, T, d, VEC>(uo, a, bb, line);
+  const T vo = line[own_layer];
+  T dn = T(0);
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    const T x = __ldg(uo + face_node<N>(d, i, a, bb));
-    if (i == own_layer) vo = x;
-    dn += dphi_own[i] * x;
-  }
+  for (int i = 0; i < N; ++i) dn += dphi_own[i] * line[i];
   dn *= sgn_h;
   const int32_t nb = __ldg(nbr + c * 6 + F);
   if (nb >= 0) {
     const T *un = src + int64_t(nb) * N3;
-    T vn = T(0), dnn = T(0);
+    normal_line<N, T, d, VEC>(un, a, bb, line);
+    const T vn = line[nb_layer];
+    T dnn = T(0);
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-      const T x = __ldg(un + face_node<N>(d, i, a, bb));
-      if (i == nb_layer) vn = x;
-      dnn += dphi_nb[i] * x;
-    }
+    for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * line[i];
     dnn *= sgn_h;
     const T jump = vo - vn;
     f1 = sigma * jump - T(0.5) * (dn + dnn);
@@ -102,7 +117,7 @@ template <int N> constexpr int dg_threads() { return ((6 * dg_batch<N>() * N * N
 // Phases 1-3 exchange data only among the N^2 threads of one face of one cell; where N^2
 // divides 32 (N = 2, 4) those threads lie in one warp and a warp barrier orders them, so a
 // batch takes two block barriers instead of four.  No shared-memory atomics.
-template <int N, typename T>
+template <int N, typename T, bool VEC>
 __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __grid_constant__ DGTab<N, T> tab,
                                                                   const __grid_constant__ DGGeo geo,
                                                                   const T *__restrict__ src,
@@ -132,12 +147,12 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
         // f is uniform over a warp where B * N^2 is a multiple of 32 (N = 2, 4); elsewhere a
         // warp can span two faces and takes both branches
         switch (f) {
-        case 0: face_flux<N, T, 0>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
-        case 1: face_flux<N, T, 1>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
-        case 2: face_flux<N, T, 2>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
-        case 3: face_flux<N, T, 3>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
-        case 4: face_flux<N, T, 4>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
-        default: face_flux<N, T, 5>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 0: face_flux<N, T, 0, VEC>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 1: face_flux<N, T, 1, VEC>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 2: face_flux<N, T, 2, VEC>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 3: face_flux<N, T, 3, VEC>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        case 4: face_flux<N, T, 4, VEC>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
+        default: face_flux<N, T, 5, VEC>(tab, geo, src, nbr, c, a, bb, sgn_h, sigma, f1, f2); break;
         }
       }
       F1[f][b][ab] = f1 * area;
@@ -367,10 +382,16 @@ void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, i
     } else {
       constexpr int B = dg_batch<N>();
       const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 8);
-      dg_face_kernel<N, T><<<std::max(grid, 1), dg_threads<N>(), 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
-                                                                         static_cast<const T *>(src),
-                                                                         static_cast<T *>(dst), h.nbr.as<int32_t>(),
-                                                                         n_cells);
+      // 16-byte loads of the x-normal lines where the rows allow them and src is aligned
+      constexpr bool rows16 = (N * sizeof(T)) % 16 == 0;
+      if (rows16 && reinterpret_cast<uintptr_t>(src) % 16 == 0)
+        dg_face_kernel<N, T, rows16><<<std::max(grid, 1), dg_threads<N>(), 0, s>>>(
+            make_dg_tab<N, T>(h), make_geo(h), static_cast<const T *>(src), static_cast<T *>(dst),
+            h.nbr.as<int32_t>(), n_cells);
+      else
+        dg_face_kernel<N, T, false><<<std::max(grid, 1), dg_threads<N>(), 0, s>>>(
+            make_dg_tab<N, T>(h), make_geo(h), static_cast<const T *>(src), static_cast<T *>(dst),
+            h.nbr.as<int32_t>(), n_cells);
     }
   }
   PMG_LAUNCH_CHECK();
