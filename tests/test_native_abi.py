@@ -43,3 +43,19 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(pmg.PmgError) as e:
         pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(refine=1)), 2)
     assert e.value.status == -8
+
+
+def test_new_entry_points_reject_null_arguments():
+    L = pmg.lib()
+    assert L.pmg_operator_dof_coordinates(None, None, None) == -1
+    assert L.pmg_measure_peaks(0, 1 << 30, None) == -1
+    assert "NULL" in pmg.last_error()
+
+
+def test_peaks_need_a_device():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(pmg.PmgError) as e:
+        pmg.measure_peaks(0, 1 << 30)
+    assert e.value.status == -8
