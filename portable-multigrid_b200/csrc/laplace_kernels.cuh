@@ -250,7 +250,9 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
 //   phase 3 (Y-slab), per x node i:        out = Sz^T a + SDz^T c, scatter
 // Each lane overwrites only its own slab's region of the buffers between the two
 // exchanges, so only the two exchanges (and the end of a group) need a __syncwarp.
-// compile-time overrides of the even/odd choices below (-1: the tuned default, 0: off, 1: on)
+// compile-time overrides of the tuned choices in vmult_slab_kernel (-1: the tuned default,
+// 0: off, 1: on): even/odd phase-2 contractions (EO2), rolled deferred passes and phase 3
+// (TUNR), phase 2 without accumulators (DEFER), paired-point x contractions (EO1X)
 #ifndef PMG_VMULT_EO_PHASE2
 #define PMG_VMULT_EO_PHASE2 -1
 #endif
