@@ -48,9 +48,12 @@ def parse():
     ap.add_argument("--cells", type=int, default=128, help="cells per direction (power of 2)")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
-    ap.add_argument("--extra", action="store_true", help="also time the FP32 operator")
     ap.add_argument("--skip-solve", action="store_true",
                     help="omit the time-to-solution leg (Q6 variable-kappa ph-multigrid CG)")
+    ap.add_argument("--case", choices=sorted(PROFILE_CASES), default=None,
+                    help="profiling mode: run one representative launch set of a solver path "
+                         "inside the NVTX range 'prof' and exit (no bench line)")
+    ap.add_argument("--refine", type=int, default=None, help="refinements of the --case mesh")
     return ap.parse_args()
 
 
@@ -283,6 +286,65 @@ def e2e_vmults(op, src_host, steps, torch, dev, barrier):
     del srcs, dsts, src_pinned, dst_pinned
     torch.cuda.synchronize()
     return t_pipe, t_serial
+
+
+def vmult_sweep(torch, pmg, dev, peak, steps=100, warmup=10, sizes=(16, 32, 64)):
+    """The deformed-cube Q4 vmult at the smaller sizes of the refinement sweep, FP64 and FP32:
+    GDoF/s over `steps` event-timed vmults after `warmup`, and the cell kernel's algorithmic
+    bytes over its average event-timed duration as a fraction of the HBM peak.  At 16^3 and
+    32^3 the inputs fit in L2 (31 MB / 248 MB FP64), so those rates are L2-resident, not HBM
+    rates."""
+    out = {}
+    stream = torch.cuda.current_stream()
+    for cells in sizes:
+        mesh = pmg.Mesh(pmg.Box.make(refine=box_for(cells), deform=1, amp=0.1))
+        for name, dt, tdt in (("f64", pmg.F64, torch.float64), ("f32", pmg.F32, torch.float32)):
+            op = pmg.LaplaceOperator(mesh, 4, dt, pmg.GEOMETRY_FULL, device=dev)
+            n = op.m()
+            src = torch.from_numpy(np.random.default_rng(1234).uniform(-1.0, 1.0, n)).to(tdt).to(f"cuda:{dev}")
+            dst = torch.empty_like(src)
+            for _ in range(warmup):
+                op.vmult(dst, src)
+            torch.cuda.synchronize()
+            total_ms, cell_ms, cell_n, _ = time_vmults(op, dst, src, steps, torch, stream)
+            bw = op.bytes_per_vmult() / (cell_ms / max(cell_n, 1) * 1e-3) / 1e9
+            out[f"{cells}^3_{name}"] = {"n_dofs": n, "gdofs": n * steps / (total_ms * 1e-3) / 1e9,
+                                        "cell_kernel_gbs": bw, "frac_of_hbm": bw / peak}
+            del op, src, dst
+        del mesh
+    torch.cuda.empty_cache()
+    return out
+
+
+def plain_method(torch, pmg, dev, repeats=3):
+    """The plain method: -lap u = 3 pi^2 sin(pi x) sin(pi y) sin(pi z) on [0,1]^3, FE_Q(2) on 16^3
+    cells (35,937 DoFs), geometric multigrid at degree 2 on every level 16^3 .. 2^3,
+    Chebyshev(3), FP64 CG to a relative residual of 1e-10; FP64 and FP32 V-cycles, median of
+    `repeats` solves after one warm-up, with the L2 error against the exact solution."""
+    box = pmg.Box.make(coarse=(2, 2, 2), refine=3)
+    res = {}
+    for name, dt in (("fp64_mg", pmg.F64), ("fp32_mg", pmg.F32)):
+        h = pmg.Hierarchy(box, [2], mg_dtype=dt, cheb_degree=3, h_degree=2, device=dev)
+        b = h.fine64.assemble_rhs(1, 4)
+        h.estimate()
+        h.solve(b, reduce=1e-10)
+        times, info, x = [], None, None
+        for _ in range(repeats):
+            x = h.fine64.initialize_dof_vector()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            x, info = h.solve(b, x=x, reduce=1e-10)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) * 1e-3)
+        res[name] = {"seconds": float(np.median(times)), "iterations": info["iterations"],
+                     "reduction_per_step": info["reduction_per_step"], "l2_error": h.fine64.l2_error(x, 1)}
+        n = h.fine64.m()
+        del h, b, x
+    res["n_dofs"] = n
+    res["config"] = "Q2, 16^3 cells, h-multigrid at degree 2 to 2^3, Chebyshev(3), FP64 CG to 1e-10"
+    return res
 
 
 def time_to_solution(torch, pmg, dev, refine=4, repeats=3):
@@ -553,20 +615,27 @@ def gpu_arm(args):
     traffic = traffic_per_dof * N if traffic_per_dof else None
 
     extra = {}
-    if args.extra and rank == 0:
+    if rank == 0 and args.dtype == "f64":
+        # the FP32 variant of the same workload (not the headline value)
         op32 = pmg.LaplaceOperator(mesh, 4, pmg.F32, pmg.GEOMETRY_FULL, device=dev)
         s32, d32 = src.float(), torch.empty(N, dtype=torch.float32, device=f"cuda:{dev}")
-        for _ in range(3):
+        for _ in range(max(args.warmup, 3)):
             op32.vmult(d32, s32)
+        torch.cuda.synchronize()
         t32, c32, n32, _ = time_vmults(op32, d32, s32, args.steps, torch, stream)
-        extra["fp32_vmult_gdofs"] = N * args.steps / (t32 * 1e-3) / 1e9
-        extra["fp32_cell_kernel_frac_of_hbm"] = op32.bytes_per_vmult() / (c32 / n32 * 1e-3) / 1e9 / peak
-        del op32
+        bw32 = op32.bytes_per_vmult() / (c32 / max(n32, 1) * 1e-3) / 1e9
+        extra["fp32_vmult"] = {"value": N * args.steps / (t32 * 1e-3) / 1e9, "unit": "GDoF/s",
+                               "ms_per_step": t32 / args.steps, "cell_kernel_gbs": bw32,
+                               "frac_of_hbm": bw32 / peak,
+                               "algorithmic_bytes_per_launch": op32.bytes_per_vmult()}
+        del op32, s32, d32
 
     tts = None
     if not args.skip_solve and world == 1:  # the solver figures are single-GPU measurements
         del op, src, dst
         torch.cuda.empty_cache()
+        extra["vmult_sweep"] = vmult_sweep(torch, pmg, dev, peak)
+        extra["plain_method_q2_time_to_1e-10"] = plain_method(torch, pmg, dev)
         tts = time_to_solution(torch, pmg, dev)
         tts["q6_cell_kernels"] = q6_kernel_rates(torch, pmg, dev, peaks)
         extra["dg_time_to_1e-10"] = dg_time_to_solution(torch, pmg, dev)
@@ -620,9 +689,98 @@ def gpu_arm(args):
         torch.distributed.destroy_process_group()
 
 
+# ----------------------------------------------------------------------------------------
+# profiling cases (--case): operators are set up outside the NVTX range "prof", the launches
+# to profile run inside it (ncu --nvtx --nvtx-include prof/ ...); the V-cycle runs as plain
+# launches (PMG_MG_GRAPH=0), so every kernel is visible
+#   q6_kappa   one FP64 CG iteration of the Q6 variable-coefficient problem (3^3 coarse cells
+#              refined R times, default 4 = 48^3) preconditioned by one FP32 V-cycle
+#   dg_q3      one FP64 CG iteration of DG-SIPG Q3 on 2^R cells per axis (default 6) with the
+#              FP32 DG -> CG Q3 -> Q1 -> h multigrid
+#   adjoint_q4 the mass-matrix vmult and the per-point form of the adjoint gradient, Q4 FP64
+#              on 2^R cells per axis (default 6)
+#   vmult_q4   one Q4 FP64 vmult on the deformed cube with 2^R cells per axis (default 5)
+# ----------------------------------------------------------------------------------------
+def _prof_range(torch, fn):
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("prof")
+    fn()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+
+
+def _one_cg_iteration(pmg, h, b):
+    x = h.fine64.initialize_dof_vector()
+    pmg.solve_cg(h.fine64, x, b, h.mg, 1e-10, 1e-16, 1, raise_on_noconv=False)
+
+
+def _case_q6_kappa(torch, pmg, refine):
+    box = pmg.Box.make(coarse=(3, 3, 3), refine=refine)
+    h = pmg.Hierarchy(box, [6, 3, 2, 1], mg_dtype=pmg.F32, cheb_degree=4, geometry=pmg.GEOMETRY_AFFINE,
+                      coeff_kind=pmg.COEFF_KAPPA)
+    b = h.fine64.assemble_rhs(0)
+    h.estimate()
+    _one_cg_iteration(pmg, h, b)
+    _prof_range(torch, lambda: _one_cg_iteration(pmg, h, b))
+
+
+def _case_dg_q3(torch, pmg, refine):
+    p = 3
+    h = pmg.Hierarchy(pmg.Box.make(refine=refine), [3, 1], mg_dtype=pmg.F32, cheb_degree=5, dg=True,
+                      penalty=2.0 * (p + 1) ** 2)
+    b = h.fine64.assemble_rhs(2, p + 2)
+    h.estimate()
+    _one_cg_iteration(pmg, h, b)
+    _prof_range(torch, lambda: _one_cg_iteration(pmg, h, b))
+
+
+def _case_adjoint_q4(torch, pmg, refine):
+    mesh = pmg.Mesh(pmg.Box.make(refine=refine))
+    op = pmg.LaplaceOperator(mesh, 4, pmg.F64, pmg.GEOMETRY_AFFINE, pmg.COEFF_VALUES)
+    xq = op.quadrature_points()
+    op.set_coefficient(torch.exp(0.5 * torch.sin(3.0 * xq[..., 0]) * torch.cos(2.0 * xq[..., 1])))
+    M = pmg.MassOperator(mesh, 4, pmg.F64)
+    u = torch.rand(M.m(), dtype=torch.float64, device="cuda")
+    v = torch.rand_like(u)
+    out = torch.empty_like(u)
+    g = op.qp_form(u, v, -1.0)
+
+    def run():
+        M.vmult(out, u)
+        op.qp_form(u, v, -1.0, out=g)
+
+    run()
+    _prof_range(torch, run)
+
+
+def _case_vmult_q4(torch, pmg, refine):
+    op = pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(refine=refine, deform=1, amp=0.1)), 4, pmg.F64,
+                             pmg.GEOMETRY_FULL)
+    src = torch.from_numpy(np.random.default_rng(1234).uniform(-1.0, 1.0, op.m())).cuda()
+    dst = torch.empty_like(src)
+    for _ in range(3):
+        op.vmult(dst, src)
+    _prof_range(torch, lambda: op.vmult(dst, src))
+
+
+PROFILE_CASES = {"q6_kappa": (_case_q6_kappa, 4), "dg_q3": (_case_dg_q3, 6),
+                 "adjoint_q4": (_case_adjoint_q4, 6), "vmult_q4": (_case_vmult_q4, 5)}
+
+
+def profile_case(args):
+    os.environ.setdefault("PMG_MG_GRAPH", "0")
+    import torch
+    import pmg
+    fn, default_refine = PROFILE_CASES[args.case]
+    fn(torch, pmg, default_refine if args.refine is None else args.refine)
+    print(f"{args.case}: done", flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.case:
+        profile_case(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

@@ -165,6 +165,18 @@ pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host)
 pmg_status pmg_operator_copy_constrained(const pmg_operator *op, uint8_t *host);
 pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host);
 
+/* Shape of the last launch of one of the operator's grid-stride kernels (inspection; the
+ * reference launches one Kokkos team per cell batch and has no counterpart): *units = the
+ * work units (warp groups of cells; cell batches for the DG face kernel) and *parallel =
+ * the warps (blocks for the DG face kernel) of the grid that shared them, so a launch with
+ * units >= 2 * parallel gave every warp two or more units.  Zero before the first launch. */
+#define PMG_KERNEL_VMULT_CELL 0 /* the cell kernel of vmult                              */
+#define PMG_KERNEL_DG_FACES 1   /* the face kernel of a DG vmult                         */
+#define PMG_KERNEL_MASS 2       /* the cell kernel of a mass-matrix vmult                */
+#define PMG_KERNEL_QP_FORM 3    /* the kernel of pmg_operator_qp_form                    */
+pmg_status pmg_operator_last_launch(const pmg_operator *op, int32_t kernel, int64_t *units,
+                                    int64_t *parallel);
+
 /* Coefficient fields and per-point forms (the adjoint path; no counterpart in the reference).
  * set_coefficient: new PMG_COEFF_VALUES values [C][nq^3] (FP64; on_device selects a device
  * or a host pointer), rebuilding G / the per-point factors / the mass weights on the stream.
@@ -221,6 +233,10 @@ pmg_status pmg_transfer_prolongate_and_add(const pmg_transfer *transfer, void *d
 /* restrict_and_add(dst_coarse, src_fine) */
 pmg_status pmg_transfer_restrict_and_add(const pmg_transfer *transfer, void *dst_coarse,
                                          const void *src_fine, void *stream);
+/* Shape of the last launch (inspection, no reference counterpart): *units = patches (the
+ * DG <-> CG transfer: entries; the runtime-size kernel: patch batches) and *parallel = the
+ * warps (threads; blocks) of the grid that shared them.  Zero before the first launch. */
+pmg_status pmg_transfer_last_launch(const pmg_transfer *transfer, int64_t *units, int64_t *parallel);
 
 /* ---------------------------------------------------------------------------------- */
 /* Smoother: deal.II PreconditionChebyshev<LaplaceOperatorBase, Vector> as configured at */
@@ -316,7 +332,10 @@ pmg_status pmg_adjoint_gradient(pmg_operator *A, const pmg_operator *M, pmg_mg *
 /* ---------------------------------------------------------------------------------- */
 
 /* *result = sum_i a_i b_i over n entries of dtype, accumulated in FP64 with a fixed
- * reduction order (deterministic); synchronises the stream to return the value. */
+ * reduction order (deterministic); synchronises the stream to return the value.  The
+ * reductions of the library (this dot, the fused CG and Jacobi updates inside pmg_cg_solve,
+ * the Chebyshev estimate) share one partial-sum buffer per device: they must not run
+ * concurrently on one device from different host threads or unordered streams. */
 pmg_status pmg_vector_dot(const void *a, const void *b, int32_t dtype, int64_t n, double *result,
                           void *stream);
 /* The dot product of pmg_vector_dot for callers that cannot allocate device memory at the
@@ -325,9 +344,13 @@ pmg_status pmg_vector_dot(const void *a, const void *b, int32_t dtype, int64_t n
  * Allocates nothing: its scratch is a fixed 32 KB array in the library's device image,
  * held on every GPU that loads the library until exit.  *result_dev (a caller-owned device
  * double) receives the FP64-accumulated sum, ordered on stream, without a host
- * synchronisation.  n is limited to 268,435,456 entries (PMG_EINVAL beyond).  The first
- * call on a device looks up the scratch address and should come before any stream capture.
- * Calls that overlap on the GPU share the scratch and race. */
+ * synchronisation.  The reduction order is fixed for a given n and device (deterministic)
+ * but differs from pmg_vector_dot's, so the two may differ in the last bits.  n is limited
+ * to 268,435,456 entries (PMG_EINVAL beyond).  The first call on a device looks up the
+ * scratch address and should come before any stream capture; the address is kept for the
+ * life of the process, which assumes the device's primary context is never reset
+ * (cudaDeviceReset) and that calls run in it.  Calls that overlap on the GPU share the
+ * scratch and race. */
 pmg_status pmg_vector_dot_noalloc(const void *a, const void *b, int32_t dtype, int64_t n,
                                   double *result_dev, void *stream);
 /* dst (dt_dst) = src (dt_src), n entries, converting between FP64 and FP32. */

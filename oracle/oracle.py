@@ -123,6 +123,8 @@ def _declare(L):
     L.orc_box_l2_error_sine.restype = C.c_double
     L.orc_solve_box.argtypes = [BP, _p(i32), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                 C.c_double, C.c_double, C.c_int, C.POINTER(SolveInfo), C.c_void_p]
+    L.orc_solve_box_hdeg.argtypes = [BP, _p(i32), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_double, C.c_double, C.c_int, C.POINTER(SolveInfo), C.c_void_p]
     L.orc_transfer_sizes.argtypes = [BP, C.c_int, C.c_int, C.POINTER(C.c_int64),
                                      C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.orc_transfer_apply.argtypes = [BP, C.c_int, C.c_int, C.c_int, C.c_int, _p(d), _p(d)]
@@ -258,7 +260,9 @@ def l2_error_sine(box, p, nq, plain, u):
 
 
 def solve_box(box, pseq, cheb=5, h_times=1, rhs_kind=0, coeff_kind=0, reduce=1e-9, abs_tol=1e-16,
-              maxit=100, want_x=False):
+              maxit=100, want_x=False, h_degree=1):
+    """Multigrid-preconditioned CG on a box: FE_Q(h_degree) on every refinement (h-levels),
+    then the degrees of pseq (descending, ending in h_degree) on the finest mesh."""
     info = SolveInfo()
     pseq = np.ascontiguousarray(pseq, dtype=np.int32)
     x = None
@@ -268,8 +272,8 @@ def solve_box(box, pseq, cheb=5, h_times=1, rhs_kind=0, coeff_kind=0, reduce=1e-
         N = int(np.prod([nm * (c << box.refine) + 1 for c in box.coarse]))
         x = np.zeros(N)
         xp = x.ctypes.data_as(C.c_void_p)
-    rc = lib().orc_solve_box(C.byref(box), pseq, len(pseq), cheb, h_times, rhs_kind, coeff_kind,
-                             reduce, abs_tol, maxit, C.byref(info), xp)
+    rc = lib().orc_solve_box_hdeg(C.byref(box), pseq, len(pseq), h_degree, cheb, h_times, rhs_kind,
+                                  coeff_kind, reduce, abs_tol, maxit, C.byref(info), xp)
     if rc != 0:
         raise ValueError("orc_solve_box failed")
     return info, x

@@ -1239,27 +1239,30 @@ typedef struct {
 } orc_solve_info;
 
 /* The multigrid solver of tests/common/portable_multigrid_solver.h restated on the CPU:
- * h-levels 0..refine with FE_Q(1) on every refinement of the box, then p-levels on the
- * finest mesh for the degrees in pseq (descending, last = 1, as p_levels in
- * tests/poisson_cube_bk3/program.cc:289-292); Chebyshev degree `cheb` with range 15 and
- * 10 eigenvalue iterations on levels > 0, Chebyshev-to-1e-3 on level 0; PCG with
+ * h-levels 0..refine with FE_Q(h_degree) on every refinement of the box, then p-levels on
+ * the finest mesh for the degrees in pseq (descending, last = h_degree).  h_degree = 1 is the
+ * ph-multigrid of tests/poisson_cube_bk3/program.cc:263-292 (p_levels as at :289-292); pseq =
+ * {p} with h_degree = p is the plain geometric multigrid of
+ * source/geometric_multigrid/program.cc:245-249 (GeometricTransfer<dim, fe_degree> between
+ * consecutive refinements at one degree).  Chebyshev degree `cheb` with range 15 and 10
+ * eigenvalue iterations on levels > 0, Chebyshev-to-1e-3 on level 0; PCG with
  * ReductionControl(maxit, abs_tol, reduce) (portable_multigrid_solver.h:147-169).
  * x_out (nullable) receives the solution on the finest level. */
-int orc_solve_box(const orc_box *box, const int32_t *pseq, int n_pseq, int cheb, int h_times,
-                  int rhs_kind, int coeff_kind, double reduce, double abs_tol, int maxit,
-                  orc_solve_info *info, double *x_out)
+int orc_solve_box_hdeg(const orc_box *box, const int32_t *pseq, int n_pseq, int h_degree, int cheb,
+                       int h_times, int rhs_kind, int coeff_kind, double reduce, double abs_tol,
+                       int maxit, orc_solve_info *info, double *x_out)
 {
   memset(info, 0, sizeof(*info));
   const int n_h = box->refine + 1;
   const int n_levels = n_h + n_pseq - 1;
-  if (n_levels > 32 || pseq[n_pseq - 1] != 1) return -1;
+  if (n_levels > 32 || h_degree < 1 || pseq[n_pseq - 1] != h_degree) return -1;
   orc_mg mg;
   mg.n_levels = n_levels;
   mg.levels = (orc_level *)calloc(n_levels, sizeof(orc_level));
   mg.transfers = (orc_transfer *)calloc(n_levels, sizeof(orc_transfer));
   for (int l = 0; l < n_levels; ++l) {
     orc_box b = *box;
-    int p = 1;
+    int p = h_degree;
     if (l < n_h) b.refine = l;
     else p = pseq[n_pseq - 1 - (l - n_h + 1)];
     level_init(&mg.levels[l], &b, p, coeff_kind);
@@ -1336,6 +1339,15 @@ int orc_solve_box(const orc_box *box, const int32_t *pseq, int n_pseq, int cheb,
   free(mg.levels);
   free(mg.transfers);
   return 0;
+}
+
+/* ph-multigrid with FE_Q(1) h-levels (pseq ends in 1). */
+int orc_solve_box(const orc_box *box, const int32_t *pseq, int n_pseq, int cheb, int h_times,
+                  int rhs_kind, int coeff_kind, double reduce, double abs_tol, int maxit,
+                  orc_solve_info *info, double *x_out)
+{
+  return orc_solve_box_hdeg(box, pseq, n_pseq, 1, cheb, h_times, rhs_kind, coeff_kind, reduce, abs_tol,
+                            maxit, info, x_out);
 }
 
 /* Single-level transfer construction for tests: p-transfer between degrees pc < pf on the

@@ -267,6 +267,18 @@ pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host) {
   });
 }
 
+pmg_status pmg_operator_last_launch(const pmg_operator *op, int32_t kernel, int64_t *units,
+                                   int64_t *parallel) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(units);
+    NEED(parallel);
+    PMG_REQUIRE(kernel >= PMG_KERNEL_VMULT_CELL && kernel <= PMG_KERNEL_QP_FORM, "bad kernel id");
+    *units = op->launch_units[kernel];
+    *parallel = op->launch_par[kernel];
+  });
+}
+
 pmg_status pmg_operator_set_coefficient(pmg_operator *op, const double *coeff_qp, int32_t on_device,
                                         void *stream) {
   return guarded(__func__, [&] {
@@ -358,6 +370,16 @@ pmg_status pmg_transfer_restrict_and_add(const pmg_transfer *t, void *dst_coarse
     NEED(t);
     PMG_CUDA(cudaSetDevice(t->device));
     pmg::transfer_apply(*t, 1, dst_coarse, src_fine, as_stream(stream));
+  });
+}
+
+pmg_status pmg_transfer_last_launch(const pmg_transfer *t, int64_t *units, int64_t *parallel) {
+  return guarded(__func__, [&] {
+    NEED(t);
+    NEED(units);
+    NEED(parallel);
+    *units = t->launch_units;
+    *parallel = t->launch_par;
   });
 }
 

@@ -367,7 +367,7 @@ DGGeo make_geo(const DGHost &h) {
 
 template <int N, typename T>
 void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms, cudaStream_t s,
-                 bool diag) {
+                 bool diag, int64_t *units, int64_t *blocks) {
   if (diag) {
     const int grid = (int)std::min<int64_t>((n_cells * N * N * N + 255) / 256, (int64_t)sms * 16);
     dg_face_diag_kernel<N, T><<<std::max(grid, 1), 256, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
@@ -376,12 +376,16 @@ void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, i
     if (face_form() == 0) {
       constexpr int B = dg_batch_seq<N>();
       const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 16);
+      if (units) *units = (n_cells + B - 1) / B;
+      if (blocks) *blocks = std::max(grid, 1);
       dg_face_seq_kernel<N, T><<<std::max(grid, 1), 128, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
                                                                   static_cast<const T *>(src), static_cast<T *>(dst),
                                                                   h.nbr.as<int32_t>(), n_cells);
     } else {
       constexpr int B = dg_batch<N>();
       const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 8);
+      if (units) *units = (n_cells + B - 1) / B;
+      if (blocks) *blocks = std::max(grid, 1);
       // 16-byte loads of the x-normal lines where the rows allow them and src is aligned
       constexpr bool rows16 = (N * sizeof(T)) % 16 == 0;
       if (rows16 && reinterpret_cast<uintptr_t>(src) % 16 == 0)
@@ -399,14 +403,14 @@ void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, i
 
 template <typename T>
 void face_dispatch(int degree, const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms,
-                   cudaStream_t s, bool diag) {
+                   cudaStream_t s, bool diag, int64_t *units = nullptr, int64_t *blocks = nullptr) {
   switch (degree) {
-  case 1: face_launch<2, T>(h, src, dst, n_cells, sms, s, diag); break;
-  case 2: face_launch<3, T>(h, src, dst, n_cells, sms, s, diag); break;
-  case 3: face_launch<4, T>(h, src, dst, n_cells, sms, s, diag); break;
-  case 4: face_launch<5, T>(h, src, dst, n_cells, sms, s, diag); break;
-  case 5: face_launch<6, T>(h, src, dst, n_cells, sms, s, diag); break;
-  case 6: face_launch<7, T>(h, src, dst, n_cells, sms, s, diag); break;
+  case 1: face_launch<2, T>(h, src, dst, n_cells, sms, s, diag, units, blocks); break;
+  case 2: face_launch<3, T>(h, src, dst, n_cells, sms, s, diag, units, blocks); break;
+  case 3: face_launch<4, T>(h, src, dst, n_cells, sms, s, diag, units, blocks); break;
+  case 4: face_launch<5, T>(h, src, dst, n_cells, sms, s, diag, units, blocks); break;
+  case 5: face_launch<6, T>(h, src, dst, n_cells, sms, s, diag, units, blocks); break;
+  case 6: face_launch<7, T>(h, src, dst, n_cells, sms, s, diag, units, blocks); break;
   default: fail(PMG_EINVAL, "DG degree must be in [1,6]");
   }
 }
@@ -449,9 +453,9 @@ void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen) {
 }
 
 void dg_apply_faces(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells,
-                    int sms, cudaStream_t s) {
-  if (dtype == PMG_F64) face_dispatch<double>(degree, h, src, dst, n_cells, sms, s, false);
-  else face_dispatch<float>(degree, h, src, dst, n_cells, sms, s, false);
+                    int sms, cudaStream_t s, int64_t *units, int64_t *blocks) {
+  if (dtype == PMG_F64) face_dispatch<double>(degree, h, src, dst, n_cells, sms, s, false, units, blocks);
+  else face_dispatch<float>(degree, h, src, dst, n_cells, sms, s, false, units, blocks);
 }
 
 void dg_add_face_diagonal(const DGHost &h, int degree, int dtype, void *diag, int64_t n_cells, int sms,

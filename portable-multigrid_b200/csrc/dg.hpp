@@ -16,8 +16,9 @@ struct DGHost {
 };
 
 void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen);
+// units / blocks (if set) receive the cell batches and the blocks of the face-kernel launch
 void dg_apply_faces(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells,
-                    int sms, cudaStream_t s);
+                    int sms, cudaStream_t s, int64_t *units = nullptr, int64_t *blocks = nullptr);
 void dg_add_face_diagonal(const DGHost &h, int degree, int dtype, void *diag, int64_t n_cells, int sms,
                           cudaStream_t s);
 void dg_add_boundary_rhs(const DGHost &h, const BoxMesh &mesh, int degree, int nq, int dtype, void *b,

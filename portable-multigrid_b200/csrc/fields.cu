@@ -74,12 +74,15 @@ template <int N, typename T> void mass_launch(const pmg_operator &op, const void
     const int grid = resident_grid(k, 32 * kWarps, smem, blocks);
     k<<<grid, 32 * kWarps, smem, s>>>(tab, static_cast<const T *>(src), static_cast<T *>(dst),
                                       op.idx.as<uint32_t>(), op.geo.as<T>(), nullptr, op.n_groups);
+    op.launch_par[PMG_KERNEL_MASS] = (int64_t)grid * kWarps;
   } else {
     auto k = kern::mass_slab_kernel<N, T, 0>;
     const int grid = resident_grid(k, 32 * kWarps, smem, blocks);
     k<<<grid, 32 * kWarps, smem, s>>>(tab, static_cast<const T *>(src), static_cast<T *>(dst),
                                       op.idx.as<uint32_t>(), nullptr, op.coef.as<T>(), op.n_groups);
+    op.launch_par[PMG_KERNEL_MASS] = (int64_t)grid * kWarps;
   }
+  op.launch_units[PMG_KERNEL_MASS] = op.n_groups;
   PMG_LAUNCH_CHECK();
 }
 
@@ -114,6 +117,8 @@ void qp_form_geom(const pmg_operator &op, const void *u, const void *v, double a
                                static_cast<const T *>(v), out, op.idx.as<uint32_t>(), op.geo.as<T>(),
                                op.coef.as<T>(), op.n_groups, op.n_cells, alpha);
   PMG_LAUNCH_CHECK();
+  op.launch_units[PMG_KERNEL_QP_FORM] = op.n_groups;
+  op.launch_par[PMG_KERNEL_QP_FORM] = (int64_t)grid * W;
 }
 
 template <int N, typename T>

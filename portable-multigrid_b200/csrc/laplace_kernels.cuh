@@ -1011,6 +1011,7 @@ struct SlabLaunch {
   unsigned int *err; // device flag set when a bounded wait gives up
   cudaStream_t stream;
   const double *S, *SD, *D, *W; // host tables (double), converted to the kernel type
+  int64_t *launched;            // if set: receives the number of warps the vmult launched
 };
 void launch_vmult_p1(const SlabLaunch &);
 void launch_vmult_p2(const SlabLaunch &);

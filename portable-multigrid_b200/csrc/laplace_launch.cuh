@@ -181,6 +181,7 @@ template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabL
       make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
       static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err);
   PMG_LAUNCH_CHECK();
+  if (L.launched) *L.launched = (int64_t)grid * sh.wpb;
 }
 
 // The src-staging pipeline (PIPE 2) is built for the direct-load variant only: together with

@@ -9,17 +9,24 @@
 // GPU loading the library holds until the process exits.
 //
 // Limits and rules:
-//  * each block reduces a fixed chunk of kChunk entries, so n may be at most
-//    kMaxBlocks * kChunk = 268,435,456; larger n is rejected with PMG_EINVAL;
+//  * each block reduces one chunk of consecutive entries, a multiple of the block size
+//    chosen from n so that about eight blocks per SM share the vector (at most kMaxBlocks
+//    partial sums); n may be at most kMaxN = 268,435,456 entries, larger n is rejected with
+//    PMG_EINVAL;
+//  * for a given n and device the reduction order is fixed (deterministic), but it is not
+//    pmg_vector_dot's order, so the two may differ in the last bits;
 //  * the result is written to a caller-owned device double, ordered on the stream; the
 //    host is not synchronised;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, that device current); make that first call
-//    before any stream capture;
+//    before any stream capture.  The address is kept per device ordinal for the life of the
+//    process: it assumes the device's primary context is not reset (cudaDeviceReset) and
+//    that the calls run in that primary context;
 //  * every call shares the one array: calls whose kernels overlap on the GPU (different
 //    streams without ordering) race and give wrong results;
 //  * every block writes its partial before the final kernel reads exactly those partials,
 //    so the array never needs clearing; it keeps the last call's partials.
+#include <algorithm>
 #include <mutex>
 
 #include "pmg_internal.hpp"
@@ -27,19 +34,19 @@
 namespace pmg {
 namespace {
 
-constexpr int kMaxBlocks = 4096;           // partial sums held by the scratch array
+constexpr int kMaxBlocks = 4096; // partial sums held by the scratch array
 constexpr int kThreads = 256;
-constexpr int64_t kChunk = 256 * kThreads; // entries reduced by one block
-constexpr int64_t kMaxN = int64_t(kMaxBlocks) * kChunk;
+constexpr int64_t kMaxN = int64_t(kMaxBlocks) * 256 * kThreads;
 
 static __device__ __align__(256) double g_dot_partials[kMaxBlocks];
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) dot_chunk_kernel(const T *__restrict__ a,
                                                              const T *__restrict__ b, int64_t n,
+                                                             int64_t chunk,
                                                              double *__restrict__ partials) {
-  const int64_t base = int64_t(blockIdx.x) * kChunk;
-  const int64_t end = min(base + kChunk, n);
+  const int64_t base = int64_t(blockIdx.x) * chunk;
+  const int64_t end = min(base + chunk, n);
   double v = 0.0;
   for (int64_t i = base + threadIdx.x; i < end; i += kThreads) v += (double)a[i] * (double)b[i];
   __shared__ double red[kThreads / 32];
@@ -96,19 +103,24 @@ void vector_dot_noalloc(const void *a, const void *b, int dtype, int64_t n, doub
   PMG_REQUIRE(n >= 0, "n must be >= 0");
   if (n > kMaxN)
     fail(PMG_EINVAL, "n = " + std::to_string(n) + " exceeds the no-allocation dot limit of " +
-                         std::to_string(kMaxN) + " entries (" + std::to_string(kMaxBlocks) +
-                         " partial sums of " + std::to_string(kChunk) + " entries)");
+                         std::to_string(kMaxN) + " entries");
   int device = 0;
   PMG_CUDA(cudaGetDevice(&device));
   double *partials = scratch_address(device);
-  const int n_blocks = (int)((n + kChunk - 1) / kChunk);
+  int sms = 0;
+  PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  // chunk: a multiple of the block size, about eight blocks per SM, at most kMaxBlocks blocks
+  const int64_t target = std::min<int64_t>(kMaxBlocks, 8 * (int64_t)std::max(sms, 1));
+  const int64_t per_block = (n + target - 1) / target;
+  const int64_t chunk = std::max<int64_t>(kThreads, (per_block + kThreads - 1) / kThreads * kThreads);
+  const int n_blocks = (int)((n + chunk - 1) / chunk);
   if (n_blocks > 0) {
     if (dtype == PMG_F64)
       dot_chunk_kernel<double><<<n_blocks, kThreads, 0, s>>>(static_cast<const double *>(a),
-                                                             static_cast<const double *>(b), n, partials);
+                                                             static_cast<const double *>(b), n, chunk, partials);
     else
       dot_chunk_kernel<float><<<n_blocks, kThreads, 0, s>>>(static_cast<const float *>(a),
-                                                            static_cast<const float *>(b), n, partials);
+                                                            static_cast<const float *>(b), n, chunk, partials);
     PMG_LAUNCH_CHECK();
   }
   dot_finish_kernel<<<1, 1024, 0, s>>>(partials, n_blocks, result);

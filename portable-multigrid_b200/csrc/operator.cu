@@ -509,13 +509,16 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
     L.resident_warps = op.warps_vmult;
     L.resident_warps_ring = op.warps_vmult_ring;
     L.err = op.err_flag.as<unsigned int>();
+    L.launched = &op.launch_par[PMG_KERNEL_VMULT_CELL];
+    op.launch_units[PMG_KERNEL_VMULT_CELL] = op.n_groups;
     {
       prof::Scope scope("vmult_cell", s);
       vmult_fn(op.degree)(L);
     }
     if (op.dg) {
       prof::Scope scope("vmult_dg_faces", s);
-      dg_apply_faces(*op.dg, op.degree, op.dtype, src, dst, op.n_cells, op.sms, s);
+      dg_apply_faces(*op.dg, op.degree, op.dtype, src, dst, op.n_cells, op.sms, s,
+                     &op.launch_units[PMG_KERNEL_DG_FACES], &op.launch_par[PMG_KERNEL_DG_FACES]);
     }
   }
 }

@@ -207,6 +207,11 @@ struct pmg_operator {
   std::vector<pmg::DeviceBuffer> cg_work;   // CG work vectors kept between solves
   std::vector<pmg::DeviceBuffer> adj_work;  // adjoint-gradient work vectors
   pmg::DeviceBuffer err_flag;               // set by bounded device waits that give up
+  // shape of the last launch of each grid-stride kernel (pmg_operator_last_launch): work
+  // units (warp groups or cell batches) and the warps (or blocks) that shared them;
+  // index PMG_KERNEL_VMULT_CELL .. PMG_KERNEL_QP_FORM
+  mutable int64_t launch_units[4] = {0, 0, 0, 0};
+  mutable int64_t launch_par[4] = {0, 0, 0, 0};
 };
 
 namespace pmg {

@@ -328,12 +328,9 @@ void cg_solve(pmg_operator &A, pmg_mg *mg, void *x, const void *b, double reduce
     for (int i = 0; i < 4; ++i) A.cg_work.emplace_back(bytes);
   }
   DeviceBuffer &r = A.cg_work[0], &z = A.cg_work[1], &p = A.cg_work[2], &v = A.cg_work[3];
-  // r = b - A x
+  // r = b - A x and ||r|| in one pass
   operator_vmult(A, v.get(), x, s);
-  PMG_CUDA(cudaMemcpyAsync(r.get(), b, bytes, cudaMemcpyDeviceToDevice, s));
-  vec::residual(v.get(), r.get(), dt, N, s);
-  PMG_CUDA(cudaMemcpyAsync(r.get(), v.get(), bytes, cudaMemcpyDeviceToDevice, s));
-  double res = std::sqrt(vec::dot(r.get(), r.get(), dt, N, s));
+  double res = std::sqrt(vec::residual_dot(r.get(), b, v.get(), dt, N, s));
   check_finite(res, "CG residual");
   info = pmg_cg_info{};
   info.initial_residual = res;

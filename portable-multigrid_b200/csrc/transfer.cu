@@ -205,6 +205,8 @@ void patch_launch(const pmg_transfer &t, void *dst, const void *src, cudaStream_
   }
   const int64_t want = (t.n_patches + kPatchWarps - 1) / kPatchWarps;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)blocks * t.sms));
+  t.launch_units = t.n_patches;
+  t.launch_par = (int64_t)grid * kPatchWarps;
   k<<<grid, 32 * kPatchWarps, smem, s>>>(P, static_cast<const T *>(src), static_cast<T *>(dst),
                                          t.coarse_idx.as<uint32_t>(), t.fine_idx.as<uint32_t>(),
                                          t.weights.as<T>(), t.n_patches);
@@ -360,6 +362,8 @@ void transfer_apply(const pmg_transfer &t, int dir, void *dst, const void *src, 
   if (t.kind == 2) {
     const int64_t n = t.n_patches * t.nf * t.nf * t.nf;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)t.sms * 16));
+    t.launch_units = n;
+    t.launch_par = (int64_t)grid * 256;
     if (t.dtype == PMG_F64) {
       if (dir == 0)
         transfer_identity_kernel<double, 0><<<grid, 256, 0, s>>>(static_cast<const double *>(src), static_cast<double *>(dst),
@@ -388,6 +392,8 @@ void transfer_apply(const pmg_transfer &t, int dir, void *dst, const void *src, 
     else done = dir == 0 ? patch_dispatch<float, 0>(t, dst, src, s) : patch_dispatch<float, 1>(t, dst, src, s);
     if (done) return;
   }
+  t.launch_units = (t.n_patches + t.ppb - 1) / t.ppb;
+  t.launch_par = t.grid;
   if (t.dtype == PMG_F64)
     transfer_kernel<double><<<t.grid, 128, t.smem, s>>>(dir, t.nc, t.nf, t.ppb, t.P1d.as<double>(),
                                                         static_cast<const double *>(src), static_cast<double *>(dst),

@@ -17,6 +17,9 @@ struct pmg_transfer {
   size_t smem = 0;
   int sms = 0;               // SM count of the device
   bool patch_kernels = true; // warp-per-patch kernels for the compiled (nc, nf) pairs
+  // last launch (pmg_transfer_last_launch): patches (or entries) and the warps (or threads)
+  // of the grid that shared them
+  mutable int64_t launch_units = 0, launch_par = 0;
 };
 
 namespace pmg {

@@ -13,8 +13,21 @@ namespace {
 constexpr int kBlock = 256;
 constexpr int kMaxPartials = 1024;
 
+// SM count of the current device (cached per device)
+int current_sms() {
+  static std::mutex mu;
+  static int sms[64] = {0};
+  int dev = 0;
+  PMG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  int &n = sms[dev & 63];
+  if (n == 0) PMG_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  return n;
+}
+
+// grid of an elementwise grid-stride kernel: eight 256-thread blocks per SM at most
 inline int grid_for(int64_t n) {
-  return (int)std::max<int64_t>(1, std::min<int64_t>((n + kBlock - 1) / kBlock, 8 * 148));
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + kBlock - 1) / kBlock, 8 * (int64_t)current_sms()));
 }
 
 #define GRID_STRIDE(i, n)                                                                     \
@@ -107,6 +120,18 @@ __global__ void cg_update_k(T *x, T *r, const T *p, const T *v, T alpha, int64_t
   GRID_STRIDE(i, n) {
     x[i] += alpha * p[i];
     const T ri = r[i] - alpha * v[i];
+    r[i] = ri;
+    acc += (double)ri * (double)ri;
+  }
+  block_reduce_store<T>(acc, partials);
+}
+
+// r = b - Ax and partial sums of r*r
+template <typename T>
+__global__ void residual_dot_k(T *r, const T *b, const T *Ax, int64_t n, double *partials) {
+  double acc = 0.0;
+  GRID_STRIDE(i, n) {
+    const T ri = b[i] - Ax[i];
     r[i] = ri;
     acc += (double)ri * (double)ri;
   }
@@ -280,6 +305,16 @@ double cg_update(void *x, void *r, const void *p, const void *v, double alpha, i
                                                           (T)alpha, n, w.partials.as<double>()));
   PMG_LAUNCH_CHECK();
   return finish(w, grid, 1, s);
+}
+
+double residual_dot(void *r, const void *b, const void *Ax, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_reduce", s);
+  Workspace &w = workspace();
+  const int grid = reduce_grid(n);
+  DISPATCH(dtype, residual_dot_k<T><<<grid, kBlock, 0, s>>>(static_cast<T *>(r), static_cast<const T *>(b),
+                                                             static_cast<const T *>(Ax), n, w.partials.as<double>()));
+  PMG_LAUNCH_CHECK();
+  return finish(w, grid, 3, s);
 }
 
 double jacobi_dot(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s) {

@@ -30,6 +30,8 @@ double dot(const void *a, const void *b, int dtype, int64_t n, cudaStream_t s);
 double cg_update(void *x, void *r, const void *p, const void *v, double alpha, int dtype, int64_t n,
                  cudaStream_t s);
 double jacobi_dot(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s);
+// r = b - Ax; returns r.r
+double residual_dot(void *r, const void *b, const void *Ax, int dtype, int64_t n, cudaStream_t s);
 
 } // namespace vec
 } // namespace pmg

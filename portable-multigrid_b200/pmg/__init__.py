@@ -34,6 +34,7 @@ F64, F32 = 0, 1
 GEOMETRY_AUTO, GEOMETRY_FULL, GEOMETRY_AFFINE, GEOMETRY_INVJAC = 0, 1, 2, 3
 COEFF_NONE, COEFF_KAPPA, COEFF_VALUES = 0, 1, 2
 OP_LAPLACE, OP_DG_SIPG, OP_MASS = 0, 1, 2
+KERNEL_VMULT_CELL, KERNEL_DG_FACES, KERNEL_MASS, KERNEL_QP_FORM = 0, 1, 2, 3
 INVALID = 0xFFFFFFFF
 STATUS = {0: "PMG_OK", -1: "PMG_EINVAL", -2: "PMG_ENOMEM", -3: "PMG_ECUDA",
           -4: "PMG_ENONFINITE", -5: "PMG_ENOCONV", -6: "PMG_EBOUNDS", -7: "PMG_ESTATE",
@@ -158,6 +159,8 @@ def _declare(L):
         "pmg_operator_copy_dof_indices": ([vp, vp], i32),
         "pmg_operator_copy_constrained": ([vp, vp], i32),
         "pmg_operator_copy_geometry": ([vp, vp], i32),
+        "pmg_operator_last_launch": ([vp, i32, P(i64), P(i64)], i32),
+        "pmg_transfer_last_launch": ([vp, P(i64), P(i64)], i32),
         "pmg_operator_set_coefficient": ([vp, vp, i32, vp], i32),
         "pmg_operator_interpolate_coefficient": ([vp, vp, vp], i32),
         "pmg_operator_quadrature_points": ([vp, vp, vp], i32),
@@ -367,6 +370,12 @@ class LaplaceOperator:
         check(lib().pmg_operator_copy_geometry(self.h, out.ctypes.data_as(C.c_void_p)))
         return out.reshape(-1, 6, nq3)
 
+    def last_launch(self, kernel=KERNEL_VMULT_CELL):
+        """(work units, warps or blocks) of the last launch of one of the operator's kernels."""
+        u, p = C.c_int64(), C.c_int64()
+        check(lib().pmg_operator_last_launch(self.h, kernel, C.byref(u), C.byref(p)))
+        return u.value, p.value
+
     # -- coefficient fields and per-point forms (adjoint path) --------------------------
     def set_coefficient(self, values):
         """New PMG_COEFF_VALUES values [C, nq^3]: a float64 CUDA tensor or a host array."""
@@ -430,6 +439,12 @@ class Transfer:
 
     def restrict_and_add(self, dst_coarse, src_fine):
         check(lib().pmg_transfer_restrict_and_add(self.h, _ptr(dst_coarse), _ptr(src_fine), _stream()))
+
+    def last_launch(self):
+        """(patches, warps) of the last launch."""
+        u, p = C.c_int64(), C.c_int64()
+        check(lib().pmg_transfer_last_launch(self.h, C.byref(u), C.byref(p)))
+        return u.value, p.value
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
@@ -516,24 +531,27 @@ def solve_cg(A: LaplaceOperator, x, b, precond: VCycleMultigrid | None = None, r
 
 
 class Hierarchy:
-    """The ph-multigrid hierarchy of the reference's LaplaceProblem
-    (tests/poisson_cube_bk3/program.cc:263-515): FE_Q(1) on every refinement of the box
-    (h-levels), then the degrees of `pseq` (descending, ending in 1) on the finest mesh;
-    Chebyshev(cheb_degree, range 15, 10 eigenvalue iterations) on levels > 0 and
-    Chebyshev-to-1e-3 on level 0.  With dg=True an FE_DGQ(pseq[0]) SIPG level sits on top,
-    connected by the DG <-> CG transfer.  The finest-level FP64 operator `fine64` is the CG
-    matrix."""
+    """The multigrid hierarchies of the reference's drivers: FE_Q(h_degree) on every
+    refinement of the box (h-levels), then the degrees of `pseq` (descending, ending in
+    h_degree) on the finest mesh.  h_degree = 1 is the ph-multigrid of LaplaceProblem
+    (tests/poisson_cube_bk3/program.cc:263-515); pseq = [p] with h_degree = p is the plain
+    geometric multigrid of source/geometric_multigrid/program.cc:245-249
+    (GeometricTransfer<dim, fe_degree> at one degree on every level).  Chebyshev(cheb_degree,
+    range 15, 10 eigenvalue iterations) on levels > 0 and Chebyshev-to-1e-3 on level 0.  With
+    dg=True an FE_DGQ(pseq[0]) SIPG level sits on top, connected by the DG <-> CG transfer.
+    The finest-level FP64 operator `fine64` is the CG matrix."""
 
     def __init__(self, box: Box, pseq, mg_dtype=F32, cheb_degree=5, geometry=GEOMETRY_AUTO,
                  coeff_kind=COEFF_NONE, coeff_qp=None, device=0, smoothing_range=15.0,
-                 eig_iterations=10, coarse_dtype=None, dg=False, penalty=0.0):
-        assert pseq[-1] == 1 and list(pseq) == sorted(pseq, reverse=True)
+                 eig_iterations=10, coarse_dtype=None, dg=False, penalty=0.0, h_degree=1):
+        if pseq[-1] != h_degree or list(pseq) != sorted(pseq, reverse=True):
+            raise ValueError("pseq must be descending and end in h_degree")
         self.box = box
         coarse_dtype = mg_dtype if coarse_dtype is None else coarse_dtype
         self.meshes = [Mesh(box.with_refine(r)) for r in range(box.refine + 1)]
         self.levels, self.transfers, self.smoothers = [], [None], []
         n_h = box.refine + 1
-        degrees = [1] * n_h + list(reversed(pseq))[1:]
+        degrees = [h_degree] * n_h + list(reversed(pseq))[1:]
         for l, p in enumerate(degrees):
             mesh = self.meshes[min(l, n_h - 1)]
             dt = coarse_dtype if l == 0 else mg_dtype

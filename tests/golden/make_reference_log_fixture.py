@@ -1,15 +1,21 @@
 """Extract the reference's logged solver/vmult results into tests/golden/reference_logs.json.
 
-Run once in a container that has the reference checkout (REFERENCE_ROOT, default
-/root/reference); the JSON it writes is committed and is what the tests read.  Each row
-keeps the file and line of the log it came from.
+Run once where the reference checkout is available, naming its root:
+
+    REFERENCE_ROOT=<path to the reference checkout> python tests/golden/make_reference_log_fixture.py
+    python tests/golden/make_reference_log_fixture.py <path to the reference checkout>
+
+The JSON it writes is committed and is what the tests read.  Each row keeps the file and
+line of the log it came from.
 """
 import json
 import os
 import re
 import sys
 
-ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT")
+if __name__ == "__main__" and not ROOT:
+    sys.exit("name the reference checkout: REFERENCE_ROOT=<path> or the first argument")
 LOGS = {
     "fp64": "tests/poisson_cube_bk3_fp64/results/single-gpu-batched.out",
     "mixed": "tests/poisson_cube_bk3/results/signle-gpu-batched-mixed-precision.out",

@@ -169,3 +169,43 @@ def test_variable_kappa_q6_phmg_matches_oracle(oracle, mg_dtype):
     assert info["converged"]
     assert abs(info["iterations"] - info_o.iterations) <= (0 if mg_dtype == pmg.F64 else 1)
     assert rel_err(x.cpu().numpy(), x_o) < 1e-8
+
+
+@pytest.mark.parametrize("mg_dtype", [pmg.F64, pmg.F32])
+def test_plain_q2_h_multigrid_matches_oracle(oracle, mg_dtype):
+    """The plain method: -lap u = 3 pi^2 sin(pi x) sin(pi y) sin(pi z) on [0,1]^3 with FE_Q(2) on
+    16^3 cells, geometric multigrid at degree 2 on every level (16^3 -> 8^3 -> 4^3 -> 2^3,
+    GeometricTransfer<dim, fe_degree> as in source/geometric_multigrid/program.cc:245-249),
+    Chebyshev(3), FP64 CG to 1e-10.  The FP64 V-cycle takes the oracle's iterations and
+    solution; the FP32 V-cycle converges within one iteration of it."""
+    box = pmg.Box.make(coarse=(2, 2, 2), refine=3)
+    ob = oracle.Box.make(coarse=(2, 2, 2), refine=3)
+    info_o, x_o = oracle.solve_box(ob, [2], cheb=3, rhs_kind=1, reduce=1e-10, want_x=True, h_degree=2)
+    h = pmg.Hierarchy(box, [2], mg_dtype=mg_dtype, cheb_degree=3, h_degree=2)
+    assert [lv.degree for lv in h.levels] == [2, 2, 2, 2]
+    assert [lv.n_cells() for lv in h.levels] == [8, 64, 512, 4096]
+    b = h.fine64.assemble_rhs(1, 4)
+    x, info = h.solve(b, reduce=1e-10)
+    torch.cuda.synchronize()
+    assert h.fine64.m() == info_o.n_dofs == 35937
+    assert info["converged"]
+    if mg_dtype == pmg.F64:
+        assert info["iterations"] == info_o.iterations
+        assert abs(info["reduction_per_step"] / info_o.reduction_per_step - 1) < 1e-6
+    else:
+        assert abs(info["iterations"] - info_o.iterations) <= 1
+    assert rel_err(x.cpu().numpy(), x_o) < 1e-8
+    assert abs(h.fine64.l2_error(x, 1) / info_o.l2_error - 1) < 1e-6
+
+
+def test_plain_q2_h_multigrid_converges_at_rate_three():
+    """L2 error of the config-1 solve on 8^3, 16^3, 32^3 cells falls like h^3 (FE_Q(2))."""
+    errs = []
+    for refine in (2, 3, 4):
+        h = pmg.Hierarchy(pmg.Box.make(coarse=(2, 2, 2), refine=refine), [2], mg_dtype=pmg.F32,
+                          cheb_degree=3, h_degree=2)
+        x, info = h.solve(h.fine64.assemble_rhs(1, 4), reduce=1e-10)
+        assert info["converged"] and info["iterations"] <= 8
+        errs.append(h.fine64.l2_error(x, 1))
+    rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert all(2.85 < r < 3.15 for r in rates), rates

@@ -62,3 +62,21 @@ def test_manufactured_solution_convergence(oracle, p):
         errs.append(info.l2_error)
     rates = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
     assert rates[-1] > p + 1 - 0.35, (errs, rates)
+
+
+def test_plain_q2_h_multigrid_oracle(oracle):
+    """The plain method (FE_Q(2), geometric multigrid at degree 2 on every level down to 2^3
+    cells, Chebyshev(3), CG to 1e-10): a few iterations independent of the mesh size, and the
+    L2 error falling like h^3 between 8^3 and 16^3 cells."""
+    infos = []
+    for refine in (2, 3):
+        info, _ = oracle.solve_box(oracle.Box.make(coarse=(2, 2, 2), refine=refine), [2], cheb=3,
+                                   rhs_kind=1, reduce=1e-10, h_degree=2)
+        assert info.n_levels == refine + 1
+        assert all(info.level_degree[l] == 2 for l in range(info.n_levels))
+        infos.append(info)
+    assert infos[1].n_dofs == 35937
+    assert [i.iterations for i in infos] == [7, 7]
+    assert 2.9 < np.log2(infos[0].l2_error / infos[1].l2_error) < 3.1
+    with pytest.raises(ValueError):
+        oracle.solve_box(oracle.Box.make(refine=1), [2, 1], h_degree=2)

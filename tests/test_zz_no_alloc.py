@@ -51,6 +51,20 @@ def test_noalloc_dot_matches_allocating_dot_twice(dtype, n):
     assert results[0] != results[1]
 
 
+def test_noalloc_dot_accepts_the_maximum_size():
+    """n = 268,435,456 FP32 entries (two 1 GiB vectors): the largest accepted input, spread
+    over more partial sums than the finishing block has threads."""
+    g = torch.Generator(device="cuda").manual_seed(11)
+    a = torch.rand(MAX_N, generator=g, device="cuda", dtype=torch.float32) - 0.5
+    b = torch.rand(MAX_N, generator=g, device="cuda", dtype=torch.float32)
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ref = pmg.vector_dot(a, b)
+    got = dot_noalloc(a, b, out)
+    assert abs(got - ref) <= 1e-13 * np.log2(MAX_N) * float(torch.dot(a.double().abs(), b.double().abs()))
+    del a, b
+    torch.cuda.empty_cache()
+
+
 def test_noalloc_dot_rejects_oversized_input():
     a = torch.zeros(4, dtype=torch.float64, device="cuda")
     out = torch.zeros(1, dtype=torch.float64, device="cuda")
