@@ -122,6 +122,44 @@ typedef struct {
 pmg_status pmg_operator_create(const pmg_mesh *mesh, const pmg_operator_params *params,
                                pmg_operator **op);
 pmg_status pmg_operator_destroy(pmg_operator *op);
+
+/* An operator on the caller's own discretisation, as LaplaceOperatorBK3 takes it from
+ * deal.II's MatrixFree: setup_dof_indices_per_color (bk3.h:360-437) gives the cell -> DoF map
+ * in lexicographic cell-local order with the sentinel on constrained DoFs, and
+ * compute_G_tensors (bk3.h:456-515) forms G from MatrixFree's inv_jacobian and JxW.  All arrays
+ * are host arrays, read during the call; the library regroups the cells (consecutive caller
+ * cells share a warp, so a locality-preserving cell order reads HBM best) and permutes the
+ * maps and geometry into its device layouts.
+ *   dof_indices   [n_cells][(degree+1)^3] uint32, node (i,j,k) of a cell at (k*nm+j)*nm+i,
+ *                 entries < n_dofs or 0xFFFFFFFF (constrained: no contribution);
+ *   constrained   the DoFs whose rows are the identity (copy_constrained_values, bk3.h:230);
+ *                 map entries naming one of them are treated as the sentinel;
+ *   PMG_MAPS_G:   G [n_cells][6][(degree+1)^3] = JxW J^{-1} J^{-T} in the order rr, rs, rt, ss,
+ *                 st, tt at the (degree+1)-point Gauss points (x fastest), coefficient folded in;
+ *   PMG_MAPS_INVJAC: inv_jacobian [n_cells][(degree+1)^3][3][3] with [d][e] = d xi_d / d x_e
+ *                 (MatrixFree's inverse Jacobian, portable_local_laplace_operator.h:329-347) and
+ *                 JxW [n_cells][(degree+1)^3]: the deal.II-style formulation.
+ * params: degree, dtype and device are used; kind must be PMG_OP_LAPLACE and coeff_kind
+ * PMG_COEFF_NONE.  An entry >= n_dofs fails with PMG_EBOUNDS.  Such an operator has no box
+ * mesh: the calls that evaluate data on the mesh (right-hand side, error norm, coordinates,
+ * quadrature points, coefficients) and pmg_transfer_create fail with PMG_ESTATE; transfers
+ * to and from it come from pmg_transfer_create_from_maps. */
+#define PMG_INVALID_INDEX 0xFFFFFFFFu /* the constrained-DoF sentinel of an index map */
+#define PMG_MAPS_G 0
+#define PMG_MAPS_INVJAC 1
+typedef struct {
+  int64_t n_cells;
+  int64_t n_dofs;
+  const uint32_t *dof_indices;
+  const uint32_t *constrained;
+  int64_t n_constrained;
+  int32_t geometry; /* PMG_MAPS_G or PMG_MAPS_INVJAC */
+  const double *G;
+  const double *inv_jacobian;
+  const double *JxW;
+} pmg_operator_maps;
+pmg_status pmg_operator_create_from_maps(const pmg_operator_maps *maps, const pmg_operator_params *params,
+                                         pmg_operator **op);
 /* m() / n() (bk3.h:570-582). */
 pmg_status pmg_operator_m(const pmg_operator *op, int64_t *m);
 pmg_status pmg_operator_n(const pmg_operator *op, int64_t *n);
@@ -164,6 +202,12 @@ pmg_status pmg_operator_assemble_rhs(const pmg_operator *op, int32_t f_kind, int
 pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host);
 pmg_status pmg_operator_copy_constrained(const pmg_operator *op, uint8_t *host);
 pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host);
+
+/* Node-lattice coordinates (i, j, k) of every DoF of a continuous operator on a box mesh,
+ * host array ijk[N][3] (x fastest in the lattice of degree * cells + 1 points per direction):
+ * the support points a partitioned mesh matches across ranks (the ghost DoFs of
+ * portable_laplace_operator_bk3.h:187-227).  PMG_ESTATE for DG and caller-map operators. */
+pmg_status pmg_operator_dof_lattice(const pmg_operator *op, int32_t *ijk);
 
 /* Shape of the last launch of one of the operator's grid-stride kernels (inspection; the
  * reference launches one Kokkos team per cell batch and has no counterpart): *units = the
@@ -226,6 +270,35 @@ pmg_status pmg_operator_qp_form(const pmg_operator *op, const void *u, const voi
  * mesh.  Both operators must have the same dtype. */
 pmg_status pmg_transfer_create(const pmg_operator *coarse, const pmg_operator *fine,
                                pmg_transfer **transfer);
+/* reinit(mf_coarse, mf_fine, constraints_coarse, constraints_fine) from the caller's own maps
+ * (the index arrays PolynomialTransfer / GeometricTransfer / ContinuousTransfer build from
+ * MatrixFree and the constraints: portable_polynomial_transfer.h:1116-1245,
+ * portable_geometric_transfer.h:1294-1330, portable_continuous_transfer.h:339-485).  One
+ * patch is a cell of the fine mesh (polynomial, DG <-> CG) or of the coarse mesh (geometric):
+ *   kind            PMG_TRANSFER_POLYNOMIAL: nc = degree_c+1, nf = degree_f+1, degree_c < degree_f,
+ *                   the 1D matrix interpolates FE_Q(degree_c) at FE_Q(degree_f)'s nodes;
+ *                   PMG_TRANSFER_GEOMETRIC: equal degrees p, nc = p+1, nf = 2p+1 (the patch's
+ *                   two children per direction share their middle nodes), the 1D matrix
+ *                   interpolates at the children's nodes;
+ *                   PMG_TRANSFER_DG_CG: equal degrees, fine = FE_DGQ, identity per entry;
+ *   coarse_indices  [n_patches][nc^3] lexicographic, 0xFFFFFFFF for constrained coarse DoFs;
+ *   fine_indices    [n_patches][nf^3] lexicographic, every fine DoF of the patch;
+ *   weights         [n_patches][nf^3] or NULL: NULL gives the reference's 1 / (number of
+ *                   patches holding the fine DoF), 0 on the fine operator's constrained DoFs.
+ * Host arrays, read during the call; entries out of range fail with PMG_EBOUNDS.  The
+ * operators may come from a mesh or from caller maps; they fix n_dofs, dtype and device. */
+#define PMG_TRANSFER_POLYNOMIAL 0
+#define PMG_TRANSFER_GEOMETRIC 1
+#define PMG_TRANSFER_DG_CG 2
+typedef struct {
+  int32_t kind;
+  int64_t n_patches;
+  const uint32_t *coarse_indices;
+  const uint32_t *fine_indices;
+  const double *weights;
+} pmg_transfer_maps;
+pmg_status pmg_transfer_create_from_maps(const pmg_operator *coarse, const pmg_operator *fine,
+                                         const pmg_transfer_maps *maps, pmg_transfer **transfer);
 pmg_status pmg_transfer_destroy(pmg_transfer *transfer);
 /* prolongate_and_add(dst_fine, src_coarse) */
 pmg_status pmg_transfer_prolongate_and_add(const pmg_transfer *transfer, void *dst_fine,
@@ -353,6 +426,13 @@ pmg_status pmg_vector_dot(const void *a, const void *b, int32_t dtype, int64_t n
  * scratch and race. */
 pmg_status pmg_vector_dot_noalloc(const void *a, const void *b, int32_t dtype, int64_t n,
                                   double *result_dev, void *stream);
+/* Vector updates of the CG and Chebyshev iterations (LinearAlgebra::distributed::Vector add /
+ * sadd / scale, used by SolverCG), n entries of dtype, ordered on stream:
+ * axpy: y += alpha x;  xpay: y = x + alpha y;  pointwise_mult: z = d .* r. */
+pmg_status pmg_vector_axpy(void *y, const void *x, double alpha, int32_t dtype, int64_t n, void *stream);
+pmg_status pmg_vector_xpay(void *y, const void *x, double alpha, int32_t dtype, int64_t n, void *stream);
+pmg_status pmg_vector_pointwise_mult(void *z, const void *d, const void *r, int32_t dtype, int64_t n,
+                                     void *stream);
 /* dst (dt_dst) = src (dt_src), n entries, converting between FP64 and FP32. */
 pmg_status pmg_vector_copy(void *dst, int32_t dt_dst, const void *src, int32_t dt_src, int64_t n,
                            void *stream);

@@ -188,6 +188,25 @@ def dofs(box, p):
     return plain.reshape(C_, nm3), constrained, idx.reshape(C_, nm3)
 
 
+def dof_lattice(box, p):
+    """Node-lattice coordinates (i, j, k) of every DoF, int32 [N, 3], and the lattice itself
+    [L2, L1, L0] -> DoF (x fastest)."""
+    C_ = box.ncells()
+    nm3 = (p + 1) ** 3
+    L = [p * (c << box.refine) + 1 for c in box.coarse]
+    plain = np.zeros(C_ * nm3, np.uint32)
+    constrained = np.zeros(int(np.prod(L)), np.uint8)
+    lat = np.zeros(int(np.prod(L)), np.uint32)
+    N = lib().orc_box_dofs(C.byref(box), p, plain, constrained, lat.ctypes.data_as(C.c_void_p))
+    ijk = np.zeros((N, 3), np.int32)
+    t = np.arange(lat.size)
+    ok = lat != INVALID
+    ijk[lat[ok], 0] = t[ok] % L[0]
+    ijk[lat[ok], 1] = (t[ok] // L[0]) % L[1]
+    ijk[lat[ok], 2] = t[ok] // (L[0] * L[1])
+    return ijk, lat.reshape(L[2], L[1], L[0])
+
+
 def colors(box):
     cx, cy, cz = cell_coords(box)
     return ((cx & 1) | ((cy & 1) << 1) | ((cz & 1) << 2)).astype(np.uint8)

@@ -117,6 +117,18 @@ pmg_status pmg_operator_create(const pmg_mesh *mesh, const pmg_operator_params *
   });
 }
 
+pmg_status pmg_operator_create_from_maps(const pmg_operator_maps *maps, const pmg_operator_params *params,
+                                         pmg_operator **op) {
+  return guarded(__func__, [&] {
+    NEED(maps);
+    NEED(params);
+    NEED(op);
+    auto o = std::make_unique<pmg_operator>();
+    pmg::operator_setup_from_maps(*o, *maps, *params);
+    *op = o.release();
+  });
+}
+
 pmg_status pmg_operator_destroy(pmg_operator *op) {
   if (op) {
     cudaSetDevice(op->device);
@@ -245,7 +257,7 @@ pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host)
     NEED(host);
     for (size_t e = 0; e < op->num.plain.size(); ++e) {
       const uint32_t d = op->num.plain[e];
-      host[e] = op->num.constrained[d] ? pmg::kInvalid : d;
+      host[e] = (d == pmg::kInvalid || op->num.constrained[d]) ? pmg::kInvalid : d;
     }
   });
 }
@@ -264,6 +276,24 @@ pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host) {
     NEED(host);
     PMG_CUDA(cudaSetDevice(op->device));
     pmg::operator_copy_geometry(*op, host);
+  });
+}
+
+pmg_status pmg_operator_dof_lattice(const pmg_operator *op, int32_t *ijk) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(ijk);
+    if (op->from_maps || op->kind == PMG_OP_DG_SIPG || op->num.lattice.empty())
+      pmg::fail(PMG_ESTATE, "DoF lattice coordinates exist for continuous operators on box meshes only");
+    const int64_t L0 = op->num.L[0], L1 = op->num.L[1];
+    const int64_t n_lat = (int64_t)op->num.lattice.size();
+    for (int64_t t = 0; t < n_lat; ++t) {
+      const uint32_t d = op->num.lattice[t];
+      if (d == pmg::kInvalid) continue;
+      ijk[3 * (int64_t)d + 0] = (int32_t)(t % L0);
+      ijk[3 * (int64_t)d + 1] = (int32_t)((t / L0) % L1);
+      ijk[3 * (int64_t)d + 2] = (int32_t)(t / (L0 * L1));
+    }
   });
 }
 
@@ -343,6 +373,19 @@ pmg_status pmg_transfer_create(const pmg_operator *coarse, const pmg_operator *f
     NEED(transfer);
     auto t = std::make_unique<pmg_transfer>();
     pmg::transfer_setup(*t, *coarse, *fine);
+    *transfer = t.release();
+  });
+}
+
+pmg_status pmg_transfer_create_from_maps(const pmg_operator *coarse, const pmg_operator *fine,
+                                         const pmg_transfer_maps *maps, pmg_transfer **transfer) {
+  return guarded(__func__, [&] {
+    NEED(coarse);
+    NEED(fine);
+    NEED(maps);
+    NEED(transfer);
+    auto t = std::make_unique<pmg_transfer>();
+    pmg::transfer_setup_from_maps(*t, *coarse, *fine, *maps);
     *transfer = t.release();
   });
 }
@@ -546,6 +589,38 @@ pmg_status pmg_vector_dot_noalloc(const void *a, const void *b, int32_t dtype, i
                                   double *result_dev, void *stream) {
   return guarded(__func__, [&] {
     pmg::vector_dot_noalloc(a, b, dtype, n, result_dev, as_stream(stream));
+  });
+}
+
+pmg_status pmg_vector_axpy(void *y, const void *x, double alpha, int32_t dtype, int64_t n, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(y);
+    NEED(x);
+    PMG_REQUIRE(dtype == PMG_F64 || dtype == PMG_F32, "bad dtype");
+    PMG_REQUIRE(n >= 0, "n must be >= 0");
+    if (n > 0) pmg::vec::axpy(y, x, alpha, dtype, n, as_stream(stream));
+  });
+}
+
+pmg_status pmg_vector_xpay(void *y, const void *x, double alpha, int32_t dtype, int64_t n, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(y);
+    NEED(x);
+    PMG_REQUIRE(dtype == PMG_F64 || dtype == PMG_F32, "bad dtype");
+    PMG_REQUIRE(n >= 0, "n must be >= 0");
+    if (n > 0) pmg::vec::xpay(y, x, alpha, dtype, n, as_stream(stream));
+  });
+}
+
+pmg_status pmg_vector_pointwise_mult(void *z, const void *d, const void *r, int32_t dtype, int64_t n,
+                                     void *stream) {
+  return guarded(__func__, [&] {
+    NEED(z);
+    NEED(d);
+    NEED(r);
+    PMG_REQUIRE(dtype == PMG_F64 || dtype == PMG_F32, "bad dtype");
+    PMG_REQUIRE(n >= 0, "n must be >= 0");
+    if (n > 0) pmg::vec::jacobi(z, d, r, dtype, n, as_stream(stream));
   });
 }
 

@@ -160,6 +160,23 @@ __device__ __forceinline__ uint32_t ld_stream(const uint32_t *p, uint64_t pol) {
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
+// the same loads as volatile asm: issued where they stand in the program, not sunk towards
+// their first use (the register pipeline of vmult_slab_kernel issues them a phase early)
+__device__ __forceinline__ uint32_t ld_stream_early(const uint32_t *p, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_keep_early(const double *p, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_keep_early(const float *p, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
 // gathered loads that are reused by neighbouring cells
 __device__ __forceinline__ double ld_keep(const double *p, uint64_t pol) {
   double v;
@@ -349,14 +366,15 @@ template <int N, typename T, int GEOM = 1> struct Unroll {
 
 // Shared memory per warp of vmult_slab_kernel: 3 exchange buffers, plus (SMEM_G) the
 // geometry column ring and its two mbarriers, plus the gather pipeline (PIPE): 1 = one
-// group's index block, 2 = one group's gathered src values and two index blocks.
+// group's index block, 2 = one group's gathered src values and two index blocks, 3 (the
+// register pipeline) nothing.
 template <int N, typename T, bool SMEM_G, int PIPE = 0> struct SlabSmem {
   static constexpr size_t XCHG = size_t(3) * Layout<N>::CPW * Stride<N>::CELL * sizeof(T);
   static constexpr size_t CHUNK = size_t(N) * 6 * Layout<N>::LANES * sizeof(T); // one x column
   static constexpr size_t GEO = SMEM_G ? 2 * CHUNK : 0;                         // two-slot ring
   static constexpr size_t IDXB = size_t(Layout<N>::N2) * Layout<N>::LANES * 4;   // one index block
   static constexpr size_t SRC = PIPE == 2 ? size_t(Layout<N>::N2) * Layout<N>::LANES * sizeof(T) : 0;
-  static constexpr size_t IDX = PIPE == 0 ? 0 : (PIPE == 1 ? 1 : 2) * IDXB;
+  static constexpr size_t IDX = (PIPE == 0 || PIPE == 3) ? 0 : (PIPE == 1 ? 1 : 2) * IDXB;
   static constexpr size_t OFF_SRC = ((GEO + XCHG + 15) / 16) * 16;
   static constexpr size_t OFF_IDX = OFF_SRC + ((SRC + 15) / 16) * 16;
   static constexpr size_t PER_WARP = OFF_IDX + ((IDX + 15) / 16) * 16 + (SMEM_G ? 16 : 0);
@@ -372,7 +390,12 @@ template <int N, typename T, bool SMEM_G, int PIPE = 0> struct SlabSmem {
 //   1: the next group's index block is copied once the current gather has read its own;
 //   2: the next group's src values are copied (zero-filled at Dirichlet entries) right after
 //      the current group's first phase, from an index block copied a group earlier still;
-//      the scatter reads its indices from shared memory as well.
+//      the scatter reads its indices from shared memory as well;
+//   3: a register pipeline without shared memory: the next group's index block is loaded
+//      into registers when phase 2 starts (it lands during phase 2) and its src values when
+//      phase 3 starts (they land during the scatter); phase 1 then starts with the gathered
+//      values in registers.  It costs N^2 index registers through phase 2 and N^2 values
+//      through phase 3, which the shared-memory-bound ring variant has to spare.
 template <int N, typename T, int GEOM, bool SMEM_G, int PIPE = 0>
 __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N, T, GEOM>::value))
     vmult_slab_kernel(const __grid_constant__ Tab<N, T> tab, const T *__restrict__ src, T *__restrict__ dst,
@@ -468,6 +491,32 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     cp_async_commit();
   };
   int it = 0; // groups done by this warp (PIPE 2: index slot of group g = it & 1)
+  // PIPE 3: the next group's index block and gathered src values, carried in registers
+  constexpr int RP = PIPE == 3 ? N : 1;
+  uint32_t nidx[RP][RP];
+  T nsrc[RP][RP];
+  auto load_next_idx = [&](int64_t gg) {
+    if (PIPE == 3 && gg < n_groups) {
+      const uint32_t *ip = idx + gg * (N2 * LANES) + lane;
+#pragma unroll
+      for (int k = 0; k < RP; ++k)
+#pragma unroll
+        for (int i = 0; i < RP; ++i) nidx[k][i] = ld_stream_early(ip + (k * N + i) * LANES, pol_first);
+    }
+  };
+  auto load_next_src = [&](int64_t gg) {
+    if (PIPE == 3 && gg < n_groups) {
+#pragma unroll
+      for (int k = 0; k < RP; ++k)
+#pragma unroll
+        for (int i = 0; i < RP; ++i)
+          nsrc[k][i] = nidx[k][i] != kInvalidIdx ? ld_keep_early(src + nidx[k][i], pol_last) : T(0);
+    }
+  };
+  if (PIPE == 3) {
+    load_next_idx(warp0);
+    load_next_src(warp0);
+  }
   if (PIPE == 1) issue_idx(warp0, 0);
   if (PIPE == 2) {
     issue_idx(warp0, 0);
@@ -485,7 +534,12 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     // ---- phase 1: gather the Y-slab y = s, u[k][i] = src at node (i, s, k) ----
     {
       T u[N][N];
-      if (PIPE == 2) {
+      if (PIPE == 3) {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+          for (int i = 0; i < N; ++i) u[k][i] = nsrc[k < RP ? k : 0][i < RP ? i : 0];
+      } else if (PIPE == 2) {
         cp_async_wait<1>(); // this group's src values (the next index block may be in flight)
 #pragma unroll
         for (int k = 0; k < N; ++k)
@@ -606,6 +660,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     }
     // the gather's shared-memory entries are consumed: refill them for the next group
     if (PIPE == 1) issue_idx(g + nwarps, 0);
+    if (PIPE == 3) load_next_idx(g + nwarps); // lands during phase 2
     if (PIPE == 2) {
       cp_async_wait<0>(); // the next group's index block
       issue_src(g + nwarps < n_groups, slot ^ 1);
@@ -642,7 +697,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
           }
           if (!mbar_wait_bounded(&bars[chunk & 1], (chunk >> 1) & 1, err, 1u << 24)) {
             if (lane == 0) mbar_wait_bounded(&bars[(chunk + 1) & 1], ((chunk + 1) >> 1) & 1, err, 1u << 24);
-            if (PIPE) cp_async_wait<0>();
+            if (PIPE == 1 || PIPE == 2) cp_async_wait<0>();
             return; // the error flag is set; let copies in flight land before leaving
           }
           gcol = ring + (chunk & 1) * CHUNK_ELEMS;
@@ -833,6 +888,8 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     }
     __syncwarp(MASK);
 
+    if (PIPE == 3) load_next_src(g + nwarps); // lands during the scatter
+
     // ---- phase 3: Y-slab y = s, out = Sz^T a + SDz^T c, scatter ----
 #pragma unroll TUNR
     for (int i = 0; i < N; ++i) {
@@ -868,7 +925,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     if (PIPE == 2) issue_idx(g + 2 * nwarps, slot); // this group's index slot is free
     __syncwarp(MASK); // buffers are rewritten by the next group
   }
-  if (PIPE) cp_async_wait<0>(); // no copy may land after the warp has left
+  if (PIPE == 1 || PIPE == 2) cp_async_wait<0>(); // no copy may land after the warp has left
 }
 
 // Diagonal of the cell operator summed into diag (atomic), same layout and slab scheme:

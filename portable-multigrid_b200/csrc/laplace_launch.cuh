@@ -91,7 +91,7 @@ template <typename T> bool use_ring() {
   if (o == 0 || o == 1) return o == 1;
   return sizeof(T) == 8 ? kN != 7 : (kN == 3 || kN == 4);
 }
-// gather pipeline depth (PIPE template parameter); PMG_VMULT_PIPE=0/1/2 overrides
+// gather pipeline (PIPE template parameter); PMG_VMULT_PIPE=0/1/2/3 overrides
 inline int pipe_override() {
   static const int v = [] {
     const char *e = std::getenv("PMG_VMULT_PIPE");
@@ -106,7 +106,7 @@ inline int pipe_override() {
 // and FP64 Q6 affine lose 15-35 %).
 template <typename T, int GEOM, bool SG> int use_pipe() {
   const int o = pipe_override();
-  if (o >= 0 && o <= 2) return o;
+  if (o >= 0 && o <= 3) return o;
   if (SG) return (sizeof(T) == 8 && kN >= 6) ? 1 : 0;
   if ((GEOM == 1 || GEOM == 2) && kN == 7 && sizeof(T) == 4) return 1;
   return 0;
@@ -195,7 +195,8 @@ template <typename T, int GEOM, bool SG> void vmult_pipe(const SlabLaunch &L) {
       return;
     }
   }
-  if (pp >= 1) vmult_launch<T, GEOM, SG, 1>(L);
+  if (pp == 3) vmult_launch<T, GEOM, SG, 3>(L);
+  else if (pp >= 1) vmult_launch<T, GEOM, SG, 1>(L);
   else vmult_launch<T, GEOM, SG, 0>(L);
 }
 

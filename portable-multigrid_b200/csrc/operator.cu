@@ -294,7 +294,185 @@ SlabLaunch slab_launch(const pmg_operator &op, const Tables1D &t, cudaStream_t s
   return L;
 }
 
+// The index map with the sentinel, permuted into the Y-slab layout [group][k*N+i][e*N+j]
+// (setup_dof_indices_per_color, bk3.h:360-437) from op.num: entries that are constrained
+// DoFs, or the sentinel already, become the sentinel.
+void build_slab_index(pmg_operator &op) {
+  const int N = op.nm, N2 = N * N, N3 = N2 * N;
+  std::vector<uint32_t> perm((size_t)op.n_groups * N2 * op.lanes, kInvalid);
+  const uint32_t *plain = op.num.plain.data();
+  const uint8_t *cons = op.num.constrained.data();
+  const int64_t C = op.n_cells, lanes = op.lanes, cpw = op.cpw;
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < C; ++c) {
+    const int64_t grp = c / cpw, e = c % cpw;
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          const uint32_t d = plain[c * N3 + (k * N + j) * N + i];
+          perm[(grp * N2 + k * N + i) * lanes + e * N + j] = (d == kInvalid || cons[d]) ? kInvalid : d;
+        }
+  }
+  op.idx = upload(perm);
+}
+
+// the constrained DoFs as a list and a bitmask (copy_constrained_values, bk3.h:230)
+void build_constrained(pmg_operator &op) {
+  std::vector<uint32_t> list;
+  for (int64_t i = 0; i < op.n_dofs; ++i)
+    if (op.num.constrained[i]) list.push_back((uint32_t)i);
+  op.n_constrained = (int64_t)list.size();
+  op.constrained_list = upload(list);
+  std::vector<uint32_t> bits((size_t)(op.n_dofs + 31) / 32, 0u);
+  for (uint32_t i : list) bits[i >> 5] |= 1u << (i & 31);
+  op.constrained_bits = upload(bits);
+}
+
+// persistent grids (as many warps as can be resident on this device) and the error flag
+void finish_setup(pmg_operator &op) {
+  PMG_CUDA(cudaDeviceSynchronize());
+  const int sms = num_sms(op.device);
+  const int gc = geom_code(op);
+  const int occ = occupancy(false, op.degree, op.dtype, gc);
+  op.warps_vmult = (int64_t)std::max(1, occ & 0xffff) * sms;
+  op.warps_vmult_ring = (int64_t)std::max(1, occ >> 16) * sms;
+  op.warps_diag = (int64_t)std::max(1, occupancy(true, op.degree, op.dtype, gc)) * sms;
+  op.err_flag.allocate(sizeof(unsigned int));
+  PMG_CUDA(cudaMemset(op.err_flag.get(), 0, sizeof(unsigned int)));
+}
+
+// Caller geometry (cell order of the caller, points lexicographic x fastest) into the slab
+// layout [group][x point p][y point q][ncomp][lane = e*N + z point r]:
+//   mode 0: in = G[C][6][nq^3] (rr, rs, rt, ss, st, tt);
+//   mode 1: in = inv_jacobian[C][nq^3][3][3] (components 0..8), in2 = JxW[C][nq^3] (component 9).
+// One thread per input value: reads are coalesced, writes land in lane-contiguous runs.
+template <typename T>
+__global__ void geometry_from_caller_kernel(const double *__restrict__ in, const double *__restrict__ in2,
+                                            int mode, int64_t n_cells, int N, int cpw, int lanes,
+                                            T *__restrict__ out) {
+  const int N2 = N * N, N3 = N2 * N, ncomp = mode == 0 ? 6 : 10, nin = mode == 0 ? 6 : 9;
+  const int64_t total = n_cells * N3 * (mode == 0 ? 6 : 10);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t c;
+    int comp, pt;
+    double v;
+    if (mode == 0) {
+      c = t / (6 * N3);
+      const int64_t r = t - c * 6 * N3;
+      comp = (int)(r / N3);
+      pt = (int)(r - (int64_t)comp * N3);
+      v = in[t];
+    } else if (t < n_cells * N3 * nin) {
+      c = t / (N3 * nin);
+      const int64_t r = t - c * N3 * nin;
+      pt = (int)(r / nin);
+      comp = (int)(r - (int64_t)pt * nin);
+      v = in[t];
+    } else {
+      const int64_t u = t - n_cells * N3 * nin;
+      c = u / N3;
+      pt = (int)(u - c * N3);
+      comp = 9;
+      v = in2[u];
+    }
+    const int p = pt % N, q = (pt / N) % N, r = pt / N2;
+    const int64_t grp = c / cpw;
+    const int e = (int)(c - grp * cpw);
+    out[((grp * N2 + p * N + q) * ncomp + comp) * lanes + e * N + r] = (T)v;
+  }
+}
+
 } // namespace
+
+void operator_setup_from_maps(pmg_operator &op, const pmg_operator_maps &m, const pmg_operator_params &prm) {
+  PMG_REQUIRE(prm.degree >= 1 && prm.degree <= kMaxDegree, "degree must be in [1,6]");
+  PMG_REQUIRE(prm.dtype == PMG_F64 || prm.dtype == PMG_F32, "dtype must be PMG_F64 or PMG_F32");
+  PMG_REQUIRE(prm.kind == PMG_OP_LAPLACE, "operators from caller maps are continuous Laplace operators");
+  PMG_REQUIRE(prm.coeff_kind == PMG_COEFF_NONE,
+              "a coefficient of a caller-described operator is folded into its G or JxW");
+  PMG_REQUIRE(m.n_cells >= 0 && m.n_dofs >= 0, "negative size");
+  PMG_REQUIRE(m.n_dofs < (int64_t(1) << 32) - 1, "too many DoFs for 32-bit indices");
+  PMG_REQUIRE(m.n_cells < (int64_t(1) << 31), "too many cells");
+  PMG_REQUIRE(m.n_cells == 0 || m.dof_indices, "dof_indices is NULL");
+  PMG_REQUIRE(m.n_constrained >= 0 && (m.n_constrained == 0 || m.constrained), "bad constrained list");
+  PMG_REQUIRE(m.geometry == PMG_MAPS_G || m.geometry == PMG_MAPS_INVJAC, "geometry must be PMG_MAPS_G or PMG_MAPS_INVJAC");
+  if (m.n_cells > 0) {
+    if (m.geometry == PMG_MAPS_G) PMG_REQUIRE(m.G, "G is NULL");
+    else PMG_REQUIRE(m.inv_jacobian && m.JxW, "inv_jacobian or JxW is NULL");
+  }
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
+    (void)cudaGetLastError();
+    fail(PMG_ENODEV, "no CUDA device available");
+  }
+  PMG_REQUIRE(prm.device >= 0 && prm.device < n_dev, "bad device ordinal");
+  PMG_CUDA(cudaSetDevice(prm.device));
+  op.device = prm.device;
+  op.from_maps = true;
+  op.kind = PMG_OP_LAPLACE;
+  op.degree = prm.degree;
+  op.nm = op.nq = prm.degree + 1;
+  op.dtype = prm.dtype;
+  op.coeff_kind = PMG_COEFF_NONE;
+  op.geometry = m.geometry == PMG_MAPS_G ? PMG_GEOMETRY_FULL : PMG_GEOMETRY_INVJAC;
+  op.has_coeff_values = false;
+  op.n_cells = m.n_cells;
+  op.n_dofs = m.n_dofs;
+  op.mesh = BoxMesh{};
+  op.mesh.n_cells = m.n_cells;
+  const int N = op.nm, N2 = N * N, N3 = N2 * N;
+  op.cpw = 32 / N;
+  op.lanes = op.cpw * N;
+  op.n_groups = (op.n_cells + op.cpw - 1) / op.cpw;
+  op.sms = num_sms(op.device);
+  // the caller's numbering: index map (sentinel = constrained) and identity rows
+  op.num = Numbering{};
+  op.num.p = op.degree;
+  op.num.n_dofs = m.n_dofs;
+  op.num.plain.assign(m.dof_indices, m.dof_indices + (size_t)m.n_cells * N3);
+  op.num.constrained.assign((size_t)m.n_dofs, 0);
+  for (int64_t i = 0; i < m.n_constrained; ++i) {
+    const uint32_t d = m.constrained[i];
+    if ((int64_t)d >= m.n_dofs)
+      fail(PMG_EBOUNDS, "constrained DoF " + std::to_string(d) + " >= n_dofs " + std::to_string(m.n_dofs));
+    op.num.constrained[d] = 1;
+  }
+  for (size_t e = 0; e < op.num.plain.size(); ++e) {
+    uint32_t &d = op.num.plain[e];
+    if (d == kInvalid) continue;
+    if ((int64_t)d >= m.n_dofs)
+      fail(PMG_EBOUNDS, "dof_indices[" + std::to_string(e) + "] = " + std::to_string(d) + " >= n_dofs " +
+                            std::to_string(m.n_dofs));
+    if (op.num.constrained[d]) d = kInvalid;
+  }
+  build_slab_index(op);
+  build_constrained(op);
+  // geometry: the caller's arrays, permuted into the slab layout on the device
+  const size_t s = dtype_size(op.dtype);
+  const bool ij = m.geometry == PMG_MAPS_INVJAC;
+  const int ncomp = ij ? 10 : 6;
+  op.geo.allocate(s * std::max<int64_t>(1, op.n_groups) * N2 * ncomp * op.lanes);
+  PMG_CUDA(cudaMemset(op.geo.get(), 0, op.geo.bytes()));
+  if (op.n_cells > 0) {
+    const int64_t n_in = op.n_cells * N3 * (ij ? 9 : 6);
+    DeviceBuffer in(sizeof(double) * n_in), in2;
+    PMG_CUDA(cudaMemcpy(in.get(), ij ? m.inv_jacobian : m.G, sizeof(double) * n_in, cudaMemcpyHostToDevice));
+    if (ij) {
+      in2.allocate(sizeof(double) * op.n_cells * N3);
+      PMG_CUDA(cudaMemcpy(in2.get(), m.JxW, sizeof(double) * op.n_cells * N3, cudaMemcpyHostToDevice));
+    }
+    const int grid = (int)std::min<int64_t>((op.n_cells * N3 * ncomp + 255) / 256, (int64_t)op.sms * 32);
+    if (op.dtype == PMG_F64)
+      geometry_from_caller_kernel<double><<<grid, 256>>>(in.as<double>(), in2.as<double>(), ij ? 1 : 0, op.n_cells,
+                                                         N, op.cpw, op.lanes, op.geo.as<double>());
+    else
+      geometry_from_caller_kernel<float><<<grid, 256>>>(in.as<double>(), in2.as<double>(), ij ? 1 : 0, op.n_cells,
+                                                        N, op.cpw, op.lanes, op.geo.as<float>());
+    PMG_LAUNCH_CHECK();
+    PMG_CUDA(cudaDeviceSynchronize()); // the input buffers are freed on return
+  }
+  finish_setup(op);
+}
 
 void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_params &prm) {
   PMG_REQUIRE(prm.degree >= 1 && prm.degree <= kMaxDegree, "degree must be in [1,6]");
@@ -345,35 +523,8 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
     dg_setup(*op.dg, mesh.m, op.degree, prm.penalty);
   }
 
-  // index map with the sentinel, permuted into the Y-slab layout [group][k*N+i][e*N+j]
-  {
-    std::vector<uint32_t> perm((size_t)op.n_groups * N2 * op.lanes, kInvalid);
-    const uint32_t *plain = op.num.plain.data();
-    const uint8_t *cons = op.num.constrained.data();
-    const int64_t C = op.n_cells, lanes = op.lanes, cpw = op.cpw;
-#pragma omp parallel for schedule(static)
-    for (int64_t c = 0; c < C; ++c) {
-      const int64_t grp = c / cpw, e = c % cpw;
-      for (int k = 0; k < N; ++k)
-        for (int j = 0; j < N; ++j)
-          for (int i = 0; i < N; ++i) {
-            const uint32_t d = plain[c * N3 + (k * N + j) * N + i];
-            perm[(grp * N2 + k * N + i) * lanes + e * N + j] = cons[d] ? kInvalid : d;
-          }
-    }
-    op.idx = upload(perm);
-  }
-  // constrained list (copy_constrained_values, bk3.h:230)
-  {
-    std::vector<uint32_t> list;
-    for (int64_t i = 0; i < op.n_dofs; ++i)
-      if (op.num.constrained[i]) list.push_back((uint32_t)i);
-    op.n_constrained = (int64_t)list.size();
-    op.constrained_list = upload(list);
-    std::vector<uint32_t> bits((size_t)(op.n_dofs + 31) / 32, 0u);
-    for (uint32_t i : list) bits[i >> 5] |= 1u << (i & 31);
-    op.constrained_bits = upload(bits);
-  }
+  build_slab_index(op);
+  build_constrained(op);
   // geometry (compute_G_tensors, bk3.h:456-515), computed on the device
   const size_t s = dtype_size(op.dtype);
   op.cell_xyz = upload(mesh.m.cell_xyz);
@@ -468,16 +619,8 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
       PMG_LAUNCH_CHECK();
     }
   }
-  PMG_CUDA(cudaDeviceSynchronize());
-  // persistent grids: as many warps as can be resident on this device
-  const int gc = geom_code(op);
-  const int occ = occupancy(false, op.degree, op.dtype, gc);
-  op.warps_vmult = (int64_t)std::max(1, occ & 0xffff) * sms;
-  op.warps_vmult_ring = (int64_t)std::max(1, occ >> 16) * sms;
-  op.warps_diag = (int64_t)std::max(1, occupancy(true, op.degree, op.dtype, gc)) * sms;
-  op.err_flag.allocate(sizeof(unsigned int));
-  PMG_CUDA(cudaMemset(op.err_flag.get(), 0, sizeof(unsigned int)));
   // the index lattice is only needed for building h-transfers: keep it
+  finish_setup(op);
 }
 
 void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s, bool compute) {
@@ -557,6 +700,7 @@ void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s) {
 }
 
 void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, cudaStream_t s) {
+  require_mesh(op, "the right-hand side");
   PMG_REQUIRE(f_kind >= 0 && f_kind <= 2, "f_kind must be 0, 1 or 2");
   if (nq <= 0) nq = op.nq;
   PMG_REQUIRE(nq >= 1 && nq <= kMaxNq, "nq must be in [1,8]");
@@ -613,6 +757,7 @@ int64_t operator_bytes(const pmg_operator &op) {
 // (full geometry), the per-point factors (affine), or the mass weights.  The inverse
 // diagonal is not recomputed here.
 void operator_set_coefficient(pmg_operator &op, const double *values, bool on_device, cudaStream_t s) {
+  require_mesh(op, "a coefficient update");
   PMG_REQUIRE(op.coeff_kind == PMG_COEFF_VALUES, "the operator was not created with PMG_COEFF_VALUES");
   PMG_REQUIRE(values, "null coefficient array");
   PMG_CUDA(cudaSetDevice(op.device));
@@ -646,6 +791,8 @@ void operator_set_coefficient(pmg_operator &op, const double *values, bool on_de
 
 // dst's coefficient := src's coefficient field at dst's quadrature points (nested boxes).
 void operator_interpolate_coefficient(pmg_operator &dst, pmg_operator &src, cudaStream_t s) {
+  require_mesh(dst, "coefficient interpolation");
+  require_mesh(src, "coefficient interpolation");
   PMG_REQUIRE(dst.coeff_kind == PMG_COEFF_VALUES && src.coeff_kind == PMG_COEFF_VALUES,
               "both operators need PMG_COEFF_VALUES");
   PMG_REQUIRE(dst.device == src.device, "operators on different devices");
@@ -664,6 +811,7 @@ void operator_interpolate_coefficient(pmg_operator &dst, pmg_operator &src, cuda
 }
 
 void operator_quadrature_points(const pmg_operator &op, double *xq, cudaStream_t s) {
+  require_mesh(op, "the quadrature points");
   PMG_REQUIRE(xq, "null output");
   PMG_CUDA(cudaSetDevice(op.device));
   if (op.n_cells == 0) return;
@@ -690,6 +838,7 @@ void operator_qp_form(const pmg_operator &op, const void *u, const void *v, doub
 // (the points at which deal.II's VectorTools::interpolate_boundary_values evaluates the
 // Dirichlet function, source/plain_solver/program.cc:125-131)
 void operator_dof_coordinates(const pmg_operator &op, double *xyz, cudaStream_t s) {
+  require_mesh(op, "the DoF coordinates");
   PMG_REQUIRE(xyz, "null output");
   PMG_CUDA(cudaSetDevice(op.device));
   if (op.n_cells == 0) return;
@@ -703,6 +852,7 @@ void operator_dof_coordinates(const pmg_operator &op, double *xyz, cudaStream_t 
 }
 
 double operator_l2_error(const pmg_operator &op, const void *u, int exact_kind, int nq, cudaStream_t s) {
+  require_mesh(op, "the error norm");
   PMG_REQUIRE(u, "null vector");
   PMG_REQUIRE(exact_kind == 1 || exact_kind == 2, "exact_kind must be 1 (sine) or 2 (exp-sine-cosine)");
   if (nq <= 0) nq = op.nq + 1;

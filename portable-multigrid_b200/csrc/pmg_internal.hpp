@@ -176,6 +176,7 @@ struct DGHost;
 
 struct pmg_operator {
   int device = 0;
+  bool from_maps = false;           // built from a caller's index map and geometry (no mesh)
   int kind = PMG_OP_LAPLACE;        // PMG_OP_LAPLACE, PMG_OP_DG_SIPG or PMG_OP_MASS
   std::shared_ptr<pmg::DGHost> dg;  // face data of a DG operator
   int degree = 1, nm = 2, nq = 2;
@@ -217,6 +218,12 @@ struct pmg_operator {
 namespace pmg {
 // operator.cu
 void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_params &prm);
+void operator_setup_from_maps(pmg_operator &op, const pmg_operator_maps &maps, const pmg_operator_params &prm);
+// fails with PMG_ESTATE for operators built from caller maps (no box mesh behind them)
+inline void require_mesh(const pmg_operator &op, const char *what) {
+  if (op.from_maps)
+    fail(PMG_ESTATE, std::string(what) + " needs the library's box mesh; this operator was built from caller maps");
+}
 void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s,
                     bool compute = true);
 void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s);

@@ -250,9 +250,104 @@ bool same_box_geometry(const pmg_box &a, const pmg_box &b) {
   return a.deform == b.deform && a.amp == b.amp && a.dirichlet_mask == b.dirichlet_mask;
 }
 
+// weights (1 / multiplicity of the fine DoF over all patches, 0 when constrained, unless
+// given), the 1D matrix and the maps on the device, launch parameters
+void transfer_finish(pmg_transfer &t, const pmg_operator &fine, const std::vector<double> &P,
+                     const std::vector<uint32_t> &cidx, const std::vector<uint32_t> &fidx,
+                     const double *given_weights) {
+  std::vector<double> w(fidx.size());
+  if (given_weights) {
+    std::copy(given_weights, given_weights + fidx.size(), w.begin());
+  } else {
+    std::vector<double> mult(t.n_fine, 0.0);
+    for (uint32_t d : fidx) mult[d] += 1.0;
+    for (int64_t i = 0; i < t.n_fine; ++i)
+      mult[i] = (fine.num.constrained[i] || mult[i] == 0.0) ? 0.0 : 1.0 / mult[i];
+    for (size_t e = 0; e < fidx.size(); ++e) w[e] = mult[fidx[e]];
+  }
+  t.P_host = P;
+  if (t.dtype == PMG_F64) {
+    t.P1d = upload(P);
+    t.weights = upload(w);
+  } else {
+    t.P1d = upload(cast<float>(P));
+    t.weights = upload(cast<float>(w));
+  }
+  t.coarse_idx = upload(cidx);
+  t.fine_idx = upload(fidx);
+  const size_t s = dtype_size(t.dtype);
+  const int nf3 = t.nf * t.nf * t.nf;
+  t.ppb = (int)std::max<size_t>(1, (32 * 1024) / (3 * nf3 * s));
+  t.smem = s * (((t.nc * t.nf + 3) & ~3) + (size_t)t.ppb * 3 * nf3);
+  int sms = 0;
+  PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t.device));
+  t.sms = sms;
+  t.patch_kernels = patch_kernels_enabled();
+  t.grid = (int)std::max<int64_t>(1, std::min<int64_t>((t.n_patches + t.ppb - 1) / t.ppb, (int64_t)sms * 8));
+  if (t.dtype == PMG_F64)
+    PMG_CUDA(cudaFuncSetAttribute(transfer_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  else
+    PMG_CUDA(cudaFuncSetAttribute(transfer_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+}
+
 } // namespace
 
+void transfer_setup_from_maps(pmg_transfer &t, const pmg_operator &coarse, const pmg_operator &fine,
+                              const pmg_transfer_maps &m) {
+  PMG_REQUIRE(coarse.dtype == fine.dtype, "transfer levels must have the same dtype");
+  PMG_REQUIRE(coarse.device == fine.device, "transfer levels must live on one device");
+  PMG_REQUIRE(m.n_patches >= 0, "negative patch count");
+  PMG_REQUIRE(m.n_patches == 0 || (m.coarse_indices && m.fine_indices), "null index map");
+  PMG_CUDA(cudaSetDevice(fine.device));
+  t.device = fine.device;
+  t.dtype = fine.dtype;
+  t.n_coarse = coarse.n_dofs;
+  t.n_fine = fine.n_dofs;
+  t.n_patches = m.n_patches;
+  const int pc = coarse.degree, pf = fine.degree;
+  std::vector<double> P;
+  if (m.kind == PMG_TRANSFER_POLYNOMIAL) {
+    PMG_REQUIRE(pc < pf, "polynomial transfer needs degree_coarse < degree_fine");
+    t.kind = 0;
+    t.nc = pc + 1;
+    t.nf = pf + 1;
+    P = p_transfer_matrix(pc, pf);
+  } else if (m.kind == PMG_TRANSFER_GEOMETRIC) {
+    PMG_REQUIRE(pc == pf, "geometric transfer needs equal degrees");
+    t.kind = 1;
+    t.nc = pc + 1;
+    t.nf = 2 * pc + 1;
+    P = h_transfer_matrix(pc);
+  } else if (m.kind == PMG_TRANSFER_DG_CG) {
+    PMG_REQUIRE(pc == pf, "DG <-> CG transfer needs equal degrees");
+    t.kind = 2;
+    t.nc = t.nf = pc + 1;
+    P.assign(t.nc * t.nf, 0.0);
+    for (int i = 0; i < t.nc; ++i) P[i * t.nf + i] = 1.0;
+  } else {
+    fail(PMG_EINVAL, "kind must be PMG_TRANSFER_POLYNOMIAL, _GEOMETRIC or _DG_CG");
+  }
+  const size_t nc3 = (size_t)t.nc * t.nc * t.nc, nf3 = (size_t)t.nf * t.nf * t.nf;
+  std::vector<uint32_t> cidx(m.coarse_indices, m.coarse_indices + m.n_patches * nc3);
+  std::vector<uint32_t> fidx(m.fine_indices, m.fine_indices + m.n_patches * nf3);
+  for (size_t e = 0; e < cidx.size(); ++e) {
+    uint32_t &d = cidx[e];
+    if (d == kInvalid) continue;
+    if ((int64_t)d >= t.n_coarse)
+      fail(PMG_EBOUNDS, "coarse_indices[" + std::to_string(e) + "] = " + std::to_string(d) + " >= " +
+                            std::to_string(t.n_coarse));
+    if (coarse.num.constrained[d]) d = kInvalid;
+  }
+  for (size_t e = 0; e < fidx.size(); ++e)
+    if ((int64_t)fidx[e] >= t.n_fine)
+      fail(PMG_EBOUNDS, "fine_indices[" + std::to_string(e) + "] = " + std::to_string(fidx[e]) + " >= " +
+                            std::to_string(t.n_fine));
+  transfer_finish(t, fine, P, cidx, fidx, m.weights);
+}
+
 void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_operator &fine) {
+  PMG_REQUIRE(!coarse.from_maps && !fine.from_maps,
+              "operators built from caller maps take their transfers from pmg_transfer_create_from_maps");
   PMG_REQUIRE(coarse.dtype == fine.dtype, "transfer levels must have the same dtype");
   PMG_REQUIRE(coarse.device == fine.device, "transfer levels must live on one device");
   PMG_REQUIRE(same_box_geometry(coarse.mesh.box, fine.mesh.box), "levels must discretise the same box");
@@ -323,36 +418,7 @@ void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_opera
             fidx[c * nf3 + (k * nf + j) * nf + i] = fine.num.lattice[((bz + k) * L1 + (by + j)) * L0 + bx + i];
     }
   }
-  // weights: 1 / multiplicity of the fine DoF over all patches, 0 when constrained
-  std::vector<double> mult(t.n_fine, 0.0);
-  for (uint32_t d : fidx) mult[d] += 1.0;
-  for (int64_t i = 0; i < t.n_fine; ++i)
-    mult[i] = (fine.num.constrained[i] || mult[i] == 0.0) ? 0.0 : 1.0 / mult[i];
-  std::vector<double> w(fidx.size());
-  for (size_t e = 0; e < fidx.size(); ++e) w[e] = mult[fidx[e]];
-  t.P_host = P;
-  if (t.dtype == PMG_F64) {
-    t.P1d = upload(P);
-    t.weights = upload(w);
-  } else {
-    t.P1d = upload(cast<float>(P));
-    t.weights = upload(cast<float>(w));
-  }
-  t.coarse_idx = upload(cidx);
-  t.fine_idx = upload(fidx);
-  const size_t s = dtype_size(t.dtype);
-  const int nf3 = t.nf * t.nf * t.nf;
-  t.ppb = (int)std::max<size_t>(1, (32 * 1024) / (3 * nf3 * s));
-  t.smem = s * (((t.nc * t.nf + 3) & ~3) + (size_t)t.ppb * 3 * nf3);
-  int sms = 0;
-  PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t.device));
-  t.sms = sms;
-  t.patch_kernels = patch_kernels_enabled();
-  t.grid = (int)std::max<int64_t>(1, std::min<int64_t>((t.n_patches + t.ppb - 1) / t.ppb, (int64_t)sms * 8));
-  if (t.dtype == PMG_F64)
-    PMG_CUDA(cudaFuncSetAttribute(transfer_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-  else
-    PMG_CUDA(cudaFuncSetAttribute(transfer_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  transfer_finish(t, fine, P, cidx, fidx, nullptr);
 }
 
 void transfer_apply(const pmg_transfer &t, int dir, void *dst, const void *src, cudaStream_t s) {

@@ -24,6 +24,8 @@ struct pmg_transfer {
 
 namespace pmg {
 void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_operator &fine);
+void transfer_setup_from_maps(pmg_transfer &t, const pmg_operator &coarse, const pmg_operator &fine,
+                              const pmg_transfer_maps &maps);
 // dir 0: dst_fine += P src_coarse;  dir 1: dst_coarse += P^T src_fine
 void transfer_apply(const pmg_transfer &t, int dir, void *dst, const void *src, cudaStream_t s);
 } // namespace pmg

@@ -93,6 +93,10 @@ template <typename T> __global__ void xpay_k(T *p, const T *z, T beta, int64_t n
   GRID_STRIDE(i, n) p[i] = z[i] + beta * p[i];
 }
 
+template <typename T> __global__ void axpy_k(T *y, const T *x, T alpha, int64_t n) {
+  GRID_STRIDE(i, n) y[i] += alpha * x[i];
+}
+
 // block partial sums of a*b (or of the CG update's new r*r), FP64 accumulation
 template <typename T>
 __device__ __forceinline__ void block_reduce_store(double v, double *partials) {
@@ -282,6 +286,12 @@ void jacobi(void *z, const void *invd, const void *r, int dtype, int64_t n, cuda
 void xpay(void *p, const void *z, double beta, int dtype, int64_t n, cudaStream_t s) {
   prof::Scope scope_("vector_update", s);
   DISPATCH(dtype, xpay_k<T><<<grid_for(n), kBlock, 0, s>>>(static_cast<T *>(p), static_cast<const T *>(z), (T)beta, n));
+  PMG_LAUNCH_CHECK();
+}
+
+void axpy(void *y, const void *x, double alpha, int dtype, int64_t n, cudaStream_t s) {
+  prof::Scope scope_("vector_update", s);
+  DISPATCH(dtype, axpy_k<T><<<grid_for(n), kBlock, 0, s>>>(static_cast<T *>(y), static_cast<const T *>(x), (T)alpha, n));
   PMG_LAUNCH_CHECK();
 }
 

@@ -26,6 +26,7 @@ void cheb_update_into(void *out, const void *cur, const void *prev, const void *
 void residual(void *t, const void *def, int dtype, int64_t n, cudaStream_t s);
 void jacobi(void *z, const void *invd, const void *r, int dtype, int64_t n, cudaStream_t s);
 void xpay(void *p, const void *z, double beta, int dtype, int64_t n, cudaStream_t s);
+void axpy(void *y, const void *x, double alpha, int dtype, int64_t n, cudaStream_t s); // y += alpha x
 double dot(const void *a, const void *b, int dtype, int64_t n, cudaStream_t s);
 double cg_update(void *x, void *r, const void *p, const void *v, double alpha, int dtype, int64_t n,
                  cudaStream_t s);

@@ -35,6 +35,8 @@ GEOMETRY_AUTO, GEOMETRY_FULL, GEOMETRY_AFFINE, GEOMETRY_INVJAC = 0, 1, 2, 3
 COEFF_NONE, COEFF_KAPPA, COEFF_VALUES = 0, 1, 2
 OP_LAPLACE, OP_DG_SIPG, OP_MASS = 0, 1, 2
 KERNEL_VMULT_CELL, KERNEL_DG_FACES, KERNEL_MASS, KERNEL_QP_FORM = 0, 1, 2, 3
+MAPS_G, MAPS_INVJAC = 0, 1
+TRANSFER_POLYNOMIAL, TRANSFER_GEOMETRIC, TRANSFER_DG_CG = 0, 1, 2
 INVALID = 0xFFFFFFFF
 STATUS = {0: "PMG_OK", -1: "PMG_EINVAL", -2: "PMG_ENOMEM", -3: "PMG_ECUDA",
           -4: "PMG_ENONFINITE", -5: "PMG_ENOCONV", -6: "PMG_EBOUNDS", -7: "PMG_ESTATE",
@@ -98,6 +100,17 @@ class CGInfo(C.Structure):
                 ("reduction_per_step", C.c_double)]
 
 
+class OperatorMaps(C.Structure):
+    _fields_ = [("n_cells", C.c_int64), ("n_dofs", C.c_int64), ("dof_indices", C.c_void_p),
+                ("constrained", C.c_void_p), ("n_constrained", C.c_int64), ("geometry", C.c_int32),
+                ("G", C.c_void_p), ("inv_jacobian", C.c_void_p), ("JxW", C.c_void_p)]
+
+
+class TransferMaps(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_patches", C.c_int64), ("coarse_indices", C.c_void_p),
+                ("fine_indices", C.c_void_p), ("weights", C.c_void_p)]
+
+
 class Peaks(C.Structure):
     _fields_ = [("copy_gbs", C.c_double), ("fp64_fma_tflops", C.c_double), ("fp32_fma_tflops", C.c_double),
                 ("copy_bytes", C.c_int64), ("sm_count", C.c_int32)]
@@ -143,6 +156,8 @@ def _declare(L):
         "pmg_mesh_n_cells": ([vp, P(i64)], i32),
         "pmg_operator_create": ([vp, P(OperatorParams), P(vp)], i32),
         "pmg_operator_destroy": ([vp], i32),
+        "pmg_operator_create_from_maps": ([P(OperatorMaps), P(OperatorParams), P(vp)], i32),
+        "pmg_transfer_create_from_maps": ([vp, vp, P(TransferMaps), P(vp)], i32),
         "pmg_operator_m": ([vp, P(i64)], i32),
         "pmg_operator_n": ([vp, P(i64)], i32),
         "pmg_operator_n_cells": ([vp, P(i64)], i32),
@@ -185,6 +200,10 @@ def _declare(L):
         "pmg_cg_solve": ([vp, vp, vp, vp, d, d, i32, P(CGInfo), vp], i32),
         "pmg_vector_dot": ([vp, vp, i32, i64, P(d), vp], i32),
         "pmg_vector_copy": ([vp, i32, vp, i32, i64, vp], i32),
+        "pmg_vector_axpy": ([vp, vp, d, i32, i64, vp], i32),
+        "pmg_vector_xpay": ([vp, vp, d, i32, i64, vp], i32),
+        "pmg_vector_pointwise_mult": ([vp, vp, vp, i32, i64, vp], i32),
+        "pmg_operator_dof_lattice": ([vp, vp], i32),
         "pmg_profile_enable": ([i32], i32),
         "pmg_profile_reset": ([], i32),
         "pmg_profile_query": ([C.c_char_p, P(d), P(i64)], i32),
@@ -231,6 +250,21 @@ def vector_dot(a, b):
 def vector_copy(dst, src):
     """dst = src with precision conversion (copy_locally_owned_data_from)."""
     check(lib().pmg_vector_copy(_ptr(dst), _dt(dst), _ptr(src), _dt(src), src.numel(), _stream()))
+
+
+def vector_axpy(y, x, alpha):
+    """y += alpha x (device vectors of one dtype)."""
+    check(lib().pmg_vector_axpy(_ptr(y), _ptr(x), float(alpha), _dt(y), y.numel(), _stream()))
+
+
+def vector_xpay(y, x, alpha):
+    """y = x + alpha y."""
+    check(lib().pmg_vector_xpay(_ptr(y), _ptr(x), float(alpha), _dt(y), y.numel(), _stream()))
+
+
+def vector_pointwise_mult(z, d, r):
+    """z = d .* r."""
+    check(lib().pmg_vector_pointwise_mult(_ptr(z), _ptr(d), _ptr(r), _dt(z), z.numel(), _stream()))
 
 
 def profile_enable(on=True):
@@ -292,6 +326,37 @@ class LaplaceOperator:
             prm.coeff_qp = self._coeff.ctypes.data_as(C.c_void_p)
         self.h = C.c_void_p()
         check(lib().pmg_operator_create(mesh.h, C.byref(prm), C.byref(self.h)))
+
+    @classmethod
+    def from_maps(cls, n_dofs, dof_indices, constrained, degree, dtype=F64, G=None, inv_jacobian=None,
+                  JxW=None, device=0):
+        """An operator on the caller's own discretisation (pmg_operator_create_from_maps):
+        dof_indices [C, (degree+1)^3] uint32 with 0xFFFFFFFF on constrained DoFs, the list of
+        constrained DoFs, and either G [C, 6, nq^3] or inv_jacobian [C, nq^3, 3, 3] with
+        JxW [C, nq^3]."""
+        self = cls.__new__(cls)
+        self.mesh, self.degree, self.dtype, self.device, self.kind, self._coeff = None, degree, dtype, device, OP_LAPLACE, None
+        idx = np.ascontiguousarray(dof_indices, dtype=np.uint32)
+        cons = np.ascontiguousarray(constrained, dtype=np.uint32).reshape(-1)
+        nm3 = (degree + 1) ** 3
+        n_cells = idx.size // nm3
+        m = OperatorMaps(n_cells, int(n_dofs), idx.ctypes.data_as(C.c_void_p), cons.ctypes.data_as(C.c_void_p),
+                         cons.size, MAPS_G if G is not None else MAPS_INVJAC, None, None, None)
+        keep = [idx, cons]
+        if G is not None:
+            g = np.ascontiguousarray(G, dtype=np.float64)
+            keep.append(g)
+            m.G = g.ctypes.data_as(C.c_void_p)
+        else:
+            ij = np.ascontiguousarray(inv_jacobian, dtype=np.float64)
+            jw = np.ascontiguousarray(JxW, dtype=np.float64)
+            keep += [ij, jw]
+            m.inv_jacobian = ij.ctypes.data_as(C.c_void_p)
+            m.JxW = jw.ctypes.data_as(C.c_void_p)
+        prm = OperatorParams(degree, dtype, GEOMETRY_AUTO, COEFF_NONE, None, device, OP_LAPLACE, 0.0)
+        self.h = C.c_void_p()
+        check(lib().pmg_operator_create_from_maps(C.byref(m), C.byref(prm), C.byref(self.h)))
+        return self
 
     @property
     def torch_dtype(self):
@@ -358,6 +423,12 @@ class LaplaceOperator:
         out = np.zeros(self.n_cells() * nm3, dtype=np.uint32)
         check(lib().pmg_operator_copy_dof_indices(self.h, out.ctypes.data_as(C.c_void_p)))
         return out.reshape(-1, nm3)
+
+    def dof_lattice(self):
+        """Node-lattice coordinates (i, j, k) of every DoF, int32 [m, 3] (host)."""
+        out = np.zeros((self.m(), 3), dtype=np.int32)
+        check(lib().pmg_operator_dof_lattice(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out
 
     def constrained(self):
         out = np.zeros(self.m(), dtype=np.uint8)
@@ -433,6 +504,24 @@ class Transfer:
         self.coarse, self.fine = coarse, fine
         self.h = C.c_void_p()
         check(lib().pmg_transfer_create(coarse.h, fine.h, C.byref(self.h)))
+
+    @classmethod
+    def from_maps(cls, coarse: "LaplaceOperator", fine: "LaplaceOperator", kind, coarse_indices, fine_indices,
+                  weights=None):
+        """A transfer from the caller's patch maps (pmg_transfer_create_from_maps)."""
+        self = cls.__new__(cls)
+        self.coarse, self.fine = coarse, fine
+        ci = np.ascontiguousarray(coarse_indices, dtype=np.uint32)
+        fi = np.ascontiguousarray(fine_indices, dtype=np.uint32)
+        nc3 = (coarse.degree + 1) ** 3
+        m = TransferMaps(kind, ci.size // nc3, ci.ctypes.data_as(C.c_void_p), fi.ctypes.data_as(C.c_void_p), None)
+        w = None
+        if weights is not None:
+            w = np.ascontiguousarray(weights, dtype=np.float64)
+            m.weights = w.ctypes.data_as(C.c_void_p)
+        self.h = C.c_void_p()
+        check(lib().pmg_transfer_create_from_maps(coarse.h, fine.h, C.byref(m), C.byref(self.h)))
+        return self
 
     def prolongate_and_add(self, dst_fine, src_coarse):
         check(lib().pmg_transfer_prolongate_and_add(self.h, _ptr(dst_fine), _ptr(src_coarse), _stream()))
