@@ -255,9 +255,10 @@ pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host)
   return guarded(__func__, [&] {
     NEED(op);
     NEED(host);
-    for (size_t e = 0; e < op->num.plain.size(); ++e) {
-      const uint32_t d = op->num.plain[e];
-      host[e] = (d == pmg::kInvalid || op->num.constrained[d]) ? pmg::kInvalid : d;
+    const pmg::Numbering &num = pmg::host_numbering(*op);
+    for (size_t e = 0; e < num.plain.size(); ++e) {
+      const uint32_t d = num.plain[e];
+      host[e] = (d == pmg::kInvalid || num.constrained[d]) ? pmg::kInvalid : d;
     }
   });
 }
@@ -266,7 +267,8 @@ pmg_status pmg_operator_copy_constrained(const pmg_operator *op, uint8_t *host) 
   return guarded(__func__, [&] {
     NEED(op);
     NEED(host);
-    std::memcpy(host, op->num.constrained.data(), op->num.constrained.size());
+    const pmg::Numbering &num = pmg::host_numbering(*op);
+    std::memcpy(host, num.constrained.data(), num.constrained.size());
   });
 }
 
@@ -283,12 +285,13 @@ pmg_status pmg_operator_dof_lattice(const pmg_operator *op, int32_t *ijk) {
   return guarded(__func__, [&] {
     NEED(op);
     NEED(ijk);
-    if (op->from_maps || op->kind == PMG_OP_DG_SIPG || op->num.lattice.empty())
+    if (op->from_maps || op->kind == PMG_OP_DG_SIPG || !op->dlattice.get())
       pmg::fail(PMG_ESTATE, "DoF lattice coordinates exist for continuous operators on box meshes only");
-    const int64_t L0 = op->num.L[0], L1 = op->num.L[1];
-    const int64_t n_lat = (int64_t)op->num.lattice.size();
+    const pmg::Numbering &num = pmg::host_numbering(*op);
+    const int64_t L0 = num.L[0], L1 = num.L[1];
+    const int64_t n_lat = (int64_t)num.lattice.size();
     for (int64_t t = 0; t < n_lat; ++t) {
-      const uint32_t d = op->num.lattice[t];
+      const uint32_t d = num.lattice[t];
       if (d == pmg::kInvalid) continue;
       ijk[3 * (int64_t)d + 0] = (int32_t)(t % L0);
       ijk[3 * (int64_t)d + 1] = (int32_t)((t / L0) % L1);

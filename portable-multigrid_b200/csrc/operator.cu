@@ -7,6 +7,7 @@
 #include "dg.hpp"
 #include "fields.hpp"
 #include "vector_ops.hpp"
+#include "numbering.hpp"
 #include "pmg_internal.hpp"
 
 namespace pmg {
@@ -295,37 +296,17 @@ SlabLaunch slab_launch(const pmg_operator &op, const Tables1D &t, cudaStream_t s
 }
 
 // The index map with the sentinel, permuted into the Y-slab layout [group][k*N+i][e*N+j]
-// (setup_dof_indices_per_color, bk3.h:360-437) from op.num: entries that are constrained
-// DoFs, or the sentinel already, become the sentinel.
+// (setup_dof_indices_per_color, bk3.h:360-437) from the device numbering: entries that are
+// constrained DoFs, or the sentinel already, become the sentinel.
 void build_slab_index(pmg_operator &op) {
-  const int N = op.nm, N2 = N * N, N3 = N2 * N;
-  std::vector<uint32_t> perm((size_t)op.n_groups * N2 * op.lanes, kInvalid);
-  const uint32_t *plain = op.num.plain.data();
-  const uint8_t *cons = op.num.constrained.data();
-  const int64_t C = op.n_cells, lanes = op.lanes, cpw = op.cpw;
-#pragma omp parallel for schedule(static)
-  for (int64_t c = 0; c < C; ++c) {
-    const int64_t grp = c / cpw, e = c % cpw;
-    for (int k = 0; k < N; ++k)
-      for (int j = 0; j < N; ++j)
-        for (int i = 0; i < N; ++i) {
-          const uint32_t d = plain[c * N3 + (k * N + j) * N + i];
-          perm[(grp * N2 + k * N + i) * lanes + e * N + j] = (d == kInvalid || cons[d]) ? kInvalid : d;
-        }
-  }
-  op.idx = upload(perm);
+  device_slab_index(op.dplain.as<uint32_t>(), op.dcons.as<uint8_t>(), op.n_cells, op.nm, op.cpw, op.lanes,
+                    op.n_groups, op.sms, op.idx, nullptr);
 }
 
 // the constrained DoFs as a list and a bitmask (copy_constrained_values, bk3.h:230)
 void build_constrained(pmg_operator &op) {
-  std::vector<uint32_t> list;
-  for (int64_t i = 0; i < op.n_dofs; ++i)
-    if (op.num.constrained[i]) list.push_back((uint32_t)i);
-  op.n_constrained = (int64_t)list.size();
-  op.constrained_list = upload(list);
-  std::vector<uint32_t> bits((size_t)(op.n_dofs + 31) / 32, 0u);
-  for (uint32_t i : list) bits[i >> 5] |= 1u << (i & 31);
-  op.constrained_bits = upload(bits);
+  device_constrained(op.dcons.as<uint8_t>(), op.n_dofs, op.sms, op.constrained_list, op.constrained_bits,
+                     op.n_constrained, nullptr);
 }
 
 // persistent grids (as many warps as can be resident on this device) and the error flag
@@ -445,6 +426,9 @@ void operator_setup_from_maps(pmg_operator &op, const pmg_operator_maps &m, cons
                             std::to_string(m.n_dofs));
     if (op.num.constrained[d]) d = kInvalid;
   }
+  op.host_num_valid = true;
+  op.dplain = upload(op.num.plain);
+  op.dcons = upload(op.num.constrained);
   build_slab_index(op);
   build_constrained(op);
   // geometry: the caller's arrays, permuted into the slab layout on the device
@@ -513,11 +497,28 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   op.lanes = op.cpw * N;
   op.n_groups = (op.n_cells + op.cpw - 1) / op.cpw;
 
-  // numbering (setup_dof_indices_per_color, bk3.h:360-437)
-  op.num = op.kind == PMG_OP_DG_SIPG ? make_numbering_dg(mesh.m, op.degree)
-                                     : make_numbering(mesh.m, op.degree, true);
-  op.n_dofs = op.num.n_dofs;
+  // numbering (setup_dof_indices_per_color, bk3.h:360-437): first-visit order on the device
+  // for continuous operators; cell by cell for DG
   op.sms = num_sms(op.device);
+  op.cell_xyz = upload(mesh.m.cell_xyz);
+  if (op.kind == PMG_OP_DG_SIPG) {
+    op.num = make_numbering_dg(mesh.m, op.degree);
+    op.host_num_valid = true;
+    op.dplain = upload(op.num.plain);
+    op.dcons = upload(op.num.constrained);
+  } else {
+    DeviceNumbering dn;
+    device_numbering(mesh.m, op.degree, op.cell_xyz, op.sms, dn, nullptr);
+    op.num = Numbering{};
+    op.num.p = op.degree;
+    op.num.n_dofs = dn.n_dofs;
+    for (int d = 0; d < 3; ++d) op.num.L[d] = dn.L[d];
+    op.dplain = std::move(dn.plain);
+    op.dcons = std::move(dn.constrained);
+    op.dlattice = std::move(dn.lattice);
+    op.host_num_valid = false;
+  }
+  op.n_dofs = op.num.n_dofs;
   if (op.kind == PMG_OP_DG_SIPG) {
     op.dg = std::make_shared<DGHost>();
     dg_setup(*op.dg, mesh.m, op.degree, prm.penalty);
@@ -527,7 +528,6 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   build_constrained(op);
   // geometry (compute_G_tensors, bk3.h:456-515), computed on the device
   const size_t s = dtype_size(op.dtype);
-  op.cell_xyz = upload(mesh.m.cell_xyz);
   const DeviceBuffer &xyz = op.cell_xyz;
   // coefficient values (PMG_COEFF_VALUES): kept on the device in FP64 so that coarser levels
   // can interpolate them; no array given means the constant 1
@@ -842,13 +842,32 @@ void operator_dof_coordinates(const pmg_operator &op, double *xyz, cudaStream_t 
   PMG_REQUIRE(xyz, "null output");
   PMG_CUDA(cudaSetDevice(op.device));
   if (op.n_cells == 0) return;
-  DeviceBuffer plain = upload(op.num.plain);
   const GeoParams gp = make_geo_params(op, op.nq);
   const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)op.sms * 16);
   cell_geometry_kernel<double><<<grid, 128, 0, s>>>(gp, op.cell_xyz.as<int32_t>(), op.n_cells, 7, 0, nullptr, xyz,
-                                                    nullptr, 0, nullptr, plain.as<uint32_t>(), 0);
+                                                    nullptr, 0, nullptr, op.dplain.as<uint32_t>(), 0);
   PMG_LAUNCH_CHECK();
-  PMG_CUDA(cudaStreamSynchronize(s)); // the plain index map is freed on return
+  PMG_CUDA(cudaStreamSynchronize(s));
+}
+
+const Numbering &host_numbering(const pmg_operator &op) {
+  if (!op.host_num_valid) {
+    PMG_CUDA(cudaSetDevice(op.device));
+    const int64_t nm3 = (int64_t)op.nm * op.nm * op.nm;
+    op.num.plain.resize((size_t)op.n_cells * nm3);
+    op.num.constrained.resize((size_t)op.n_dofs);
+    if (!op.num.plain.empty())
+      PMG_CUDA(cudaMemcpy(op.num.plain.data(), op.dplain.get(), op.num.plain.size() * 4, cudaMemcpyDeviceToHost));
+    if (!op.num.constrained.empty())
+      PMG_CUDA(cudaMemcpy(op.num.constrained.data(), op.dcons.get(), op.num.constrained.size(),
+                          cudaMemcpyDeviceToHost));
+    if (op.dlattice.get()) {
+      op.num.lattice.resize(op.dlattice.bytes() / 4);
+      PMG_CUDA(cudaMemcpy(op.num.lattice.data(), op.dlattice.get(), op.dlattice.bytes(), cudaMemcpyDeviceToHost));
+    }
+    op.host_num_valid = true;
+  }
+  return op.num;
 }
 
 double operator_l2_error(const pmg_operator &op, const void *u, int exact_kind, int nq, cudaStream_t s) {
@@ -859,13 +878,12 @@ double operator_l2_error(const pmg_operator &op, const void *u, int exact_kind, 
   PMG_REQUIRE(nq >= 1 && nq <= kMaxNq, "nq must be in [1,8]");
   PMG_CUDA(cudaSetDevice(op.device));
   if (op.n_cells == 0) return 0.0;
-  DeviceBuffer plain = upload(op.num.plain);
   DeviceBuffer cell_err(sizeof(double) * op.n_cells);
   const GeoParams gp = make_geo_params(op, nq);
   const int grid = (int)std::min<int64_t>(op.n_cells, (int64_t)op.sms * 16);
   cell_geometry_kernel<double><<<grid, 128, 0, s>>>(gp, op.cell_xyz.as<int32_t>(), op.n_cells, 5, 0, nullptr,
                                                     cell_err.as<double>(), nullptr, exact_kind, u,
-                                                    plain.as<uint32_t>(), op.dtype == PMG_F32 ? 1 : 0);
+                                                    op.dplain.as<uint32_t>(), op.dtype == PMG_F32 ? 1 : 0);
   PMG_LAUNCH_CHECK();
   const double e2 = vec::dot(cell_err.get(), cell_err.get(), PMG_F64, op.n_cells, s); // synchronises
   return std::sqrt(e2);

@@ -188,7 +188,12 @@ struct pmg_operator {
   int64_t n_cells = 0, n_dofs = 0;
   int cpw = 1, lanes = 1;           // cells per warp group, active lanes per group
   int64_t n_groups = 0;
-  pmg::Numbering num;               // host copy (plain indices, constrained, lattice)
+  // numbering on the device: plain [C][nm^3] (no sentinel; caller maps: the sentinel kept),
+  // constrained flags [N], node lattice -> DoF (continuous box operators)
+  pmg::DeviceBuffer dplain, dcons, dlattice;
+  // host copy of the numbering, filled on first use (pmg::host_numbering); L and n_dofs always set
+  mutable pmg::Numbering num;
+  mutable bool host_num_valid = false;
   pmg::DeviceBuffer idx;            // permuted [group][nm^2][lanes] uint32
   pmg::DeviceBuffer geo;            // FULL: [group][nq^2][6][lanes]; AFFINE: [C][8]
   pmg::DeviceBuffer coef;           // AFFINE with coefficient: [group][nq^2][lanes];
@@ -219,6 +224,8 @@ namespace pmg {
 // operator.cu
 void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_params &prm);
 void operator_setup_from_maps(pmg_operator &op, const pmg_operator_maps &maps, const pmg_operator_params &prm);
+// the operator's numbering on the host (copied from the device on first use)
+const Numbering &host_numbering(const pmg_operator &op);
 // fails with PMG_ESTATE for operators built from caller maps (no box mesh behind them)
 inline void require_mesh(const pmg_operator &op, const char *what) {
   if (op.from_maps)

@@ -250,44 +250,102 @@ bool same_box_geometry(const pmg_box &a, const pmg_box &b) {
   return a.deform == b.deform && a.amp == b.amp && a.dirichlet_mask == b.dirichlet_mask;
 }
 
-// weights (1 / multiplicity of the fine DoF over all patches, 0 when constrained, unless
-// given), the 1D matrix and the maps on the device, launch parameters
+// ---- transfer maps and weights on the device (setup) ----
+// out[e] = the sentinel where plain[e] is one or a constrained DoF, else plain[e]
+__global__ void sentinel_map_kernel(const uint32_t *__restrict__ plain, const uint8_t *__restrict__ cons, int64_t n,
+                                    uint32_t *__restrict__ out) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = plain[e];
+    out[e] = (d == kInvalid || cons[d]) ? kInvalid : d;
+  }
+}
+
+// h-transfer patch of coarse cell c: the (2p+1)^3 fine nodes from 2p * (cell coordinates) on
+__global__ void h_patch_kernel(const int32_t *__restrict__ coarse_xyz, int64_t n_patches, int p,
+                               const uint32_t *__restrict__ fine_lattice, int64_t L0, int64_t L1,
+                               uint32_t *__restrict__ fidx) {
+  const int nf = 2 * p + 1, nf3 = nf * nf * nf;
+  const int64_t total = n_patches * nf3;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / nf3;
+    const int l = (int)(t - c * nf3);
+    const int i = l % nf, j = (l / nf) % nf, k = l / (nf * nf);
+    const int64_t x = 2LL * p * coarse_xyz[3 * c] + i, y = 2LL * p * coarse_xyz[3 * c + 1] + j,
+                  z = 2LL * p * coarse_xyz[3 * c + 2] + k;
+    fidx[t] = fine_lattice[(z * L1 + y) * L0 + x];
+  }
+}
+
+__global__ void multiplicity_kernel(const uint32_t *__restrict__ fidx, int64_t n, uint32_t *__restrict__ cnt) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(cnt + fidx[e], 1u);
+}
+
+// w[e] = 1 / (patches holding fine DoF fidx[e]), 0 on constrained fine DoFs
+template <typename T>
+__global__ void weights_kernel(const uint32_t *__restrict__ fidx, int64_t n, const uint32_t *__restrict__ cnt,
+                               const uint8_t *__restrict__ cons, T *__restrict__ w) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = fidx[e];
+    const uint32_t m = cnt[d];
+    w[e] = (cons[d] || m == 0) ? T(0) : (T)(1.0 / (double)m);
+  }
+}
+
+int setup_grid(int64_t n, int sms) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 32));
+}
+
+// the 1D matrix, the weights (1 / multiplicity of the fine DoF over all patches, 0 when
+// constrained, unless given), launch parameters; t.coarse_idx and t.fine_idx are set
 void transfer_finish(pmg_transfer &t, const pmg_operator &fine, const std::vector<double> &P,
-                     const std::vector<uint32_t> &cidx, const std::vector<uint32_t> &fidx,
                      const double *given_weights) {
-  std::vector<double> w(fidx.size());
-  if (given_weights) {
-    std::copy(given_weights, given_weights + fidx.size(), w.begin());
-  } else {
-    std::vector<double> mult(t.n_fine, 0.0);
-    for (uint32_t d : fidx) mult[d] += 1.0;
-    for (int64_t i = 0; i < t.n_fine; ++i)
-      mult[i] = (fine.num.constrained[i] || mult[i] == 0.0) ? 0.0 : 1.0 / mult[i];
-    for (size_t e = 0; e < fidx.size(); ++e) w[e] = mult[fidx[e]];
-  }
-  t.P_host = P;
-  if (t.dtype == PMG_F64) {
-    t.P1d = upload(P);
-    t.weights = upload(w);
-  } else {
-    t.P1d = upload(cast<float>(P));
-    t.weights = upload(cast<float>(w));
-  }
-  t.coarse_idx = upload(cidx);
-  t.fine_idx = upload(fidx);
-  const size_t s = dtype_size(t.dtype);
-  const int nf3 = t.nf * t.nf * t.nf;
-  t.ppb = (int)std::max<size_t>(1, (32 * 1024) / (3 * nf3 * s));
-  t.smem = s * (((t.nc * t.nf + 3) & ~3) + (size_t)t.ppb * 3 * nf3);
   int sms = 0;
   PMG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t.device));
   t.sms = sms;
+  const int64_t nf3 = (int64_t)t.nf * t.nf * t.nf, n_w = t.n_patches * nf3;
+  t.P_host = P;
+  if (t.dtype == PMG_F64) t.P1d = upload(P);
+  else t.P1d = upload(cast<float>(P));
+  if (given_weights) {
+    std::vector<double> w(given_weights, given_weights + n_w);
+    if (t.dtype == PMG_F64) t.weights = upload(w);
+    else t.weights = upload(cast<float>(w));
+  } else {
+    t.weights.allocate(dtype_size(t.dtype) * std::max<int64_t>(1, n_w));
+    if (n_w > 0) {
+      DeviceBuffer cnt(sizeof(uint32_t) * std::max<int64_t>(1, t.n_fine));
+      PMG_CUDA(cudaMemset(cnt.get(), 0, cnt.bytes()));
+      multiplicity_kernel<<<setup_grid(n_w, sms), 256>>>(t.fine_idx.as<uint32_t>(), n_w, cnt.as<uint32_t>());
+      PMG_LAUNCH_CHECK();
+      if (t.dtype == PMG_F64)
+        weights_kernel<double><<<setup_grid(n_w, sms), 256>>>(t.fine_idx.as<uint32_t>(), n_w, cnt.as<uint32_t>(),
+                                                              fine.dcons.as<uint8_t>(), t.weights.as<double>());
+      else
+        weights_kernel<float><<<setup_grid(n_w, sms), 256>>>(t.fine_idx.as<uint32_t>(), n_w, cnt.as<uint32_t>(),
+                                                             fine.dcons.as<uint8_t>(), t.weights.as<float>());
+      PMG_LAUNCH_CHECK();
+      PMG_CUDA(cudaDeviceSynchronize()); // cnt is freed on return
+    }
+  }
+  const size_t s = dtype_size(t.dtype);
+  t.ppb = (int)std::max<size_t>(1, (32 * 1024) / (3 * nf3 * s));
+  t.smem = s * (((t.nc * t.nf + 3) & ~3) + (size_t)t.ppb * 3 * nf3);
   t.patch_kernels = patch_kernels_enabled();
   t.grid = (int)std::max<int64_t>(1, std::min<int64_t>((t.n_patches + t.ppb - 1) / t.ppb, (int64_t)sms * 8));
   if (t.dtype == PMG_F64)
     PMG_CUDA(cudaFuncSetAttribute(transfer_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   else
     PMG_CUDA(cudaFuncSetAttribute(transfer_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+}
+
+// coarse map with the sentinel from the coarse operator's device numbering
+void coarse_map_from(pmg_transfer &t, const pmg_operator &coarse, const uint32_t *plain, int64_t n) {
+  t.coarse_idx.allocate(sizeof(uint32_t) * std::max<int64_t>(1, n));
+  if (n == 0) return;
+  sentinel_map_kernel<<<setup_grid(n, t.sms > 0 ? t.sms : 148), 256>>>(plain, coarse.dcons.as<uint8_t>(), n,
+                                                                      t.coarse_idx.as<uint32_t>());
+  PMG_LAUNCH_CHECK();
 }
 
 } // namespace
@@ -304,6 +362,7 @@ void transfer_setup_from_maps(pmg_transfer &t, const pmg_operator &coarse, const
   t.n_coarse = coarse.n_dofs;
   t.n_fine = fine.n_dofs;
   t.n_patches = m.n_patches;
+  PMG_CUDA(cudaDeviceGetAttribute(&t.sms, cudaDevAttrMultiProcessorCount, t.device));
   const int pc = coarse.degree, pf = fine.degree;
   std::vector<double> P;
   if (m.kind == PMG_TRANSFER_POLYNOMIAL) {
@@ -328,21 +387,23 @@ void transfer_setup_from_maps(pmg_transfer &t, const pmg_operator &coarse, const
     fail(PMG_EINVAL, "kind must be PMG_TRANSFER_POLYNOMIAL, _GEOMETRIC or _DG_CG");
   }
   const size_t nc3 = (size_t)t.nc * t.nc * t.nc, nf3 = (size_t)t.nf * t.nf * t.nf;
-  std::vector<uint32_t> cidx(m.coarse_indices, m.coarse_indices + m.n_patches * nc3);
-  std::vector<uint32_t> fidx(m.fine_indices, m.fine_indices + m.n_patches * nf3);
-  for (size_t e = 0; e < cidx.size(); ++e) {
-    uint32_t &d = cidx[e];
-    if (d == kInvalid) continue;
-    if ((int64_t)d >= t.n_coarse)
+  const size_t n_c = (size_t)m.n_patches * nc3, n_f = (size_t)m.n_patches * nf3;
+  for (size_t e = 0; e < n_c; ++e) {
+    const uint32_t d = m.coarse_indices[e];
+    if (d != kInvalid && (int64_t)d >= t.n_coarse)
       fail(PMG_EBOUNDS, "coarse_indices[" + std::to_string(e) + "] = " + std::to_string(d) + " >= " +
                             std::to_string(t.n_coarse));
-    if (coarse.num.constrained[d]) d = kInvalid;
   }
-  for (size_t e = 0; e < fidx.size(); ++e)
-    if ((int64_t)fidx[e] >= t.n_fine)
-      fail(PMG_EBOUNDS, "fine_indices[" + std::to_string(e) + "] = " + std::to_string(fidx[e]) + " >= " +
+  for (size_t e = 0; e < n_f; ++e)
+    if ((int64_t)m.fine_indices[e] >= t.n_fine)
+      fail(PMG_EBOUNDS, "fine_indices[" + std::to_string(e) + "] = " + std::to_string(m.fine_indices[e]) + " >= " +
                             std::to_string(t.n_fine));
-  transfer_finish(t, fine, P, cidx, fidx, m.weights);
+  // caller maps: coarse entries naming constrained coarse DoFs become the sentinel
+  DeviceBuffer craw = upload(std::vector<uint32_t>(m.coarse_indices, m.coarse_indices + n_c));
+  coarse_map_from(t, coarse, craw.as<uint32_t>(), (int64_t)n_c);
+  t.fine_idx = upload(std::vector<uint32_t>(m.fine_indices, m.fine_indices + n_f));
+  PMG_CUDA(cudaDeviceSynchronize()); // craw is freed on return
+  transfer_finish(t, fine, P, m.weights);
 }
 
 void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_operator &fine) {
@@ -356,69 +417,57 @@ void transfer_setup(pmg_transfer &t, const pmg_operator &coarse, const pmg_opera
   t.dtype = fine.dtype;
   t.n_coarse = coarse.n_dofs;
   t.n_fine = fine.n_dofs;
+  PMG_CUDA(cudaDeviceGetAttribute(&t.sms, cudaDevAttrMultiProcessorCount, t.device));
   const int pc = coarse.degree, pf = fine.degree;
+  const int64_t cnm3 = (int64_t)(pc + 1) * (pc + 1) * (pc + 1);
   std::vector<double> P;
-  std::vector<uint32_t> cidx, fidx;
-  if (fine.kind == PMG_OP_DG_SIPG) {
-    // DG <-> CG at equal degree (ContinuousTransfer): identity on every cell, unit weights
-    PMG_REQUIRE(coarse.kind == PMG_OP_LAPLACE, "the coarse level of a DG transfer must be continuous");
-    PMG_REQUIRE(pc == pf && coarse.mesh.box.refine == fine.mesh.box.refine,
-                "DG <-> CG transfer needs equal degrees on the same mesh");
-    t.kind = 2;
-    t.nc = t.nf = pc + 1;
-    t.n_patches = fine.n_cells;
-    P.assign(t.nc * t.nf, 0.0);
-    for (int i = 0; i < t.nc; ++i) P[i * t.nf + i] = 1.0;
-    cidx.resize(coarse.num.plain.size());
-    for (size_t e = 0; e < cidx.size(); ++e) {
-      const uint32_t d = coarse.num.plain[e];
-      cidx[e] = coarse.num.constrained[d] ? kInvalid : d;
+  if (fine.kind == PMG_OP_DG_SIPG || coarse.mesh.box.refine == fine.mesh.box.refine) {
+    if (fine.kind == PMG_OP_DG_SIPG) {
+      // DG <-> CG at equal degree (ContinuousTransfer): identity on every cell
+      PMG_REQUIRE(coarse.kind == PMG_OP_LAPLACE, "the coarse level of a DG transfer must be continuous");
+      PMG_REQUIRE(pc == pf && coarse.mesh.box.refine == fine.mesh.box.refine,
+                  "DG <-> CG transfer needs equal degrees on the same mesh");
+      t.kind = 2;
+      t.nc = t.nf = pc + 1;
+      P.assign(t.nc * t.nf, 0.0);
+      for (int i = 0; i < t.nc; ++i) P[i * t.nf + i] = 1.0;
+    } else {
+      PMG_REQUIRE(coarse.kind == PMG_OP_LAPLACE, "a DG level can only be the finest level of a transfer");
+      PMG_REQUIRE(pc < pf, "polynomial transfer needs degree_coarse < degree_fine");
+      t.kind = 0;
+      t.nc = pc + 1;
+      t.nf = pf + 1;
+      P = p_transfer_matrix(pc, pf);
     }
-    fidx = fine.num.plain;
-  } else if (coarse.mesh.box.refine == fine.mesh.box.refine) {
-    PMG_REQUIRE(coarse.kind == PMG_OP_LAPLACE, "a DG level can only be the finest level of a transfer");
-    PMG_REQUIRE(pc < pf, "polynomial transfer needs degree_coarse < degree_fine");
-    t.kind = 0;
-    t.nc = pc + 1;
-    t.nf = pf + 1;
+    // one patch per cell of the common mesh: the coarse map with the sentinel, the fine map
     t.n_patches = fine.n_cells;
-    P = p_transfer_matrix(pc, pf);
-    const int nc3 = t.nc * t.nc * t.nc;
-    cidx.resize((size_t)t.n_patches * nc3);
-    for (size_t e = 0; e < cidx.size(); ++e) {
-      const uint32_t d = coarse.num.plain[e];
-      cidx[e] = coarse.num.constrained[d] ? kInvalid : d;
-    }
-    fidx = fine.num.plain;
+    coarse_map_from(t, coarse, coarse.dplain.as<uint32_t>(), t.n_patches * cnm3);
+    const int64_t n_f = t.n_patches * t.nf * t.nf * t.nf;
+    t.fine_idx.allocate(sizeof(uint32_t) * std::max<int64_t>(1, n_f));
+    if (n_f > 0)
+      PMG_CUDA(cudaMemcpy(t.fine_idx.get(), fine.dplain.get(), sizeof(uint32_t) * n_f, cudaMemcpyDeviceToDevice));
   } else {
     PMG_REQUIRE(fine.mesh.box.refine == coarse.mesh.box.refine + 1,
                 "geometric transfer needs the fine mesh refined exactly once more");
     PMG_REQUIRE(pc == pf, "geometric transfer needs equal degrees");
-    PMG_REQUIRE(!fine.num.lattice.empty(), "fine operator has no node lattice");
+    PMG_REQUIRE(fine.dlattice.get() != nullptr, "fine operator has no node lattice");
     const int p = pc;
     t.kind = 1;
     t.nc = p + 1;
     t.nf = 2 * p + 1;
     t.n_patches = coarse.n_cells;
     P = h_transfer_matrix(p);
-    const int nc3 = t.nc * t.nc * t.nc, nf = t.nf, nf3 = nf * nf * nf;
-    cidx.resize((size_t)t.n_patches * nc3);
-    for (size_t e = 0; e < cidx.size(); ++e) {
-      const uint32_t d = coarse.num.plain[e];
-      cidx[e] = coarse.num.constrained[d] ? kInvalid : d;
-    }
-    fidx.resize((size_t)t.n_patches * nf3);
-    const int64_t L0 = fine.num.L[0], L1 = fine.num.L[1];
-    for (int64_t c = 0; c < t.n_patches; ++c) {
-      const int64_t bx = 2LL * p * coarse.mesh.cell_xyz[3 * c], by = 2LL * p * coarse.mesh.cell_xyz[3 * c + 1],
-                    bz = 2LL * p * coarse.mesh.cell_xyz[3 * c + 2];
-      for (int k = 0; k < nf; ++k)
-        for (int j = 0; j < nf; ++j)
-          for (int i = 0; i < nf; ++i)
-            fidx[c * nf3 + (k * nf + j) * nf + i] = fine.num.lattice[((bz + k) * L1 + (by + j)) * L0 + bx + i];
+    coarse_map_from(t, coarse, coarse.dplain.as<uint32_t>(), t.n_patches * cnm3);
+    const int64_t n_f = t.n_patches * t.nf * t.nf * t.nf;
+    t.fine_idx.allocate(sizeof(uint32_t) * std::max<int64_t>(1, n_f));
+    if (n_f > 0) {
+      h_patch_kernel<<<setup_grid(n_f, t.sms), 256>>>(coarse.cell_xyz.as<int32_t>(), t.n_patches, p,
+                                                       fine.dlattice.as<uint32_t>(), fine.num.L[0], fine.num.L[1],
+                                                       t.fine_idx.as<uint32_t>());
+      PMG_LAUNCH_CHECK();
     }
   }
-  transfer_finish(t, fine, P, cidx, fidx, nullptr);
+  transfer_finish(t, fine, P, nullptr);
 }
 
 void transfer_apply(const pmg_transfer &t, int dir, void *dst, const void *src, cudaStream_t s) {
