@@ -75,6 +75,11 @@ typedef struct {
 pmg_status pmg_mesh_create_box(const pmg_box *box, pmg_mesh **mesh);
 pmg_status pmg_mesh_destroy(pmg_mesh *mesh);
 pmg_status pmg_mesh_n_cells(const pmg_mesh *mesh, int64_t *n_cells);
+/* Integer coordinates (x, y, z) of every cell in the box's cell grid, in cell order, host
+ * array xyz[n_cells][3]: the cell's lowest node sits at degree * (x, y, z) in the node lattice
+ * (the child offsets a geometric transfer between refinements follows,
+ * include/multigrid/portable_geometric_transfer.h:1095-1098). */
+pmg_status pmg_mesh_cell_coordinates(const pmg_mesh *mesh, int32_t *xyz);
 
 /* ---------------------------------------------------------------------------------- */
 /* Level operators: Portable::LaplaceOperatorBase<3,Number>                           */
@@ -433,6 +438,11 @@ pmg_status pmg_vector_axpy(void *y, const void *x, double alpha, int32_t dtype, 
 pmg_status pmg_vector_xpay(void *y, const void *x, double alpha, int32_t dtype, int64_t n, void *stream);
 pmg_status pmg_vector_pointwise_mult(void *z, const void *d, const void *r, int32_t dtype, int64_t n,
                                      void *stream);
+/* One Chebyshev step of PreconditionChebyshev (deal.II), fused: out = cur + f1 (cur - prev) +
+ * f2 inv_diag .* (src - Ax), prev == NULL meaning zero; out may alias prev. */
+pmg_status pmg_vector_chebyshev_step(void *out, const void *cur, const void *prev, const void *src,
+                                     const void *Ax, const void *inv_diag, double f1, double f2, int32_t dtype,
+                                     int64_t n, void *stream);
 /* dst (dt_dst) = src (dt_src), n entries, converting between FP64 and FP32. */
 pmg_status pmg_vector_copy(void *dst, int32_t dt_dst, const void *src, int32_t dt_src, int64_t n,
                            void *stream);

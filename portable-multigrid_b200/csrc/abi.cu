@@ -104,6 +104,14 @@ pmg_status pmg_mesh_n_cells(const pmg_mesh *mesh, int64_t *n) {
   });
 }
 
+pmg_status pmg_mesh_cell_coordinates(const pmg_mesh *mesh, int32_t *xyz) {
+  return guarded(__func__, [&] {
+    NEED(mesh);
+    NEED(xyz);
+    std::memcpy(xyz, mesh->m.cell_xyz.data(), mesh->m.cell_xyz.size() * sizeof(int32_t));
+  });
+}
+
 // ---------------------------------------------------------------------------------------
 pmg_status pmg_operator_create(const pmg_mesh *mesh, const pmg_operator_params *params,
                                pmg_operator **op) {
@@ -624,6 +632,21 @@ pmg_status pmg_vector_pointwise_mult(void *z, const void *d, const void *r, int3
     PMG_REQUIRE(dtype == PMG_F64 || dtype == PMG_F32, "bad dtype");
     PMG_REQUIRE(n >= 0, "n must be >= 0");
     if (n > 0) pmg::vec::jacobi(z, d, r, dtype, n, as_stream(stream));
+  });
+}
+
+pmg_status pmg_vector_chebyshev_step(void *out, const void *cur, const void *prev, const void *src,
+                                     const void *Ax, const void *inv_diag, double f1, double f2, int32_t dtype,
+                                     int64_t n, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(out);
+    NEED(cur);
+    NEED(src);
+    NEED(Ax);
+    NEED(inv_diag);
+    PMG_REQUIRE(dtype == PMG_F64 || dtype == PMG_F32, "bad dtype");
+    PMG_REQUIRE(n >= 0, "n must be >= 0");
+    if (n > 0) pmg::vec::cheb_update_into(out, cur, prev, src, Ax, inv_diag, f1, f2, dtype, n, as_stream(stream));
   });
 }
 

@@ -154,6 +154,8 @@ def _declare(L):
         "pmg_mesh_create_box": ([P(Box), P(vp)], i32),
         "pmg_mesh_destroy": ([vp], i32),
         "pmg_mesh_n_cells": ([vp, P(i64)], i32),
+        "pmg_mesh_cell_coordinates": ([vp, vp], i32),
+        "pmg_vector_chebyshev_step": ([vp, vp, vp, vp, vp, vp, d, d, i32, i64, vp], i32),
         "pmg_operator_create": ([vp, P(OperatorParams), P(vp)], i32),
         "pmg_operator_destroy": ([vp], i32),
         "pmg_operator_create_from_maps": ([P(OperatorMaps), P(OperatorParams), P(vp)], i32),
@@ -267,6 +269,13 @@ def vector_pointwise_mult(z, d, r):
     check(lib().pmg_vector_pointwise_mult(_ptr(z), _ptr(d), _ptr(r), _dt(z), z.numel(), _stream()))
 
 
+def vector_chebyshev_step(out, cur, prev, src, Ax, inv_diag, f1, f2):
+    """out = cur + f1 (cur - prev) + f2 inv_diag .* (src - Ax); prev None means zero."""
+    check(lib().pmg_vector_chebyshev_step(_ptr(out), _ptr(cur), None if prev is None else _ptr(prev), _ptr(src),
+                                          _ptr(Ax), _ptr(inv_diag), float(f1), float(f2), _dt(out), out.numel(),
+                                          _stream()))
+
+
 def profile_enable(on=True):
     check(lib().pmg_profile_enable(int(on)))
 
@@ -301,6 +310,12 @@ class Mesh:
         n = C.c_int64()
         check(lib().pmg_mesh_n_cells(self.h, C.byref(n)))
         return n.value
+
+    def cell_coordinates(self):
+        """Integer cell coordinates (x, y, z) in cell order, int32 [n_cells, 3] (host)."""
+        out = np.zeros((self.n_cells(), 3), dtype=np.int32)
+        check(lib().pmg_mesh_cell_coordinates(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -1,14 +1,18 @@
-"""Operators and CG sharded over GPUs: a z-slab partition of a box mesh, one rank per GPU.
+"""Operators, multigrid and CG sharded over GPUs: a z-slab partition of a box mesh, one rank
+per GPU.
 
 The reference distributes the cells over MPI ranks and, in every vmult, updates the ghost
 DoFs of the source vector before the cell loop and adds the ghost contributions of the
 destination back to their owners after it (LaplaceOperatorBK3::vmult,
 include/operators/portable_laplace_operator_bk3.h:187-227, with the partitioner of deal.II's
-MatrixFree); CG reduces its dot products over all ranks.  Here:
+MatrixFree); its transfers exchange the ghosts of the vector they read and compress the one
+they write (include/multigrid/portable_geometric_transfer_core.h:23-157), and CG and the
+Chebyshev eigenvalue estimate reduce their dot products over all ranks.  Here:
 
 * `SlabPartition` gives rank r the coarse cells with z in [z_r, z_{r+1}) of the box and all
   their refinements: a box of its own (the interface faces are not Dirichlet faces), so every
-  multigrid level and the geometry of the deformed map are partitioned the same way.
+  multigrid level and the geometry of the deformed map are partitioned the same way and the
+  patch of an h-transfer never leaves a rank.
 * `LocalNumbering` renumbers a rank's DoFs so that the interface planes are contiguous: the
   bottom plane (shared with rank r-1, owned here) first, the top plane (owned by rank r+1,
   ghosts here) last, each ordered by lattice (y, x) with its free DoFs before its Dirichlet
@@ -18,18 +22,25 @@ MatrixFree); CG reduces its dot products over all ranks.  Here:
 * `DistributedOperator` applies A with the ghost update (rank r+1 sends its bottom plane to
   rank r) and the compress (rank r sends the free entries of its top plane to r+1, which adds
   them to its bottom plane), point to point over torch.distributed (NCCL on GPUs, gloo on
-  CPUs); `dot` is one FP64 all-reduce.  `cg_solve` is the Jacobi-preconditioned CG of
-  deal.II's SolverCG with ReductionControl on top of it.
+  CPUs); `dot` is one FP64 all-reduce.
+* `DistributedTransfer` uses the patch maps of each rank's cells with weights 1 / (patches
+  holding the fine DoF over all ranks), `DistributedChebyshev` is deal.II's
+  PreconditionChebyshev with global dot products in its eigenvalue estimate (start vector
+  (g mod 11) - mean with g the DoF's global node-lattice index, independent of the
+  partition), `DistributedMultigrid` the V-cycle of the single-GPU library over them, and
+  `cg_solve` deal.II's SolverCG with ReductionControl, Jacobi- or V-cycle-preconditioned.
 
 The local compute goes through a backend: `LibraryBackend` (this library's CUDA kernels, the
-local operator built from the renumbered maps with pmg_operator_create_from_maps) on GPUs.
-Every rank takes the same collective steps in the same order."""
+rank's operator built from its renumbered maps with pmg_operator_create_from_maps, transfers
+with pmg_transfer_create_from_maps) on GPUs.  Every rank takes the same collective steps in
+the same order."""
 from __future__ import annotations
 
 import numpy as np
 
-from . import (F32, F64, GEOMETRY_FULL, Box, LaplaceOperator, Mesh, vector_axpy, vector_copy, vector_dot,
-               vector_pointwise_mult, vector_xpay)
+from . import (F32, F64, GEOMETRY_FULL, TRANSFER_GEOMETRIC, TRANSFER_POLYNOMIAL, Box, LaplaceOperator, Mesh,
+               Transfer, vector_axpy, vector_chebyshev_step, vector_copy, vector_dot, vector_pointwise_mult,
+               vector_xpay)
 
 INVALID = 0xFFFFFFFF
 
@@ -68,14 +79,21 @@ class SlabPartition:
         r = self.box.refine if refine is None else refine
         return degree * (self.z_begin << r)
 
+    def global_lattice(self, degree, refine=None):
+        """Node-lattice extents (x, y, z) of the whole box at this degree and refinement."""
+        r = self.box.refine if refine is None else refine
+        return tuple(degree * (c << r) + 1 for c in self.box.coarse)
+
 
 class LocalNumbering:
-    """The caller-side renumbering of one rank's DoFs (see the module docstring).
+    """The renumbering of one rank's DoFs (see the module docstring).
 
     dof_indices [C, nm^3] (sentinel on constrained DoFs), constrained [N] flags and lattice [N, 3]
-    describe the rank's box operator; `perm[old] = new`."""
+    (node-lattice coordinates) describe the rank's box operator, cell_xyz [C, 3] its cells;
+    `perm[old] = new`.  `plain` is the renumbered cell -> DoF map without the sentinel and
+    `node` the local node lattice -> renumbered DoF."""
 
-    def __init__(self, dof_indices, constrained, lattice, part: SlabPartition):
+    def __init__(self, dof_indices, constrained, lattice, part: SlabPartition, cell_xyz=None, degree=None):
         cons = np.asarray(constrained).astype(bool)
         lat = np.asarray(lattice)
         n = cons.shape[0]
@@ -106,22 +124,57 @@ class LocalNumbering:
         self.dof_indices = np.where(idx == INVALID, np.uint32(INVALID),
                                     self.perm[np.minimum(idx, max(n - 1, 0))]).astype(np.uint32)
         self.constrained = self.perm[np.nonzero(cons)[0]].astype(np.uint32)
+        self.constrained_flags = np.zeros(n, bool)
+        self.constrained_flags[self.constrained] = True
         self.lattice = np.empty_like(lat)
         self.lattice[self.perm] = lat
+        if cell_xyz is not None:
+            p, nm = degree, degree + 1
+            extent = lat.max(axis=0) + 1 if n else np.zeros(3, np.int64)
+            self.node = np.zeros((extent[2], extent[1], extent[0]), np.uint32)
+            self.node[self.lattice[:, 2], self.lattice[:, 1], self.lattice[:, 0]] = np.arange(n, dtype=np.uint32)
+            xyz = np.asarray(cell_xyz, dtype=np.int64)
+            k, j, i = np.meshgrid(np.arange(nm), np.arange(nm), np.arange(nm), indexing="ij")
+            self.cell_xyz = xyz
+            self.plain = self.node[p * xyz[:, 2, None] + k.reshape(1, -1), p * xyz[:, 1, None] + j.reshape(1, -1),
+                                   p * xyz[:, 0, None] + i.reshape(1, -1)]
+
+    def global_index(self, part: SlabPartition, degree, refine=None):
+        """Global lexicographic node-lattice index (x fastest) of every local DoF."""
+        Lx, Ly, _ = part.global_lattice(degree, refine)
+        zoff = part.z_offset(degree, refine)
+        lat = self.lattice.astype(np.int64)
+        return lat[:, 0] + Lx * (lat[:, 1] + Ly * (lat[:, 2] + zoff))
+
+
+def transfer_maps(coarse: LocalNumbering, fine: LocalNumbering, degree_c, degree_f, h_transfer):
+    """The patch maps of one rank's transfer in the renumbered numberings: one patch per cell
+    (polynomial) or per coarse cell with the (2p+1)^3 fine nodes of its children (geometric)."""
+    if not h_transfer:
+        return TRANSFER_POLYNOMIAL, coarse.dof_indices, fine.plain
+    p, nf = degree_c, 2 * degree_c + 1
+    k, j, i = np.meshgrid(np.arange(nf), np.arange(nf), np.arange(nf), indexing="ij")
+    xyz = coarse.cell_xyz
+    fi = fine.node[2 * p * xyz[:, 2, None] + k.reshape(1, -1), 2 * p * xyz[:, 1, None] + j.reshape(1, -1),
+                   2 * p * xyz[:, 0, None] + i.reshape(1, -1)]
+    return TRANSFER_GEOMETRIC, coarse.dof_indices, fi
 
 
 class LibraryBackend:
     """Local compute on this rank's GPU through libpmg_b200: the local operator from the
     renumbered maps, vectors as CUDA tensors, the library's vector kernels."""
 
-    def __init__(self, part: SlabPartition, degree: int, dtype=F64, device=0):
+    def __init__(self, part: SlabPartition, degree: int, dtype=F64, device=0, refine=None):
         import torch
         self.torch = torch
         self.device = device
         self.dtype = dtype
+        self.degree = degree
         self.tdtype = torch.float64 if dtype == F64 else torch.float32
-        box_op = LaplaceOperator(Mesh(part.local_box()), degree, dtype, GEOMETRY_FULL, device=device)
-        self.numbering = LocalNumbering(box_op.dof_indices(), box_op.constrained(), box_op.dof_lattice(), part)
+        mesh = Mesh(part.local_box(refine))
+        box_op = LaplaceOperator(mesh, degree, dtype, GEOMETRY_FULL, device=device)
+        self.numbering = LocalNumbering(box_op.dof_indices(), box_op.constrained(), box_op.dof_lattice(), part,
+                                        mesh.cell_coordinates(), degree)
         geometry = box_op.geometry()
         del box_op
         nb = self.numbering
@@ -133,6 +186,12 @@ class LibraryBackend:
 
     def zeros(self, n):
         return self.torch.zeros(n, dtype=self.tdtype, device=f"cuda:{self.device}")
+
+    def from_host(self, a):
+        return self.torch.as_tensor(np.asarray(a), dtype=self.tdtype).to(f"cuda:{self.device}")
+
+    def to_host(self, v):
+        return v.double().cpu().numpy()
 
     def vmult(self, dst, src):
         self.op.vmult(dst, src)
@@ -156,9 +215,18 @@ class LibraryBackend:
     def copy(self, dst, src):
         vector_copy(dst, src)
 
+    def zero(self, v):
+        v.zero_()
+
     def reciprocal(self, v):
         """v = 1 / v in place (setup only)."""
         v.reciprocal_()
+
+    def cheb_step(self, out, cur, prev, src, Ax, invd, f1, f2):
+        vector_chebyshev_step(out, cur, prev, src, Ax, invd, f1, f2)
+
+    def transfer(self, coarse_backend, kind, coarse_indices, fine_indices, weights):
+        return Transfer.from_maps(coarse_backend.op, self.op, kind, coarse_indices, fine_indices, weights)
 
 
 class DistributedOperator:
@@ -176,6 +244,8 @@ class DistributedOperator:
 
     # -- halo exchange: every rank posts its sends and receives, then waits for all --------
     def _exchange(self, sends, recvs):
+        if not (self.dist.is_available() and self.dist.is_initialized()):
+            return
         ops = [self.dist.P2POp(self.dist.isend, t, peer) for t, peer in sends]
         ops += [self.dist.P2POp(self.dist.irecv, t, peer) for t, peer in recvs]
         if ops:
@@ -188,6 +258,10 @@ class DistributedOperator:
         sends = [(v[:nb.n_bottom], r - 1)] if self.part.has_below else []
         recvs = [(v[nb.top_begin:], r + 1)] if self.part.has_above else []
         self._exchange(sends, recvs)
+
+    def zero_ghosts(self, v):
+        if self.nb.n_top:
+            self.be.zero(v[self.nb.top_begin:])
 
     def compress(self, v):
         """Adds the free entries of v's top plane (ghost contributions) to the owner's bottom
@@ -205,14 +279,17 @@ class DistributedOperator:
         self.be.vmult(dst, src)
         self.compress(dst)
 
+    def allreduce(self, values):
+        import torch
+        dev = "cpu" if getattr(self.be, "device", None) is None else f"cuda:{self.be.device}"
+        t = torch.tensor(values, dtype=torch.float64, device=dev)
+        if self.dist.is_available() and self.dist.is_initialized() and self.dist.get_world_size() > 1:
+            self.dist.all_reduce(t)
+        return [float(v) for v in t.cpu()]
+
     def dot(self, a, b):
         """Global a.b over the owned DoFs of every rank (one FP64 all-reduce)."""
-        import torch
-        local = self.be.dot(a, b, self.n_owned)
-        t = torch.tensor([local], dtype=torch.float64, device=a.device)
-        if self.dist.is_initialized() and self.dist.get_world_size() > 1:
-            self.dist.all_reduce(t)
-        return float(t.item())
+        return self.allreduce([self.be.dot(a, b, self.n_owned)])[0]
 
     def inverse_diagonal(self):
         """1 / diag(A) on the owned DoFs (local diagonals summed across the interface), 1 on
@@ -227,13 +304,210 @@ class DistributedOperator:
         return self._inv_diag
 
 
-def cg_solve(A: DistributedOperator, x, b, reduce=1e-9, abs_tol=1e-16, max_iterations=100):
-    """Jacobi-preconditioned CG on the distributed operator (deal.II SolverCG with
-    ReductionControl(max_iterations, abs_tol, reduce), as the library's pmg_cg_solve): stops at
-    the first iterate with ||r|| <= max(abs_tol, reduce ||r_0||).  x and b are this rank's
-    local vectors (owned DoFs first, ghosts last); b's ghost entries are not read."""
+class DistributedTransfer:
+    """prolongate_and_add / restrict_and_add between two partitioned levels: the ghosts of the
+    vector read are updated first, the entries written on ghost DoFs are compressed to their
+    owners afterwards.  Weights 1 / (patches holding the fine DoF on all ranks), 0 on Dirichlet
+    DoFs."""
+
+    def __init__(self, coarse: DistributedOperator, fine: DistributedOperator, degree_c, degree_f, h_transfer):
+        self.coarse, self.fine = coarse, fine
+        kind, ci, fi = transfer_maps(coarse.nb, fine.nb, degree_c, degree_f, h_transfer)
+        be = fine.be
+        counts = be.from_host(np.bincount(np.asarray(fi, np.int64).reshape(-1), minlength=fine.n).astype(np.float64))
+        fine.compress(counts)
+        fine.update_ghosts(counts)
+        mult = be.to_host(counts)
+        w_dof = np.where(fine.nb.constrained_flags | (mult == 0), 0.0, 1.0 / np.maximum(mult, 1.0))
+        self.local = fine.be.transfer(coarse.be, kind, ci, fi, w_dof[np.asarray(fi, np.int64)])
+
+    def prolongate_and_add(self, dst_fine, src_coarse):
+        self.coarse.update_ghosts(src_coarse)
+        self.fine.zero_ghosts(dst_fine)
+        self.local.prolongate_and_add(dst_fine, src_coarse)
+        self.fine.compress(dst_fine)
+
+    def restrict_and_add(self, dst_coarse, src_fine):
+        self.fine.update_ghosts(src_fine)
+        self.coarse.zero_ghosts(dst_coarse)
+        self.local.restrict_and_add(dst_coarse, src_fine)
+        self.coarse.compress(dst_coarse)
+
+
+class DistributedChebyshev:
+    """deal.II PreconditionChebyshev with the inverse diagonal, as the library's smoother
+    (degree <= 0: chosen from smoothing_range), on a DistributedOperator."""
+
+    def __init__(self, A: DistributedOperator, global_index, n_global, degree=5, smoothing_range=15.0,
+                 eig_cg_n_iterations=10):
+        self.A, self.be = A, A.be
+        self.requested_degree, self.degree = degree, degree
+        self.range, self.eig_its = smoothing_range, eig_cg_n_iterations
+        self.gidx, self.n_global = np.asarray(global_index, np.int64), int(n_global)
+        self.estimated = False
+        n = A.n
+        self.Ax, self.x1, self.x2, self.zero_v = self.be.empty(n), self.be.empty(n), self.be.empty(n), self.be.zeros(n)
+
+    def estimate(self):
+        """At most eig_cg_n_iterations CG steps (tolerance 1e-10) from x = 0 on
+        v = (g mod 11) - mean with the Jacobi preconditioner; Lanczos matrix with deal.II's
+        one-step lag; max scaled by 1.2."""
+        A, be, n = self.A, self.be, self.A.n
+        invd = A.inverse_diagonal()
+        full, rem = divmod(self.n_global, 11)
+        mean = (full * 55.0 + rem * (rem - 1) / 2) / self.n_global if self.n_global else 0.0
+        r = be.from_host((self.gidx % 11).astype(np.float64) - mean)
+        x, z, p, v = be.zeros(n), be.empty(n), be.empty(n), be.empty(n)
+        res = np.sqrt(A.dot(r, r))
+        diag, offd, it = [], [], 0
+        if not res <= 1e-10 and self.eig_its > 0:
+            be.mult(z, invd, r)
+            rho = A.dot(r, z)
+            rho_old, alpha, beta, eig_beta_alpha = rho, 0.0, 0.0, 0.0
+            while True:
+                it += 1
+                if it > 1:
+                    beta = rho / rho_old
+                    be.xpay(p, beta, z)
+                else:
+                    be.copy(p, z)
+                A.vmult(v, p)
+                prev_alpha = alpha
+                alpha = rho / A.dot(p, v)
+                be.axpy(x, alpha, p)
+                be.axpy(r, -alpha, v)
+                res = np.sqrt(A.dot(r, r))
+                rho_old = rho
+                be.mult(z, invd, r)
+                rho = A.dot(r, z)
+                if it > 1:
+                    diag.append(1.0 / prev_alpha + eig_beta_alpha)
+                    eig_beta_alpha = beta / prev_alpha
+                    offd.append(np.sqrt(beta) / prev_alpha)
+                if it >= self.eig_its or res <= 1e-10:
+                    break
+        if diag:
+            T = np.diag(diag) + np.diag(offd[:-1], 1) + np.diag(offd[:-1], -1)
+            ev = np.linalg.eigvalsh(T)
+            self.min_ev, self.max_ev = float(ev[0]), 1.2 * float(ev[-1])
+        else:
+            self.min_ev = self.max_ev = 1.0
+        alpha_ev = self.max_ev / self.range if self.range > 1.0 else min(0.9 * self.max_ev, self.min_ev)
+        if self.requested_degree <= 0:
+            actual = self.max_ev / alpha_ev
+            sigma = (1.0 - np.sqrt(1.0 / actual)) / (1.0 + np.sqrt(1.0 / actual))
+            eps = self.range
+            self.degree = 1 + int(np.log(1.0 / eps + np.sqrt(1.0 / eps / eps - 1.0)) / np.log(1.0 / sigma))
+        self.delta = (self.max_ev - alpha_ev) * 0.5
+        self.theta = (self.max_ev + alpha_ev) * 0.5
+        self.cg_its = it
+        self.estimated = True
+
+    def apply(self, dst, src, from_zero):
+        """vmult (from zero, degree-1 products) or step (from dst, degree products)."""
+        if not self.estimated:
+            self.estimate()
+        A, be = self.A, self.be
+        invd = A.inverse_diagonal()
+        more = not (self.degree < 2 or abs(self.delta) < 1e-40)
+        d = self.degree if more else 1
+        if from_zero:
+            be.cheb_step(dst, self.zero_v, None, src, self.zero_v, invd, 0.0, 1.0 / self.theta)
+            cur, prev = dst, None
+        else:
+            A.vmult(self.Ax, dst)
+            be.copy(self.x2, dst)
+            be.cheb_step(self.x1, self.x2, None, src, self.Ax, invd, 0.0, 1.0 / self.theta)
+            cur, prev = self.x1, self.x2
+        if more:
+            rhok, sigma = self.delta / self.theta, self.theta / self.delta
+            spare = self.x1 if cur is dst else dst
+            for _ in range(1, d):
+                A.vmult(self.Ax, cur)
+                rhokp = 1.0 / (2.0 * sigma - rhok)
+                f1, f2 = rhokp * rhok, 2.0 * rhokp / self.delta
+                rhok = rhokp
+                out = prev if prev is not None else spare
+                be.cheb_step(out, cur, prev, src, self.Ax, invd, f1, f2)
+                prev, cur = cur, out
+        if cur is not dst:
+            be.copy(dst, cur)
+
+
+class DistributedMultigrid:
+    """The library's V-cycle (pre-smoothing from zero, residual, restriction, coarser cycle,
+    prolongation, post-smoothing; the level-0 Chebyshev as the coarse solve) over partitioned
+    levels; levels[0] is the coarsest."""
+
+    def __init__(self, levels, transfers, smoothers):
+        self.levels, self.transfers, self.smoothers = levels, transfers, smoothers
+        self.sol = [lv.be.zeros(lv.n) for lv in levels]
+        self.defect = [lv.be.zeros(lv.n) for lv in levels]
+        self.t = [lv.be.zeros(lv.n) for lv in levels]
+
+    def estimate(self):
+        for s in self.smoothers:
+            if not s.estimated:
+                s.estimate()
+
+    def _cycle(self, l):
+        if l == 0:
+            self.smoothers[0].apply(self.sol[0], self.defect[0], True)
+            return
+        lv, be = self.levels[l], self.levels[l].be
+        self.smoothers[l].apply(self.sol[l], self.defect[l], True)
+        lv.vmult(self.t[l], self.sol[l])
+        be.xpay(self.t[l], -1.0, self.defect[l])  # t = defect - A sol
+        self.levels[l - 1].be.zero(self.defect[l - 1])
+        self.transfers[l].restrict_and_add(self.defect[l - 1], self.t[l])
+        self._cycle(l - 1)
+        self.transfers[l].prolongate_and_add(self.sol[l], self.sol[l - 1])
+        self.smoothers[l].apply(self.sol[l], self.defect[l], False)
+
+    def vmult(self, dst, src):
+        """dst = V-cycle(src), converting precisions on entry and exit."""
+        self.estimate()
+        top = len(self.levels) - 1
+        be = self.levels[top].be
+        for l in range(top):
+            self.levels[l].be.zero(self.defect[l])
+        be.copy(self.defect[top], src)
+        self._cycle(top)
+        be.copy(dst, self.sol[top])
+
+
+def build_hierarchy(part: SlabPartition, pseq, backend_factory, cheb_degree=5, smoothing_range=15.0,
+                    eig_iterations=10, h_degree=1):
+    """The multigrid hierarchy of pmg.Hierarchy on a partition: FE_Q(h_degree) on every
+    refinement 0..box.refine, then the degrees of pseq (descending, ending in h_degree) on the
+    finest mesh.  backend_factory(part, degree, refine) makes a level's local backend.
+    Returns the DistributedMultigrid and the level operators."""
+    R = part.box.refine
+    specs = [(r, h_degree) for r in range(R + 1)] + [(R, p) for p in list(reversed(pseq))[1:]]
+    levels, transfers, smoothers = [], [None], []
+    for l, (r, p) in enumerate(specs):
+        op = DistributedOperator(part, backend_factory(part, p, r))
+        levels.append(op)
+        gidx = op.nb.global_index(part, p, r)
+        Lx, Ly, Lz = part.global_lattice(p, r)
+        n_global = Lx * Ly * Lz
+        if l == 0:
+            smoothers.append(DistributedChebyshev(op, gidx, n_global, 0, 1e-3, n_global))
+        else:
+            smoothers.append(DistributedChebyshev(op, gidx, n_global, cheb_degree, smoothing_range, eig_iterations))
+            rc, pc = specs[l - 1]
+            transfers.append(DistributedTransfer(levels[l - 1], op, pc, p, h_transfer=rc != r))
+    return DistributedMultigrid(levels, transfers, smoothers), levels
+
+
+def cg_solve(A: DistributedOperator, x, b, reduce=1e-9, abs_tol=1e-16, max_iterations=100, precond=None):
+    """CG on the distributed operator (deal.II SolverCG with ReductionControl(max_iterations,
+    abs_tol, reduce), as the library's pmg_cg_solve), preconditioned by the Jacobi diagonal or
+    a DistributedMultigrid: stops at the first iterate with ||r|| <= max(abs_tol, reduce
+    ||r_0||).  x and b are this rank's local vectors (owned DoFs first, ghosts last); b's ghost
+    entries are not read."""
     be, n = A.be, A.n
-    invd = A.inverse_diagonal()
+    invd = A.inverse_diagonal() if precond is None else None
     r, z, p, v = be.empty(n), be.empty(n), be.empty(n), be.empty(n)
     A.vmult(v, x)
     be.copy(r, b)
@@ -243,7 +517,10 @@ def cg_solve(A: DistributedOperator, x, b, reduce=1e-9, abs_tol=1e-16, max_itera
     tol = max(abs_tol, reduce * res)
     it, rho_old = 0, 0.0
     while res > tol and it < max_iterations:
-        be.mult(z, invd, r)
+        if precond is None:
+            be.mult(z, invd, r)
+        else:
+            precond.vmult(z, r)
         rho = A.dot(r, z)
         if it == 0:
             be.copy(p, z)

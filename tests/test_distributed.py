@@ -39,19 +39,68 @@ def _obox(O, b):
                       amp=b.amp, dirichlet_mask=b.dirichlet_mask)
 
 
+class NumpyTransfer:
+    """A patch transfer with explicit weights in numpy (test infrastructure)."""
+
+    def __init__(self, M, ci, fi, w):
+        self.M = M  # [nc][nf]
+        nc, nf = M.shape
+        self.ci = np.asarray(ci, np.int64).reshape(-1, nc ** 3)
+        self.fi = np.asarray(fi, np.int64).reshape(-1, nf ** 3)
+        self.w = np.asarray(w, np.float64).reshape(self.fi.shape)
+        self.valid = self.ci != 0xFFFFFFFF
+
+    def prolongate_and_add(self, dst, src):
+        nc, nf = self.M.shape
+        s = src.numpy()
+        c = np.where(self.valid, s[np.where(self.valid, self.ci, 0)], 0.0).reshape(-1, nc, nc, nc)
+        f = np.einsum("pkji,ia,jb,kc->pcba", c, self.M, self.M, self.M).reshape(-1, nf ** 3)
+        d = dst.numpy()
+        np.add.at(d, self.fi.reshape(-1), (self.w * f).reshape(-1))
+
+    def restrict_and_add(self, dst, src):
+        nc, nf = self.M.shape
+        f = (self.w * src.numpy()[self.fi]).reshape(-1, nf, nf, nf)
+        c = np.einsum("pcba,ia,jb,kc->pkji", f, self.M, self.M, self.M).reshape(-1, nc ** 3)
+        d = dst.numpy()
+        np.add.at(d, self.ci[self.valid], c[self.valid])
+
+
 class OracleBackend:
     """Local compute of one rank on the CPU oracle (test infrastructure)."""
 
-    def __init__(self, part, p, O):
+    device = None
+
+    def __init__(self, part, p, O, refine=None):
         from pmg.distributed import LocalNumbering
-        ob = _obox(O, part.local_box())
+        ob = _obox(O, part.local_box(refine))
         plain, cons, idx = O.dofs(ob, p)
         ijk, _ = O.dof_lattice(ob, p)
-        self.numbering = nb = LocalNumbering(idx, cons, ijk, part)
+        cx, cy, cz = O.cell_coords(ob)
+        self.numbering = nb = LocalNumbering(idx, cons, ijk, part, np.stack([cx, cy, cz], axis=1), p)
         self.O, self.p = O, p
         self.G = O.geometry_G(ob, p)
         self.cons = np.zeros(nb.n, np.uint8)
         self.cons[nb.constrained] = 1
+
+    def from_host(self, a):
+        return torch.tensor(np.asarray(a, np.float64))
+
+    def to_host(self, v):
+        return v.numpy().copy()
+
+    def zero(self, v):
+        v.zero_()
+
+    def cheb_step(self, out, cur, prev, src, Ax, invd, f1, f2):
+        pv = torch.zeros_like(cur) if prev is None else prev
+        out.copy_(cur + f1 * (cur - pv) + f2 * invd * (src - Ax))
+
+    def transfer(self, coarse_backend, kind, ci, fi, weights):
+        import pmg
+        pc, pf = coarse_backend.p, self.p
+        M = self.O.projection_matrix(pc, pf) if kind == pmg.TRANSFER_POLYNOMIAL else self.O.h_prolongation_matrix(pc)
+        return NumpyTransfer(M, ci, fi, weights)
 
     def empty(self, n):
         return torch.empty(n, dtype=torch.float64)
@@ -199,3 +248,85 @@ def test_partition_boxes_tile_the_global_box():
     assert parts[1].z_offset(3) == 3 * (2 << 1)
     with pytest.raises(ValueError):
         SlabPartition(pmg.Box.make(coarse=(1, 1, 2)), 3, 0)
+
+
+MG_CASES = {
+    # name: (coarse cells per direction, refine, pseq, Chebyshev degree)
+    "q2_phmg": (2, 2, [2, 1], 3),
+    "q3_phmg": (3, 1, [3, 1], 4),
+}
+
+
+def _mg_worker(rank, world, port, q, case):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    for p in (ROOT, os.path.join(ROOT, "portable-multigrid_b200")):
+        sys.path.insert(0, p)
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        import pmg
+        from pmg.distributed import DistributedOperator, SlabPartition, build_hierarchy, cg_solve
+        from oracle import oracle as O
+        c, r, pseq, cheb = MG_CASES[case]
+        gbox = _global_box(pmg, c, r)
+        part = SlabPartition(gbox, world, rank)
+        mg, levels = build_hierarchy(part, pseq, lambda pt, p, rr: OracleBackend(pt, p, O, rr), cheb_degree=cheb)
+        p = pseq[0]
+        A = DistributedOperator(part, OracleBackend(part, p, O))
+        nb = A.nb
+        _, glat = O.dof_lattice(_obox(O, gbox), p)
+        gid = glat[nb.lattice[:, 2] + part.z_offset(p), nb.lattice[:, 1], nb.lattice[:, 0]].astype(np.int64)
+        plain_g, cons_g, _ = O.dofs(_obox(O, gbox), p)
+        b_g = O.rhs(_obox(O, gbox), p, p + 1, 0, plain_g, cons_g)
+        x = torch.zeros(nb.n, dtype=torch.float64)
+        info = cg_solve(A, x, torch.from_numpy(b_g[gid].copy()), reduce=1e-10, max_iterations=100, precond=mg)
+        evs = [(s.min_ev, s.max_ev, s.degree) for s in mg.smoothers]
+        q.put((rank, gid[:nb.n_owned], x[:nb.n_owned].numpy(), info, evs))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _run_mg(case, world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mg_worker, args=(k, world, port, q, case)) for k in range(world)]
+    for pr in procs:
+        pr.start()
+    got = sorted([q.get(timeout=600) for _ in procs], key=lambda t: t[0])
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    return got
+
+
+@pytest.mark.parametrize("case,world", [("q2_phmg", 2), ("q3_phmg", 3)])
+def test_slab_partitioned_vcycle_cg_equals_one_rank(oracle, case, world):
+    """The V-cycle-preconditioned CG on 2 / 3 ranks takes the iterations of the same solver on
+    one rank and gives its solution to 1e-10; the smoothers' eigenvalue estimates agree to
+    1e-10; the one-rank solve is within one iteration of the oracle's single-domain solver."""
+    import pmg
+    c, r, pseq, cheb = MG_CASES[case]
+    one = _run_mg(case, 1)
+    many = _run_mg(case, world)
+    gbox = _obox(oracle, _global_box(pmg, c, r))
+    n = oracle.dofs(gbox, pseq[0])[1].shape[0]
+    xs = []
+    for got in (one, many):
+        x = np.zeros(n)
+        owned = np.concatenate([g[1] for g in got])
+        assert np.array_equal(np.sort(owned), np.arange(n))
+        for g in got:
+            x[g[1]] = g[2]
+            assert g[3]["converged"]
+        xs.append(x)
+    its1 = one[0][3]["iterations"]
+    assert all(g[3]["iterations"] == its1 for g in many)
+    assert np.abs(xs[1] - xs[0]).max() <= 1e-10 * np.abs(xs[0]).max()
+    for (mn1, mx1, d1), (mn2, mx2, d2) in zip(one[0][4], many[0][4]):
+        assert d1 == d2 and abs(mx2 / mx1 - 1) < 1e-10 and abs(mn2 / mn1 - 1) < 1e-8
+    info_o, x_o = oracle.solve_box(gbox, pseq, cheb=cheb, reduce=1e-10, want_x=True)
+    assert abs(its1 - info_o.iterations) <= 1
+    assert np.abs(xs[0] - x_o).max() <= 1e-8 * np.abs(x_o).max()
