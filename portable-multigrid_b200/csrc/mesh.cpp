@@ -1,12 +1,11 @@
-// Structured box meshes and the FE_Q(p) DoF numbering on them (host side, setup only).
+// Structured box meshes (host side, setup only) and the FE_DGQ numbering on them.
 //
 // The reference takes its meshes from GridGenerator::subdivided_hyper_rectangle refined
 // globally on a p4est triangulation (tests/poisson_cube_bk3/program.cc:937-957,
 // :263-278) and its numbering from deal.II's DoFHandler.  Here the box is generated
 // directly: coarse cells lexicographically, each refined cell set in Morton order (the
-// order p4est gives globally refined trees), and DoFs numbered in order of first visit
-// along that cell order with each cell's nodes in lexicographic order, so that the DoFs a
-// batch of consecutive cells touches are close together in memory.
+// order p4est gives globally refined trees).  The FE_Q numbering along that order is built on
+// the device (numbering.cu).
 #include <algorithm>
 
 #include "pmg_internal.hpp"
@@ -41,46 +40,6 @@ BoxMesh make_box(const pmg_box &b) {
           m.cell_xyz[3 * c + 2] = (tz << L) + xyz[2];
         }
   return m;
-}
-
-Numbering make_numbering(const BoxMesh &m, int p, bool keep_lattice) {
-  Numbering nb;
-  nb.p = p;
-  const int nm = p + 1, nm3 = nm * nm * nm;
-  for (int d = 0; d < 3; ++d) nb.L[d] = p * m.n[d] + 1;
-  const int64_t n_lat = nb.L[0] * nb.L[1] * nb.L[2];
-  PMG_REQUIRE(n_lat < (int64_t(1) << 32) - 1, "too many DoFs for 32-bit indices");
-  nb.lattice.assign(n_lat, kInvalid);
-  nb.plain.resize(m.n_cells * nm3);
-  std::vector<uint8_t> cons;
-  cons.reserve(n_lat);
-  const int mask = m.box.dirichlet_mask;
-  uint32_t next = 0;
-  for (int64_t c = 0; c < m.n_cells; ++c) {
-    const int64_t bx = int64_t(p) * m.cell_xyz[3 * c], by = int64_t(p) * m.cell_xyz[3 * c + 1],
-                  bz = int64_t(p) * m.cell_xyz[3 * c + 2];
-    uint32_t *out = nb.plain.data() + c * nm3;
-    for (int k = 0; k < nm; ++k)
-      for (int j = 0; j < nm; ++j) {
-        const int64_t row = ((bz + k) * nb.L[1] + (by + j)) * nb.L[0] + bx;
-        for (int i = 0; i < nm; ++i) {
-          uint32_t &slot = nb.lattice[row + i];
-          if (slot == kInvalid) {
-            slot = next++;
-            const int64_t gx = bx + i, gy = by + j, gz = bz + k;
-            const bool on = ((mask & 1) && gx == 0) || ((mask & 2) && gx == nb.L[0] - 1) ||
-                            ((mask & 4) && gy == 0) || ((mask & 8) && gy == nb.L[1] - 1) ||
-                            ((mask & 16) && gz == 0) || ((mask & 32) && gz == nb.L[2] - 1);
-            cons.push_back(on ? 1 : 0);
-          }
-          out[(k * nm + j) * nm + i] = slot;
-        }
-      }
-  }
-  nb.n_dofs = next;
-  nb.constrained = std::move(cons);
-  if (!keep_lattice) std::vector<uint32_t>().swap(nb.lattice);
-  return nb;
 }
 
 // FE_DGQ(p): every cell owns its (p+1)^3 DoFs, numbered cell by cell in lexicographic order

@@ -1,8 +1,9 @@
 // DoF numbering, index maps and transfer maps built on the device (setup).
 //
-// The numbering is the one make_numbering (mesh.cpp) produces on the host: cells in the box's
-// order (coarse cells lexicographically, Morton order inside each), the nodes of a cell in
-// lexicographic order, every node numbered when it is first visited.  In parallel: node X's
+// The numbering visits the cells in the box's order (coarse cells lexicographically, Morton
+// order inside each) and the nodes of a cell in lexicographic order, and numbers every node
+// when it is first visited, so that the DoFs a batch of consecutive cells touches are close
+// together in memory.  In parallel: node X's
 // number is the rank of (first cell containing X, X's local index in that cell) among all
 // nodes, so with cnt[c] = the nodes first visited by cell c, an exclusive scan of cnt gives
 // each cell the first number of its new nodes, and the cell numbers them in local order.

@@ -158,7 +158,6 @@ struct Numbering {
 };
 
 BoxMesh make_box(const pmg_box &b);
-Numbering make_numbering(const BoxMesh &m, int p, bool keep_lattice);
 Numbering make_numbering_dg(const BoxMesh &m, int p); // dof = cell * (p+1)^3 + l
 
 } // namespace pmg
