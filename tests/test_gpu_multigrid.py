@@ -209,3 +209,18 @@ def test_plain_q2_h_multigrid_converges_at_rate_three():
         errs.append(h.fine64.l2_error(x, 1))
     rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
     assert all(2.85 < r < 3.15 for r in rates), rates
+
+
+def test_plain_q6_kappa_h_multigrid_matches_oracle(oracle):
+    """The plain method on the variable-coefficient Q6 problem: FE_Q(6) on every level (3^3 and
+    6^3 cells, kappa = 1 + 0.9 sin(2 pi x) sin(2 pi y) sin(2 pi z)), the (2p+1)-node h-transfer
+    at p = 6, Chebyshev(4), FP64 throughout: the oracle's iterations and solution."""
+    box = pmg.Box.make(coarse=(3, 3, 3), refine=1)
+    ob = oracle.Box.make(coarse=(3, 3, 3), refine=1)
+    info_o, x_o = oracle.solve_box(ob, [6], cheb=4, coeff_kind=1, reduce=1e-10, want_x=True, h_degree=6)
+    h = pmg.Hierarchy(box, [6], mg_dtype=pmg.F64, cheb_degree=4, h_degree=6, geometry=pmg.GEOMETRY_AFFINE,
+                      coeff_kind=pmg.COEFF_KAPPA)
+    x, info = h.solve(h.fine64.assemble_rhs(0), reduce=1e-10)
+    torch.cuda.synchronize()
+    assert info["converged"] and info["iterations"] == info_o.iterations
+    assert rel_err(x.cpu().numpy(), x_o) < 1e-8
