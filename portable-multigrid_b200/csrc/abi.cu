@@ -452,7 +452,8 @@ pmg_status pmg_chebyshev_create(pmg_operator *op, const pmg_chebyshev_params *pa
 
 pmg_status pmg_chebyshev_destroy(pmg_chebyshev *c) {
   if (c) {
-    if (c->op) cudaSetDevice(c->op->device);
+    // the operator is borrowed and may already be destroyed: use the recorded device
+    cudaSetDevice(c->device);
     delete c;
   }
   return PMG_OK;
@@ -517,7 +518,7 @@ pmg_status pmg_mg_create(int32_t n_levels, pmg_operator *const *levels,
 
 pmg_status pmg_mg_destroy(pmg_mg *mg) {
   if (mg) {
-    if (!mg->levels.empty()) cudaSetDevice(mg->levels.back()->device);
+    cudaSetDevice(mg->device); // the levels are borrowed and may already be destroyed
     delete mg;
   }
   return PMG_OK;

@@ -54,6 +54,7 @@ void chebyshev_setup(pmg_chebyshev &c, pmg_operator &op, const pmg_chebyshev_par
   PMG_REQUIRE(prm.smoothing_range > 0, "smoothing_range must be positive");
   PMG_REQUIRE(prm.eig_cg_n_iterations >= 0, "eig_cg_n_iterations must be >= 0");
   c.op = &op;
+  c.device = op.device;
   c.degree = prm.degree;
   c.requested_degree = prm.degree;
   c.range = prm.smoothing_range;
@@ -202,7 +203,8 @@ void mg_setup(pmg_mg &mg, int n_levels, pmg_operator *const *levels, pmg_transfe
                   "transfer does not connect consecutive levels");
     }
   }
-  PMG_CUDA(cudaSetDevice(mg.levels.back()->device));
+  mg.device = mg.levels.back()->device;
+  PMG_CUDA(cudaSetDevice(mg.device));
   mg.sol.resize(n_levels);
   mg.def.resize(n_levels);
   mg.t.resize(n_levels);

@@ -6,7 +6,8 @@
 #include "pmg_internal.hpp"
 
 struct pmg_chebyshev {
-  pmg_operator *op = nullptr;
+  pmg_operator *op = nullptr; // borrowed: may be gone when the smoother is destroyed
+  int device = 0;             // the operator's device, kept for the destructor
   int degree = 0;
   int requested_degree = 0; // <= 0: the degree is chosen by every eigenvalue estimate
   int generation = 0;       // incremented by every eigenvalue estimate
@@ -20,6 +21,7 @@ struct pmg_chebyshev {
 };
 
 struct pmg_mg {
+  int device = 0; // the finest level's device, kept for the destructor (the levels are borrowed)
   std::vector<pmg_operator *> levels;
   std::vector<pmg_transfer *> transfers;
   std::vector<pmg_chebyshev *> smoothers;

@@ -91,10 +91,13 @@ def test_vmult_multi_group_matches_oracle(problems, case, dtype):
 
 
 @pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
-@pytest.mark.parametrize("kind,p_c,p_f,refine", [("p", 2, 4, 5), ("p", 3, 6, 4), ("h", 1, 1, 6), ("h", 2, 2, 6)])
-def test_transfer_multi_patch_matches_oracle(oracle, kind, p_c, p_f, refine, dtype):
-    """p-transfers on the 32^3 / 16^3 fine mesh (one patch per fine cell) and h-transfers onto
-    the 64^3 fine mesh (one patch per coarse 32^3 cell)."""
+@pytest.mark.parametrize("kind,p_c,p_f,refine,multi", [("p", 2, 4, 5, True), ("p", 3, 6, 4, False),
+                                                       ("h", 1, 1, 6, True), ("h", 2, 2, 6, True)])
+def test_transfer_multi_patch_matches_oracle(oracle, kind, p_c, p_f, refine, multi, dtype):
+    """p-transfers on the 32^3 mesh (one patch per cell) and h-transfers onto the 64^3 fine
+    mesh (one patch per coarse 32^3 cell), every warp taking two or more patches; Q3 -> Q6 on
+    16^3 cells (fewer patches than resident warps: the oracle's Q6 levels at 32^3 take minutes)
+    for parity only."""
     fine = pmg.Box.make(refine=refine)
     ob = obox(oracle, fine)
     if kind == "p":
@@ -114,13 +117,15 @@ def test_transfer_multi_patch_matches_oracle(oracle, kind, p_c, p_f, refine, dty
     d = torch.tensor(base_f, dtype=td, device="cuda")
     t.prolongate_and_add(d, torch.tensor(xc, dtype=td, device="cuda"))
     torch.cuda.synchronize()
-    assert_multi_unit(t.last_launch())
+    if multi:
+        assert_multi_unit(t.last_launch())
     assert rel_err(d.double().cpu().numpy(), ref) < tol
     ref = oracle.transfer_apply(ob, p_c, p_f, 1, xf, base_c.copy())
     d = torch.tensor(base_c, dtype=td, device="cuda")
     t.restrict_and_add(d, torch.tensor(xf, dtype=td, device="cuda"))
     torch.cuda.synchronize()
-    assert_multi_unit(t.last_launch())
+    if multi:
+        assert_multi_unit(t.last_launch())
     assert rel_err(d.double().cpu().numpy(), ref) < tol
 
 
