@@ -271,3 +271,30 @@ def test_invjac_coefficient_values_and_update_match_g(degree):
             out.append(d.cpu().numpy())
         torch.cuda.synchronize()
         assert rel_err(out[1], out[0]) < 1e-12
+
+
+@pytest.mark.parametrize("mask", [0x00, 0x13])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+def test_subdomain_operator_with_neumann_faces(oracle, mask, dtype):
+    """The operator of a subdomain with Neumann faces (the SubdomainLaplaceOperator the
+    reference's BNN preconditioner solves with, include/domain_decomposition/
+    portable_bnn_preconditioner.h:146-277): the same cell kernel on a box whose faces outside
+    dirichlet_mask carry no constraints.  Matches the oracle; a floating subdomain (no
+    Dirichlet face) maps the constant vector to zero."""
+    box = pmg.Box.make(coarse=(2, 1, 1), refine=1, hi=(2.0, 1.0, 1.0), deform=1, dirichlet_mask=mask)
+    ob = obox(oracle, box)
+    op = pmg.LaplaceOperator(pmg.Mesh(box), 3, dtype)
+    plain, cons, idx = oracle.dofs(ob, 3)
+    assert int(cons.sum()) == int(op.constrained().sum()) and (mask != 0 or cons.sum() == 0)
+    src = random_src(op.m(), 21)
+    ref = oracle.vmult(3, idx, oracle.geometry_G(ob, 3), cons, src)
+    d = op.initialize_dof_vector()
+    op.vmult(d, torch.tensor(src, dtype=tdtype(dtype), device="cuda"))
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype]
+    if mask == 0:
+        one = torch.ones(op.m(), dtype=tdtype(dtype), device="cuda")
+        op.vmult(d, one)
+        torch.cuda.synchronize()
+        scale = float(np.abs(ref).max())
+        assert float(d.abs().max()) < (1e-12 if dtype == pmg.F64 else 1e-5) * scale
