@@ -358,9 +358,13 @@ def time_to_solution(torch, pmg, dev, refine=4, repeats=3):
     # fp32_mg / fp64_mg: the ph-multigrid with an FP32 / FP64 V-cycle; fp64_plain_hmg: the
     # all-FP64 plain method (geometric multigrid at degree 6 on every level 48^3 .. 3^3,
     # GeometricTransfer<dim, fe_degree> as in source/geometric_multigrid/program.cc:245-249)
-    for name, dt, pseq, hdeg in (("fp32_mg", pmg.F32, [6, 3, 2, 1], 1), ("fp64_mg", pmg.F64, [6, 3, 2, 1], 1),
-                                 ("fp64_plain_hmg", pmg.F64, [6], 6)):
-        h = pmg.Hierarchy(box, pseq, mg_dtype=dt, cheb_degree=4, h_degree=hdeg,
+    # fp32_mg_tf32 / fp32_mg_3xtf32: the FP32 V-cycle with its affine levels on the tensor cores
+    for name, dt, pseq, hdeg, tc in (("fp32_mg", pmg.F32, [6, 3, 2, 1], 1, 0),
+                                     ("fp32_mg_tf32", pmg.F32, [6, 3, 2, 1], 1, 1),
+                                     ("fp32_mg_3xtf32", pmg.F32, [6, 3, 2, 1], 1, 3),
+                                     ("fp64_mg", pmg.F64, [6, 3, 2, 1], 1, 0),
+                                     ("fp64_plain_hmg", pmg.F64, [6], 6, 0)):
+        h = pmg.Hierarchy(box, pseq, mg_dtype=dt, cheb_degree=4, h_degree=hdeg, tensor_cores=tc,
                           geometry=pmg.GEOMETRY_AFFINE, coeff_kind=pmg.COEFF_KAPPA, device=dev)
         b = h.fine64.assemble_rhs(0)
         h.estimate()
@@ -404,9 +408,13 @@ def q6_kernel_rates(torch, pmg, dev, peaks, refine=4, launches=20):
     N = 7
     flops = mesh.n_cells() * (24 * N ** 4 + 6 * N ** 3)
     res = {"algorithmic_flops_per_launch": flops}
-    for name, dt, tdt, peak_key in (("fp32", pmg.F32, torch.float32, "fp32_fma_tflops"),
-                                    ("fp64", pmg.F64, torch.float64, "fp64_fma_tflops")):
+    for name, dt, tdt, peak_key, tc in (("fp32", pmg.F32, torch.float32, "fp32_fma_tflops", 0),
+                                        ("fp32_tf32", pmg.F32, torch.float32, "fp32_fma_tflops", 1),
+                                        ("fp32_3xtf32", pmg.F32, torch.float32, "fp32_fma_tflops", 3),
+                                        ("fp64", pmg.F64, torch.float64, "fp64_fma_tflops", 0)):
         op = pmg.LaplaceOperator(mesh, 6, dt, pmg.GEOMETRY_AFFINE, pmg.COEFF_KAPPA, device=dev)
+        if tc:
+            op.set_tensor_cores(tc)
         src = torch.rand(op.m(), dtype=tdt, device=f"cuda:{dev}")
         dst = torch.empty_like(src)
         for _ in range(3):

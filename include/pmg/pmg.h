@@ -208,6 +208,14 @@ pmg_status pmg_operator_copy_dof_indices(const pmg_operator *op, uint32_t *host)
 pmg_status pmg_operator_copy_constrained(const pmg_operator *op, uint8_t *host);
 pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host);
 
+/* The tensor-core variant of the cell kernel for FP32 operators with affine geometry (the
+ * BF16/TF32 contraction variant; the reference contracts on CUDA cores only): mode 1 applies
+ * the twelve 1D contractions of every cell as TF32 mma.sync products (10-bit mantissas, FP32
+ * accumulation, about 1e-3 relative), mode 3 as three TF32 products per contraction (hi*hi +
+ * hi*lo + lo*hi, about FP32 accuracy), mode 0 returns to the CUDA-core kernel.  PMG_EINVAL for
+ * FP64, DG, mass or non-affine operators. */
+pmg_status pmg_operator_set_tensor_cores(pmg_operator *op, int32_t mode);
+
 /* Node-lattice coordinates (i, j, k) of every DoF of a continuous operator on a box mesh,
  * host array ijk[N][3] (x fastest in the lattice of degree * cells + 1 points per direction):
  * the support points a partitioned mesh matches across ranks (the ghost DoFs of

@@ -289,6 +289,19 @@ pmg_status pmg_operator_copy_geometry(const pmg_operator *op, double *host) {
   });
 }
 
+pmg_status pmg_operator_set_tensor_cores(pmg_operator *op, int32_t mode) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    PMG_REQUIRE(mode == 0 || mode == 1 || mode == 3, "mode must be 0, 1 or 3");
+    if (mode != 0) {
+      PMG_REQUIRE(op->dtype == PMG_F32, "the tensor-core cell kernel is an FP32 (TF32) kernel");
+      PMG_REQUIRE(op->kind == PMG_OP_LAPLACE && op->geometry == PMG_GEOMETRY_AFFINE && !op->dg,
+                  "the tensor-core cell kernel needs the continuous Laplace operator with affine geometry");
+    }
+    op->tensor_cores = mode;
+  });
+}
+
 pmg_status pmg_operator_dof_lattice(const pmg_operator *op, int32_t *ijk) {
   return guarded(__func__, [&] {
     NEED(op);

@@ -8,6 +8,7 @@
 #include "fields.hpp"
 #include "vector_ops.hpp"
 #include "numbering.hpp"
+#include "vmult_tc.hpp"
 #include "pmg_internal.hpp"
 
 namespace pmg {
@@ -656,7 +657,8 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
     op.launch_units[PMG_KERNEL_VMULT_CELL] = op.n_groups;
     {
       prof::Scope scope("vmult_cell", s);
-      vmult_fn(op.degree)(L);
+      if (op.tensor_cores) vmult_cells_tensor_cores(op, src, dst, s);
+      else vmult_fn(op.degree)(L);
     }
     if (op.dg) {
       prof::Scope scope("vmult_dg_faces", s);

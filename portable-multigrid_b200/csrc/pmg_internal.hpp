@@ -176,6 +176,7 @@ struct DGHost;
 struct pmg_operator {
   int device = 0;
   bool from_maps = false;           // built from a caller's index map and geometry (no mesh)
+  int tensor_cores = 0;             // cell kernel: 0 CUDA cores, 1 TF32 mma, 3 three TF32 products
   int kind = PMG_OP_LAPLACE;        // PMG_OP_LAPLACE, PMG_OP_DG_SIPG or PMG_OP_MASS
   std::shared_ptr<pmg::DGHost> dg;  // face data of a DG operator
   int degree = 1, nm = 2, nq = 2;

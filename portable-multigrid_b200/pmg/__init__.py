@@ -206,6 +206,7 @@ def _declare(L):
         "pmg_vector_xpay": ([vp, vp, d, i32, i64, vp], i32),
         "pmg_vector_pointwise_mult": ([vp, vp, vp, i32, i64, vp], i32),
         "pmg_operator_dof_lattice": ([vp, vp], i32),
+        "pmg_operator_set_tensor_cores": ([vp, i32], i32),
         "pmg_profile_enable": ([i32], i32),
         "pmg_profile_reset": ([], i32),
         "pmg_profile_query": ([C.c_char_p, P(d), P(i64)], i32),
@@ -439,6 +440,10 @@ class LaplaceOperator:
         check(lib().pmg_operator_copy_dof_indices(self.h, out.ctypes.data_as(C.c_void_p)))
         return out.reshape(-1, nm3)
 
+    def set_tensor_cores(self, mode):
+        """Cell kernel of an FP32 affine operator: 0 CUDA cores, 1 TF32 mma, 3 three TF32 products."""
+        check(lib().pmg_operator_set_tensor_cores(self.h, int(mode)))
+
     def dof_lattice(self):
         """Node-lattice coordinates (i, j, k) of every DoF, int32 [m, 3] (host)."""
         out = np.zeros((self.m(), 3), dtype=np.int32)
@@ -647,7 +652,7 @@ class Hierarchy:
 
     def __init__(self, box: Box, pseq, mg_dtype=F32, cheb_degree=5, geometry=GEOMETRY_AUTO,
                  coeff_kind=COEFF_NONE, coeff_qp=None, device=0, smoothing_range=15.0,
-                 eig_iterations=10, coarse_dtype=None, dg=False, penalty=0.0, h_degree=1):
+                 eig_iterations=10, coarse_dtype=None, dg=False, penalty=0.0, h_degree=1, tensor_cores=0):
         if pseq[-1] != h_degree or list(pseq) != sorted(pseq, reverse=True):
             raise ValueError("pseq must be descending and end in h_degree")
         self.box = box
@@ -666,6 +671,11 @@ class Hierarchy:
             # coarser levels carry the finest level's field, interpolated level by level
             for l in range(len(self.levels) - 2, -1, -1):
                 self.levels[l].interpolate_coefficient(self.levels[l + 1])
+        if tensor_cores:
+            # the FP32 affine levels apply their cells on the tensor cores
+            for op in self.levels:
+                if op.dtype == F32 and geometry != GEOMETRY_FULL and not box.deform:
+                    op.set_tensor_cores(tensor_cores)
         if dg:
             self.levels.append(DGLaplaceOperator(self.meshes[-1], pseq[0], mg_dtype, penalty, device))
         for l in range(1, len(self.levels)):

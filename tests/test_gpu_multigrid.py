@@ -224,3 +224,20 @@ def test_plain_q6_kappa_h_multigrid_matches_oracle(oracle):
     torch.cuda.synchronize()
     assert info["converged"] and info["iterations"] == info_o.iterations
     assert rel_err(x.cpu().numpy(), x_o) < 1e-8
+
+
+@pytest.mark.parametrize("mode", [1, 3])
+def test_variable_kappa_q6_phmg_with_tensor_core_levels(oracle, mode):
+    """The FP32 V-cycle with its affine levels on the tensor cores (TF32 or three TF32
+    products) inside FP64 CG: converges to 1e-10 within one iteration of the oracle's count and
+    gives its solution to 1e-8."""
+    box = pmg.Box.make(coarse=(3, 3, 3), refine=1)
+    ob = oracle.Box.make(coarse=(3, 3, 3), refine=1)
+    info_o, x_o = oracle.solve_box(ob, [6, 3, 2, 1], cheb=4, coeff_kind=1, reduce=1e-10, want_x=True)
+    h = pmg.Hierarchy(box, [6, 3, 2, 1], mg_dtype=pmg.F32, cheb_degree=4, geometry=pmg.GEOMETRY_AFFINE,
+                      coeff_kind=pmg.COEFF_KAPPA, tensor_cores=mode)
+    x, info = h.solve(h.fine64.assemble_rhs(0), reduce=1e-10)
+    torch.cuda.synchronize()
+    assert info["converged"]
+    assert abs(info["iterations"] - info_o.iterations) <= 1
+    assert rel_err(x.cpu().numpy(), x_o) < 1e-8

@@ -298,3 +298,53 @@ def test_subdomain_operator_with_neumann_faces(oracle, mask, dtype):
         torch.cuda.synchronize()
         scale = float(np.abs(ref).max())
         assert float(d.abs().max()) < (1e-12 if dtype == pmg.F64 else 1e-5) * scale
+
+
+# the tensor-core cell kernel: TF32 products (mode 1, 10-bit mantissas) and three TF32 products
+# (mode 3, about FP32 accuracy), against the FP64 oracle
+TC_TOL = {1: 5e-3, 3: 2e-5}
+
+
+@pytest.mark.parametrize("mode", [1, 3])
+@pytest.mark.parametrize("degree", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("coeff", [pmg.COEFF_NONE, pmg.COEFF_KAPPA])
+def test_tensor_core_vmult_matches_oracle(oracle, mode, degree, coeff):
+    box = pmg.Box.make(coarse=(3, 2, 2), refine=1, hi=(3.0, 2.0, 2.0))
+    ob = obox(oracle, box)
+    op = pmg.LaplaceOperator(pmg.Mesh(box), degree, pmg.F32, pmg.GEOMETRY_AFFINE, coeff)
+    op.set_tensor_cores(mode)
+    plain, cons, idx = oracle.dofs(ob, degree)
+    src = random_src(op.m(), 5)
+    ref = oracle.vmult(degree, idx, oracle.geometry_G(ob, degree, coeff_kind=coeff), cons, src)
+    d = op.initialize_dof_vector()
+    op.vmult(d, torch.tensor(src, dtype=torch.float32, device="cuda"))
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), ref) < TC_TOL[mode]
+
+
+@pytest.mark.parametrize("mode", [1, 3])
+def test_tensor_core_vmult_many_cells_per_warp(oracle, mode):
+    """Q6 with kappa on 24^3 cells (the config-3 fine level at a smaller size): every warp
+    applies several cells."""
+    box = pmg.Box.make(coarse=(3, 3, 3), refine=3)
+    ob = obox(oracle, box)
+    op = pmg.LaplaceOperator(pmg.Mesh(box), 6, pmg.F32, pmg.GEOMETRY_AFFINE, pmg.COEFF_KAPPA)
+    op.set_tensor_cores(mode)
+    plain, cons, idx = oracle.dofs(ob, 6)
+    src = random_src(op.m(), 6)
+    ref = oracle.vmult(6, idx, oracle.geometry_G(ob, 6, coeff_kind=pmg.COEFF_KAPPA), cons, src)
+    d = op.initialize_dof_vector()
+    op.vmult(d, torch.tensor(src, dtype=torch.float32, device="cuda"))
+    torch.cuda.synchronize()
+    units, par = op.last_launch()
+    assert units >= 2 * par
+    assert rel_err(d.double().cpu().numpy(), ref) < TC_TOL[mode]
+
+
+def test_tensor_core_mode_rejected_where_not_built():
+    op = pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(refine=1, deform=1)), 2, pmg.F32, pmg.GEOMETRY_FULL)
+    with pytest.raises(pmg.PmgError):
+        op.set_tensor_cores(1)
+    op64 = pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(refine=1)), 2, pmg.F64, pmg.GEOMETRY_AFFINE)
+    with pytest.raises(pmg.PmgError):
+        op64.set_tensor_cores(3)
