@@ -4,18 +4,23 @@
 // source/plain_laplace_solver_dg/program.cc:128-217).
 //
 // The cell stiffness term comes from the continuous slab kernel run on the discontinuous
-// numbering (dof = cell * N^3 + l).  This file adds the face terms with one fused kernel:
-// a block takes a batch of cells, and for each of the six faces of each cell it forms its
-// own trace (the node layer on the face and the reference normal derivative) and the
-// neighbour's trace, recomputed from the neighbour's DoFs straight from L2.  The reference
-// instead writes every trace to global face buffers and reads them back in three more
-// launches.  Each face is evaluated from both sides; every cell writes only its own DoFs,
-// so there are no atomics and no face buffers.
+// numbering (dof = cell * N^3 + l).  This file adds the face terms with one fused kernel.
+// Where the box is refined at least twice (every 64 consecutive cells form a 4x4x4 cube) a
+// block takes such a tile into shared memory and evaluates each face between two of its
+// cells once, for both cells; the faces on the tile surface take the neighbour's trace from
+// L2.  Elsewhere a block takes a batch of cells, and for each of the six faces of each cell
+// it forms its own trace (the node layer on the face and the reference normal derivative)
+// and the neighbour's trace, recomputed from the neighbour's DoFs straight from L2, so each
+// face is evaluated from both sides.  The reference instead writes every trace to global
+// face buffers and reads them back in three more launches.  In both forms every block
+// writes only its own cells' DoFs: no global atomics and no face buffers.
 //
 // On GLL nodes with the (p+1)-point Gauss face rule the face integrals of products of
 // basis functions are exact, so the face quadrature is applied as the 1D GLL mass matrix
 // M1 = S diag(w) S^T in each tangential direction.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cstdlib>
 #include <vector>
 
@@ -338,11 +343,183 @@ template <typename T> __global__ void add_kernel(T *__restrict__ dst, const doub
     dst[i] += (T)src[i];
 }
 
-// PMG_DG_FACE=0 selects the face-by-face kernel (a comparison switch)
+// ---- each face once: 4x4x4 tiles of cells ----
+// With the box refined at least twice, every 64 consecutive cells (Morton order inside a
+// coarse cell) form a 4x4x4 cube.  A block loads such a tile into shared memory (one
+// coalesced read), evaluates every face between two tile cells once (144 faces: the flux
+// from the lower cell's side, its face mass, then the value and normal-derivative tests of
+// both cells, the upper cell's with the signs of its own outward normal) and every face on
+// the tile's surface from the inside (96 faces: the neighbour's normal line from global
+// memory, or the Dirichlet mirror), accumulates the test contributions in shared memory
+// (atomic adds: a node collects from up to six faces) and adds the tile to dst in one
+// coalesced pass.  The faces of the tile surface are still met from both sides.
+constexpr int kTileFaces = 240; // 3 x 48 inside, 6 x 16 on the surface
+constexpr int kTileThreads = 256;
+template <int N, typename T> constexpr size_t dg_tile_smem() {
+  return sizeof(T) * (size_t(64) * N * N * N + size_t(4) * kTileFaces * N * N);
+}
+
+__device__ __forceinline__ int tile_index(int x, int y, int z) {
+  return (x & 1) | ((y & 1) << 1) | ((z & 1) << 2) | ((x >> 1) << 3) | ((y >> 1) << 4) | ((z >> 1) << 5);
+}
+
+// face fi of a tile: direction d, the tile cell on the face's lower side (lo) and upper side
+// (up, -1 outside the tile), the face of the inside cell that lies on the tile surface (F,
+// -1 for a face inside the tile)
+__device__ __forceinline__ void tile_face(int fi, int &d, int &lo, int &up, int &F, int &in) {
+  int c[3];
+  if (fi < 144) {
+    d = fi / 48;
+    const int w = fi - 48 * d, along = w >> 4, tan = w & 15;
+    const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+    c[d] = along;
+    c[ta] = tan & 3;
+    c[tb] = tan >> 2;
+    lo = tile_index(c[0], c[1], c[2]);
+    c[d] = along + 1;
+    up = tile_index(c[0], c[1], c[2]);
+    F = -1;
+    in = lo;
+  } else {
+    const int e = fi - 144;
+    F = e >> 4;
+    d = F >> 1;
+    const int tan = e & 15, ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+    c[d] = (F & 1) ? 3 : 0;
+    c[ta] = tan & 3;
+    c[tb] = tan >> 2;
+    in = tile_index(c[0], c[1], c[2]);
+    lo = up = -1;
+  }
+}
+
+template <int N, typename T>
+__global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid_constant__ DGTab<N, T> tab,
+                                                                    const __grid_constant__ DGGeo geo,
+                                                                    const T *__restrict__ src, T *__restrict__ dst,
+                                                                    const int32_t *__restrict__ nbr, int64_t n_tiles) {
+  constexpr int N2 = N * N, N3 = N2 * N, NP = kTileFaces * N2;
+  extern __shared__ __align__(16) unsigned char dg_tile_raw[];
+  T *U = reinterpret_cast<T *>(dg_tile_raw); // the tile's values, then its output
+  T *F1 = U + 64 * N3, *F2 = F1 + NP, *G1 = F2 + NP, *G2 = G1 + NP;
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t base = tile * 64;
+    const T *ts = src + base * N3;
+    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) U[e] = ts[e];
+    __syncthreads();
+    // 1. fluxes f1 = sigma [u] - {d_n u}, f2 = -[u]/2 at every face point, times the face area
+    for (int t = threadIdx.x; t < NP; t += kTileThreads) {
+      const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
+      int d, lo, up, F, in;
+      tile_face(fi, d, lo, up, F, in);
+      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+      const T h = (T)geo.h[d], area = (T)(geo.h[ta] * geo.h[tb]), sigma = (T)(geo.c_pen / geo.h[d]);
+      T f1 = T(0), f2 = T(0);
+      if (F < 0) { // inside: the lower cell's view, outward normal +d
+        T vo = T(0), vn = T(0), dn = T(0), dnn = T(0);
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          const int l = face_node<N>(d, i, a, bb);
+          dn += tab.dphi1[i] * U[lo * N3 + l];
+          dnn += tab.dphi0[i] * U[up * N3 + l];
+        }
+        vo = U[lo * N3 + face_node<N>(d, N - 1, a, bb)];
+        vn = U[up * N3 + face_node<N>(d, 0, a, bb)];
+        const T jump = vo - vn;
+        f1 = sigma * jump - T(0.5) * (dn + dnn) / h;
+        f2 = T(-0.5) * jump;
+      } else { // on the tile surface: the inside cell's view
+        const int sd = F & 1;
+        const T sgn_h = (sd ? T(1) : T(-1)) / h;
+        const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
+        const T *dphi_nb = sd ? tab.dphi0 : tab.dphi1;
+        T dn = T(0);
+#pragma unroll
+        for (int i = 0; i < N; ++i) dn += dphi_own[i] * U[in * N3 + face_node<N>(d, i, a, bb)];
+        dn *= sgn_h;
+        const T vo = U[in * N3 + face_node<N>(d, sd ? N - 1 : 0, a, bb)];
+        const int32_t nb = __ldg(nbr + (base + in) * 6 + F);
+        if (nb >= 0) {
+          const T *un = src + int64_t(nb) * N3;
+          T dnn = T(0);
+#pragma unroll
+          for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * __ldg(un + face_node<N>(d, i, a, bb));
+          dnn *= sgn_h;
+          const T jump = vo - __ldg(un + face_node<N>(d, sd ? 0 : N - 1, a, bb));
+          f1 = sigma * jump - T(0.5) * (dn + dnn);
+          f2 = T(-0.5) * jump;
+        } else if ((geo.dirichlet >> F) & 1) { // mirror: u+ = -u-, d_n u+ = d_n u-
+          f1 = sigma * T(2) * vo - dn;
+          f2 = -vo;
+        }
+      }
+      F1[t] = f1 * area;
+      F2[t] = f2 * area;
+    }
+    __syncthreads();
+    // 2. face mass along a; the tile array becomes the output accumulator
+    for (int t = threadIdx.x; t < NP; t += kTileThreads) {
+      const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
+      const T *f1 = F1 + fi * N2 + bb * N, *f2 = F2 + fi * N2 + bb * N;
+      T g1 = T(0), g2 = T(0);
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        g1 += tab.M1[a * N + k] * f1[k];
+        g2 += tab.M1[a * N + k] * f2[k];
+      }
+      G1[t] = g1;
+      G2[t] = g2;
+    }
+    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) U[e] = T(0);
+    __syncthreads();
+    // 3. face mass along b, then the value and normal-derivative tests of the face's cells
+    for (int t = threadIdx.x; t < NP; t += kTileThreads) {
+      const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
+      int d, lo, up, F, in;
+      tile_face(fi, d, lo, up, F, in);
+      const T *g1 = G1 + fi * N2 + a, *g2 = G2 + fi * N2 + a;
+      T tv = T(0), tn = T(0);
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        tv += tab.M1[bb * N + k] * g1[k * N];
+        tn += tab.M1[bb * N + k] * g2[k * N];
+      }
+      const T h = (T)geo.h[d];
+      if (F < 0) {
+        // lower cell: outward normal +d; upper cell: -tv on its layer 0, the same derivative
+        // coefficient against its own outward normal
+        const T tnh = tn / h;
+        atomicAdd(U + lo * N3 + face_node<N>(d, N - 1, a, bb), tv);
+        atomicAdd(U + up * N3 + face_node<N>(d, 0, a, bb), -tv);
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          const int l = face_node<N>(d, i, a, bb);
+          atomicAdd(U + lo * N3 + l, tnh * tab.dphi1[i]);
+          atomicAdd(U + up * N3 + l, tnh * tab.dphi0[i]);
+        }
+      } else {
+        const int sd = F & 1;
+        const T tnh = tn * (sd ? T(1) : T(-1)) / h;
+        const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
+        atomicAdd(U + in * N3 + face_node<N>(d, sd ? N - 1 : 0, a, bb), tv);
+#pragma unroll
+        for (int i = 0; i < N; ++i) atomicAdd(U + in * N3 + face_node<N>(d, i, a, bb), tnh * dphi_own[i]);
+      }
+    }
+    __syncthreads();
+    // 4. the tile's face terms into dst
+    T *td = dst + base * N3;
+    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) td[e] += U[e];
+    __syncthreads();
+  }
+}
+
+// the face form: 2 (default) the tile kernel where the mesh allows it, else 1; PMG_DG_FACE=1 the
+// cell-batch kernel everywhere, 0 the face-by-face kernel (comparison switches)
 int face_form() {
   static const int v = [] {
     const char *e = std::getenv("PMG_DG_FACE");
-    return (e && e[0] == '0') ? 0 : 1;
+    return (e && e[0] == '0') ? 0 : ((e && e[0] == '1') ? 1 : 2);
   }();
   return v;
 }
@@ -373,7 +550,31 @@ void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, i
     dg_face_diag_kernel<N, T><<<std::max(grid, 1), 256, 0, s>>>(make_dg_tab<N, T>(h), make_geo(h),
                                                                   static_cast<T *>(dst), h.nbr.as<int32_t>(), n_cells);
   } else {
-    if (face_form() == 0) {
+    constexpr size_t tile_smem = dg_tile_smem<N, T>();
+    if (face_form() == 2 && h.tiles64 && n_cells % 64 == 0 && tile_smem <= 200 * 1024) {
+      auto k = dg_face_tile_kernel<N, T>;
+      static std::mutex mu;
+      static std::map<int, int> per_sm; // device -> resident blocks per SM
+      int dev = 0, resident = 1;
+      PMG_CUDA(cudaGetDevice(&dev));
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = per_sm.find(dev);
+        if (it == per_sm.end()) {
+          PMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
+          int nb = 0;
+          PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kTileThreads, tile_smem));
+          it = per_sm.emplace(dev, std::max(1, nb)).first;
+        }
+        resident = it->second;
+      }
+      const int64_t n_tiles = n_cells / 64;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, (int64_t)resident * sms));
+      if (units) *units = n_tiles;
+      if (blocks) *blocks = grid;
+      k<<<grid, kTileThreads, tile_smem, s>>>(make_dg_tab<N, T>(h), make_geo(h), static_cast<const T *>(src),
+                                              static_cast<T *>(dst), h.nbr.as<int32_t>(), n_tiles);
+    } else if (face_form() == 0) {
       constexpr int B = dg_batch_seq<N>();
       const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 16);
       if (units) *units = (n_cells + B - 1) / B;
@@ -432,6 +633,7 @@ void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen) {
   for (int d = 0; d < 3; ++d) h.h[d] = (mesh.box.hi[d] - mesh.box.lo[d]) / double(mesh.n[d]);
   h.c_pen = c_pen > 0 ? c_pen : degree * (degree + 1.0);
   h.dirichlet = mesh.box.dirichlet_mask;
+  h.tiles64 = mesh.box.refine >= 2;
   // neighbour table [cell][2 d + s], -1 on the boundary
   const int64_t C = mesh.n_cells, nx = mesh.n[0], ny = mesh.n[1];
   std::vector<int32_t> lut(C);

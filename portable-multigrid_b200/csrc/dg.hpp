@@ -12,6 +12,7 @@ struct DGHost {
   double h[3] = {0, 0, 0};
   double c_pen = 0;  // sigma = c_pen / h on every face (uniform boxes)
   int dirichlet = 0; // face mask
+  bool tiles64 = false; // every 64 consecutive cells form a 4x4x4 cube (refine >= 2)
   DeviceBuffer nbr;  // int32 [cell][6] neighbour cells, -1 on the boundary
 };
 

@@ -26,7 +26,19 @@ BOXES = {
     "ragged_3x2x1": dict(coarse=(3, 2, 1), refine=1, hi=(3.0, 2.0, 0.5)),
     "neumann_x": dict(coarse=(2, 1, 1), refine=1, hi=(2.0, 1.0, 1.0), dirichlet_mask=0x3C),
     "single_cell": dict(refine=0),
+    # refined twice or more: the face kernel works on 4x4x4 tiles of cells (faces inside a
+    # tile once, faces on its surface from the inside with the neighbour read from memory)
+    "ragged_r2": dict(coarse=(3, 2, 1), refine=2, hi=(3.0, 2.0, 0.5)),
+    "neumann_r2": dict(coarse=(2, 1, 1), refine=2, hi=(2.0, 1.0, 1.0), dirichlet_mask=0x3C),
 }
+
+
+def tile_form(box, p, dtype):
+    """True where the face kernel takes the tile form: the box refined at least twice and
+    the tile (64 cells' values plus four face-point arrays of 240 faces) within 200 KiB."""
+    n = p + 1
+    size = (8 if dtype == pmg.F64 else 4) * (64 * n ** 3 + 4 * 240 * n * n)
+    return box.refine >= 2 and size <= 200 * 1024
 
 
 @pytest.mark.parametrize("p", [1, 2, 3, 4, 6])
@@ -45,6 +57,9 @@ def test_dg_vmult_matches_oracle(oracle, p, dtype, boxname):
         op.vmult(d, torch.tensor(src, dtype=td, device="cuda"))
         torch.cuda.synchronize()
         assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype], c_pen
+        units, _ = op.last_launch(pmg.KERNEL_DG_FACES)
+        n_cells = op.m() // (p + 1) ** 3
+        assert units == (n_cells // 64 if tile_form(box, p, dtype) else -(-n_cells // max(1, 384 // (6 * (p + 1) ** 2))))
 
 
 @pytest.mark.parametrize("p", [1, 3, 5])

@@ -129,19 +129,28 @@ def test_transfer_multi_patch_matches_oracle(oracle, kind, p_c, p_f, refine, mul
     assert rel_err(d.double().cpu().numpy(), ref) < tol
 
 
-@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
-def test_dg_vmult_multi_batch_matches_oracle(oracle, dtype):
-    """DG-SIPG Q3 on 32^3 cells (2,097,152 DoFs): the face kernel loops over cell batches."""
+@pytest.fixture(scope="module")
+def dg_problem(oracle):
+    """DG-SIPG Q3 on 64^3 cells (16,777,216 DoFs, 4096 tiles of 4x4x4 cells) and the
+    oracle's result, shared by both dtypes."""
     p = 3
-    box = pmg.Box.make(refine=5)
-    ob = obox(oracle, box)
+    box = pmg.Box.make(coarse=(2, 2, 2), refine=5)
     c_pen = 2.0 * (p + 1) ** 2
+    ob = obox(oracle, box)
+    src = np.random.default_rng(p).uniform(-1, 1, oracle.dg_n(ob, p))
+    return p, box, c_pen, src, oracle.dg_vmult(ob, p, c_pen, src)
+
+
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+def test_dg_vmult_multi_batch_matches_oracle(dg_problem, dtype):
+    """The face kernel loops over 4x4x4 cell tiles (every block takes two or more), the cell
+    kernel over warp groups."""
+    p, box, c_pen, src, ref = dg_problem
     op = pmg.DGLaplaceOperator(pmg.Mesh(box), p, dtype, c_pen)
-    src = np.random.default_rng(p).uniform(-1, 1, op.m())
     got = apply(op, src, dtype)
     assert_multi_unit(op.last_launch(pmg.KERNEL_DG_FACES))
     assert_multi_unit(op.last_launch(pmg.KERNEL_VMULT_CELL))
-    assert rel_err(got, oracle.dg_vmult(ob, p, c_pen, src)) < TOL[dtype]
+    assert rel_err(got, ref) < TOL[dtype]
 
 
 @pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
