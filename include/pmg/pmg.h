@@ -181,6 +181,20 @@ pmg_status pmg_operator_tvmult(const pmg_operator *op, void *dst, const void *sr
 pmg_status pmg_operator_vmult_dummy(const pmg_operator *op, void *dst, const void *src,
                                     int32_t ghost_exchange_on, int32_t computation_on,
                                     void *stream);
+/* The cells [cell_begin, cell_end) of a continuous Laplace operator added into dst:
+ * dst += A_K src summed over those cells K (in the operator's cell order: the caller's for
+ * operators from maps, the mesh's otherwise).  init != 0 first sets dst as vmult does (zero,
+ * with the identity rows of the constrained DoFs), so that
+ *   vmult_cells(dst, src, 0, c, 1); vmult_cells(dst, src, c, n_cells, 0)
+ * equals vmult(dst, src) up to the order of the floating-point additions.  This is the split
+ * of the reference's colour loop (bk3.h:187-227): the cells that read no ghost DoFs are
+ * computed while the ghost update is in flight, the others after it.  cell_begin and
+ * cell_end are multiples of pmg_operator_cells_per_group (cell_end may also be n_cells);
+ * PMG_EINVAL for DG, mass and tensor-core operators. */
+pmg_status pmg_operator_vmult_cells(const pmg_operator *op, void *dst, const void *src, int64_t cell_begin,
+                                    int64_t cell_end, int32_t init, void *stream);
+/* Cells per warp group of the cell kernel: floor(32 / (degree + 1)). */
+pmg_status pmg_operator_cells_per_group(const pmg_operator *op, int32_t *cells);
 /* compute_diagonal() (bk3.h:533-561): inverse of diag(A), 1 on constrained rows. */
 pmg_status pmg_operator_compute_diagonal(pmg_operator *op, void *stream);
 /* get_matrix_diagonal_inverse() (bk3.h:563-568): device pointer owned by the operator,

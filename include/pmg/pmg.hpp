@@ -115,6 +115,18 @@ public:
     check(pmg_operator_vmult_dummy(op_.get(), dst.get_values(), src.get_values(), ghost_exchange_on,
                                    computation_on, stream_));
   }
+  /* dst += A_K src over the cells [cell_begin, cell_end); init sets dst as vmult does first
+   * (the interior / boundary split of a sharded vmult). */
+  template <typename Vector>
+  void vmult_cells(Vector &dst, const Vector &src, int64_t cell_begin, int64_t cell_end, bool init) const {
+    check(pmg_operator_vmult_cells(op_.get(), dst.get_values(), src.get_values(), cell_begin, cell_end, init,
+                                   stream_));
+  }
+  int cells_per_group() const {
+    int32_t v = 0;
+    check(pmg_operator_cells_per_group(op_.get(), &v));
+    return v;
+  }
   void compute_diagonal() { check(pmg_operator_compute_diagonal(op_.get(), stream_)); }
   /* get_matrix_diagonal_inverse(): copies the inverse diagonal into the caller's vector
    * (the storage behind the DiagonalMatrix the reference returns). */

@@ -194,6 +194,23 @@ pmg_status pmg_operator_vmult_dummy(const pmg_operator *op, void *dst, const voi
   });
 }
 
+pmg_status pmg_operator_vmult_cells(const pmg_operator *op, void *dst, const void *src, int64_t cell_begin,
+                                    int64_t cell_end, int32_t init, void *stream) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    PMG_CUDA(cudaSetDevice(op->device));
+    pmg::operator_vmult_cells(*op, dst, src, cell_begin, cell_end, init != 0, as_stream(stream));
+  });
+}
+
+pmg_status pmg_operator_cells_per_group(const pmg_operator *op, int32_t *cells) {
+  return guarded(__func__, [&] {
+    NEED(op);
+    NEED(cells);
+    *cells = op->cpw;
+  });
+}
+
 pmg_status pmg_operator_compute_diagonal(pmg_operator *op, void *stream) {
   return guarded(__func__, [&] {
     NEED(op);

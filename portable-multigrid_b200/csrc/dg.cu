@@ -350,13 +350,20 @@ template <typename T> __global__ void add_kernel(T *__restrict__ dst, const doub
 // from the lower cell's side, its face mass, then the value and normal-derivative tests of
 // both cells, the upper cell's with the signs of its own outward normal) and every face on
 // the tile's surface from the inside (96 faces: the neighbour's normal line from global
-// memory, or the Dirichlet mirror), accumulates the test contributions in shared memory
-// (atomic adds: a node collects from up to six faces) and adds the tile to dst in one
-// coalesced pass.  The faces of the tile surface are still met from both sides.
+// memory, or the Dirichlet mirror).  Then one thread per tile node sums what its six faces
+// give it, in a fixed order (no atomics, so the result does not depend on scheduling), and
+// adds that to dst in one coalesced pass.  The faces of the tile surface are still met from
+// both sides.
 constexpr int kTileFaces = 240; // 3 x 48 inside, 6 x 16 on the surface
 constexpr int kTileThreads = 256;
+// shared memory of the tile kernel: the face-point arrays F1, F2, then one region that holds
+// the tile's values in phase 1 and the face-point arrays G1, G2 from phase 2 on
+template <int N, typename T> constexpr size_t dg_tile_region() {
+  return size_t(64) * N * N * N > size_t(2) * kTileFaces * N * N ? size_t(64) * N * N * N
+                                                                  : size_t(2) * kTileFaces * N * N;
+}
 template <int N, typename T> constexpr size_t dg_tile_smem() {
-  return sizeof(T) * (size_t(64) * N * N * N + size_t(4) * kTileFaces * N * N);
+  return sizeof(T) * (size_t(2) * kTileFaces * N * N + dg_tile_region<N, T>());
 }
 
 __device__ __forceinline__ int tile_index(int x, int y, int z) {
@@ -400,8 +407,9 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
                                                                     const int32_t *__restrict__ nbr, int64_t n_tiles) {
   constexpr int N2 = N * N, N3 = N2 * N, NP = kTileFaces * N2;
   extern __shared__ __align__(16) unsigned char dg_tile_raw[];
-  T *U = reinterpret_cast<T *>(dg_tile_raw); // the tile's values, then its output
-  T *F1 = U + 64 * N3, *F2 = F1 + NP, *G1 = F2 + NP, *G2 = G1 + NP;
+  T *F1 = reinterpret_cast<T *>(dg_tile_raw), *F2 = F1 + NP;
+  T *U = F2 + NP;                  // the tile's values (phase 1)
+  T *G1 = U, *G2 = G1 + NP;        // over them from phase 2 on
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
     const T *ts = src + base * N3;
@@ -457,7 +465,7 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
       F2[t] = f2 * area;
     }
     __syncthreads();
-    // 2. face mass along a; the tile array becomes the output accumulator
+    // 2. face mass along a
     for (int t = threadIdx.x; t < NP; t += kTileThreads) {
       const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
       const T *f1 = F1 + fi * N2 + bb * N, *f2 = F2 + fi * N2 + bb * N;
@@ -470,13 +478,11 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
       G1[t] = g1;
       G2[t] = g2;
     }
-    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) U[e] = T(0);
     __syncthreads();
-    // 3. face mass along b, then the value and normal-derivative tests of the face's cells
+    // 3. face mass along b: the value-test coefficient (F1) and the normal-derivative-test
+    //    coefficient (F2, divided by h; on the tile surface times the outward normal's sign)
     for (int t = threadIdx.x; t < NP; t += kTileThreads) {
       const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
-      int d, lo, up, F, in;
-      tile_face(fi, d, lo, up, F, in);
       const T *g1 = G1 + fi * N2 + a, *g2 = G2 + fi * N2 + a;
       T tv = T(0), tn = T(0);
 #pragma unroll
@@ -484,32 +490,52 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
         tv += tab.M1[bb * N + k] * g1[k * N];
         tn += tab.M1[bb * N + k] * g2[k * N];
       }
-      const T h = (T)geo.h[d];
-      if (F < 0) {
-        // lower cell: outward normal +d; upper cell: -tv on its layer 0, the same derivative
-        // coefficient against its own outward normal
-        const T tnh = tn / h;
-        atomicAdd(U + lo * N3 + face_node<N>(d, N - 1, a, bb), tv);
-        atomicAdd(U + up * N3 + face_node<N>(d, 0, a, bb), -tv);
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-          const int l = face_node<N>(d, i, a, bb);
-          atomicAdd(U + lo * N3 + l, tnh * tab.dphi1[i]);
-          atomicAdd(U + up * N3 + l, tnh * tab.dphi0[i]);
-        }
+      int d;
+      T sg = T(1);
+      if (fi < 144) {
+        d = fi / 48;
       } else {
-        const int sd = F & 1;
-        const T tnh = tn * (sd ? T(1) : T(-1)) / h;
-        const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
-        atomicAdd(U + in * N3 + face_node<N>(d, sd ? N - 1 : 0, a, bb), tv);
-#pragma unroll
-        for (int i = 0; i < N; ++i) atomicAdd(U + in * N3 + face_node<N>(d, i, a, bb), tnh * dphi_own[i]);
+        const int F = (fi - 144) >> 4;
+        d = F >> 1;
+        sg = (F & 1) ? T(1) : T(-1);
       }
+      F1[t] = tv;
+      F2[t] = tn * sg / (T)geo.h[d];
     }
     __syncthreads();
-    // 4. the tile's face terms into dst
+    // 4. one thread per tile node sums its six faces in a fixed order (deterministic): the
+    //    value test on the face layer (minus for the upper cell of an inside face, whose
+    //    outward normal is opposite to the one the face was evaluated with) and the
+    //    normal-derivative test on every layer, then adds the sum to dst
     T *td = dst + base * N3;
-    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) td[e] += U[e];
+    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) {
+      const int ct = e / N3, l = e - ct * N3;
+      const int cx = (ct & 1) | (((ct >> 3) & 1) << 1), cy = ((ct >> 1) & 1) | (((ct >> 4) & 1) << 1),
+                cz = ((ct >> 2) & 1) | (((ct >> 5) & 1) << 1);
+      const int cc[3] = {cx, cy, cz};
+      const int idx[3] = {l % N, (l / N) % N, l / N2};
+      T v = T(0);
+#pragma unroll
+      for (int F = 0; F < 6; ++F) {
+        const int d = F >> 1, sd = F & 1;
+        const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+        const int tan = cc[ta] + 4 * cc[tb];
+        int fi;
+        T sv = T(1);
+        if (sd && cc[d] < 3) {
+          fi = 48 * d + 16 * cc[d] + tan; // lower cell of an inside face
+        } else if (!sd && cc[d] > 0) {
+          fi = 48 * d + 16 * (cc[d] - 1) + tan; // upper cell of an inside face
+          sv = T(-1);
+        } else {
+          fi = 144 + 16 * F + tan; // on the tile surface
+        }
+        const int pab = fi * N2 + idx[tb] * N + idx[ta];
+        v += F2[pab] * (sd ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]]);
+        if (idx[d] == (sd ? N - 1 : 0)) v += sv * F1[pab];
+      }
+      td[e] += v;
+    }
     __syncthreads();
   }
 }

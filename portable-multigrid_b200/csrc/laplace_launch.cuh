@@ -169,6 +169,21 @@ template <typename T, int GEOM, bool SG, int PIPE> VmultShape vmult_shape() {
   return best;
 }
 
+// L2 policies of vmult_slab_kernel's first read of each index block and of its L2 prefetch
+// of the next group's geometry (0 evict-first, 1 evict-last, 2 evict-normal; packed two bits
+// each); PMG_VMULT_IDX_POLICY and PMG_VMULT_PREFETCH_POLICY override
+inline int idx_policy() {
+  static const int v = [] {
+    auto get = [](const char *name) {
+      const char *e = std::getenv(name);
+      const int o = e ? std::atoi(e) : -1;
+      return (o >= 0 && o <= 2) ? o : 0;
+    };
+    return get("PMG_VMULT_IDX_POLICY") | (get("PMG_VMULT_PREFETCH_POLICY") << 2);
+  }();
+  return v;
+}
+
 template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabLaunch &L) {
   auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
   const VmultShape sh = vmult_shape<T, GEOM, SG, PIPE>();
@@ -181,7 +196,7 @@ template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabL
   const size_t smem = (size_t)sh.wpb * kern::SlabSmem<kN, T, SG, PIPE>::PER_WARP;
   k<<<grid, 32 * sh.wpb, smem, L.stream>>>(
       make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
-      static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err);
+      static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err, idx_policy());
   PMG_LAUNCH_CHECK();
   if (L.launched) *L.launched = (int64_t)grid * sh.wpb;
 }

@@ -624,12 +624,11 @@ void operator_setup(pmg_operator &op, const pmg_mesh &mesh, const pmg_operator_p
   finish_setup(op);
 }
 
-void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s, bool compute) {
-  PMG_REQUIRE(dst && src, "null vector");
-  PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");
+namespace {
+// dst = 0 (bk3.h:134) with the identity rows of copy_constrained_values (bk3.h:230) written
+// in the same pass: the cell kernels never touch constrained entries (index sentinel)
+void vmult_init(const pmg_operator &op, void *dst, const void *src, cudaStream_t s) {
   const size_t bytes = dtype_size(op.dtype) * op.n_dofs;
-  // dst = 0 (bk3.h:134) with the identity rows of copy_constrained_values (bk3.h:230) written
-  // in the same pass: the cell kernels never touch constrained entries (index sentinel)
   if (op.n_constrained > 0) {
     prof::Scope scope("vmult_init", s);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((op.n_dofs + 255) / 256, (int64_t)op.sms * 16));
@@ -643,6 +642,13 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
   } else {
     PMG_CUDA(cudaMemsetAsync(dst, 0, bytes, s));
   }
+}
+} // namespace
+
+void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s, bool compute) {
+  PMG_REQUIRE(dst && src, "null vector");
+  PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");
+  vmult_init(op, dst, src, s);
   if (compute && op.n_cells > 0 && op.kind == PMG_OP_MASS) {
     prof::Scope scope("vmult_mass", s);
     mass_vmult_cells(op, src, dst, s);
@@ -666,6 +672,43 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
                      &op.launch_units[PMG_KERNEL_DG_FACES], &op.launch_par[PMG_KERNEL_DG_FACES]);
     }
   }
+}
+
+// The cells [cell_begin, cell_end) of the operator's cell order added into dst (after
+// vmult_init when init is set): the cell kernel on the warp groups that hold them, with the
+// index map, geometry and coefficient pointers advanced to the first of those groups.
+void operator_vmult_cells(const pmg_operator &op, void *dst, const void *src, int64_t cell_begin,
+                          int64_t cell_end, bool init, cudaStream_t s) {
+  PMG_REQUIRE(dst && src, "null vector");
+  PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");
+  PMG_REQUIRE(op.kind == PMG_OP_LAPLACE && !op.dg, "cell ranges are applied by continuous Laplace operators");
+  PMG_REQUIRE(op.tensor_cores == 0, "cell ranges are applied by the CUDA-core cell kernel");
+  PMG_REQUIRE(0 <= cell_begin && cell_begin <= cell_end && cell_end <= op.n_cells, "cell range out of bounds");
+  PMG_REQUIRE(cell_begin % op.cpw == 0 && (cell_end % op.cpw == 0 || cell_end == op.n_cells),
+              "cell range bounds must be multiples of the cells per warp group (or the cell count)");
+  if (init) vmult_init(op, dst, src, s);
+  const int64_t g0 = cell_begin / op.cpw, g1 = (cell_end + op.cpw - 1) / op.cpw;
+  if (g1 <= g0) return;
+  const int N2 = op.nm * op.nm;
+  const size_t sz = dtype_size(op.dtype);
+  SlabLaunch L = slab_launch(op, cached_tables(op.degree), s);
+  const int gc = geom_code(op);
+  L.idx = op.idx.as<uint32_t>() + g0 * N2 * op.lanes;
+  if (gc == 0 || gc == 3)
+    L.geo = static_cast<const char *>(op.geo.get()) + sz * g0 * N2 * (gc == 3 ? 10 : 6) * op.lanes;
+  else
+    L.geo = static_cast<const char *>(op.geo.get()) + sz * g0 * op.cpw * 8;
+  if (op.coef.get()) L.coef = static_cast<const char *>(op.coef.get()) + sz * g0 * N2 * op.lanes;
+  L.n_groups = g1 - g0;
+  L.src = src;
+  L.dst = dst;
+  L.resident_warps = op.warps_vmult;
+  L.resident_warps_ring = op.warps_vmult_ring;
+  L.err = op.err_flag.as<unsigned int>();
+  L.launched = &op.launch_par[PMG_KERNEL_VMULT_CELL];
+  op.launch_units[PMG_KERNEL_VMULT_CELL] = L.n_groups;
+  prof::Scope scope("vmult_cell", s);
+  vmult_fn(op.degree)(L);
 }
 
 void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s) {

@@ -167,6 +167,8 @@ def _declare(L):
         "pmg_operator_vmult": ([vp, vp, vp, vp], i32),
         "pmg_operator_tvmult": ([vp, vp, vp, vp], i32),
         "pmg_operator_vmult_dummy": ([vp, vp, vp, i32, i32, vp], i32),
+        "pmg_operator_vmult_cells": ([vp, vp, vp, i64, i64, i32, vp], i32),
+        "pmg_operator_cells_per_group": ([vp, P(i32)], i32),
         "pmg_operator_compute_diagonal": ([vp, vp], i32),
         "pmg_operator_get_inverse_diagonal": ([vp, P(vp)], i32),
         "pmg_operator_copy_inverse_diagonal": ([vp, vp, vp], i32),
@@ -404,6 +406,17 @@ class LaplaceOperator:
     def vmult_dummy(self, dst, src, ghost_exchange_on=True, computation_on=True):
         check(lib().pmg_operator_vmult_dummy(self.h, _ptr(dst), _ptr(src), int(ghost_exchange_on),
                                              int(computation_on), _stream()))
+
+    def vmult_cells(self, dst, src, cell_begin, cell_end, init):
+        """dst += A_K src over the cells [cell_begin, cell_end) of the operator's cell order;
+        init first sets dst as vmult does (pmg_operator_vmult_cells)."""
+        check(lib().pmg_operator_vmult_cells(self.h, _ptr(dst), _ptr(src), int(cell_begin), int(cell_end),
+                                             int(bool(init)), _stream()))
+
+    def cells_per_group(self):
+        v = C.c_int32()
+        check(lib().pmg_operator_cells_per_group(self.h, C.byref(v)))
+        return v.value
 
     def compute_diagonal(self):
         check(lib().pmg_operator_compute_diagonal(self.h, _stream()))

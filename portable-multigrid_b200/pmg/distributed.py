@@ -22,7 +22,9 @@ Chebyshev eigenvalue estimate reduce their dot products over all ranks.  Here:
 * `DistributedOperator` applies A with the ghost update (rank r+1 sends its bottom plane to
   rank r) and the compress (rank r sends the free entries of its top plane to r+1, which adds
   them to its bottom plane), point to point over torch.distributed (NCCL on GPUs, gloo on
-  CPUs); `dot` is one FP64 all-reduce.
+  CPUs); the cells that read no ghost DoFs (all but the top layer, which `LocalNumbering`
+  puts last in the cell order) are computed while the ghost update is in flight; `dot` is
+  one FP64 all-reduce.
 * `DistributedTransfer` uses the patch maps of each rank's cells with weights 1 / (patches
   holding the fine DoF over all ranks), `DistributedChebyshev` is deal.II's
   PreconditionChebyshev with global dot products in its eigenvalue estimate (start vector
@@ -123,6 +125,13 @@ class LocalNumbering:
         idx = np.asarray(dof_indices, dtype=np.uint32)
         self.dof_indices = np.where(idx == INVALID, np.uint32(INVALID),
                                     self.perm[np.minimum(idx, max(n - 1, 0))]).astype(np.uint32)
+        # cells that read ghost DoFs (the top layer) last: the others are computed while the
+        # ghost update is in flight
+        cells = self.dof_indices if self.dof_indices.ndim == 2 else self.dof_indices.reshape(-1, (degree + 1) ** 3)
+        touch = ((cells != INVALID) & (cells >= self.top_begin)).any(axis=1) if self.n_top else \
+            np.zeros(cells.shape[0], bool)
+        self.cell_order = np.concatenate([np.nonzero(~touch)[0], np.nonzero(touch)[0]]).astype(np.int64)
+        self.n_inner_cells = int((~touch).sum())
         self.constrained = self.perm[np.nonzero(cons)[0]].astype(np.uint32)
         self.constrained_flags = np.zeros(n, bool)
         self.constrained_flags[self.constrained] = True
@@ -178,8 +187,14 @@ class LibraryBackend:
         geometry = box_op.geometry()
         del box_op
         nb = self.numbering
-        self.op = LaplaceOperator.from_maps(nb.n, nb.dof_indices, nb.constrained, degree, dtype, G=geometry,
+        n_cells = nb.cell_order.shape[0]
+        # the operator holds the cells in the numbering's cell order (inner cells first)
+        self.op = LaplaceOperator.from_maps(nb.n, nb.dof_indices.reshape(n_cells, -1)[nb.cell_order], nb.constrained,
+                                            degree, dtype, G=geometry.reshape(n_cells, -1)[nb.cell_order],
                                             device=device)
+        cpw = self.op.cells_per_group()
+        self.n_cells = n_cells
+        self.split = (nb.n_inner_cells // cpw) * cpw  # first cell of the boundary pass
 
     def empty(self, n):
         return self.torch.empty(n, dtype=self.tdtype, device=f"cuda:{self.device}")
@@ -195,6 +210,9 @@ class LibraryBackend:
 
     def vmult(self, dst, src):
         self.op.vmult(dst, src)
+
+    def vmult_cells(self, dst, src, begin, end, init):
+        self.op.vmult_cells(dst, src, begin, end, init)
 
     def inverse_diagonal(self):
         self.op.compute_diagonal()
@@ -243,21 +261,26 @@ class DistributedOperator:
         self._inv_diag = None
 
     # -- halo exchange: every rank posts its sends and receives, then waits for all --------
-    def _exchange(self, sends, recvs):
+    def _post(self, sends, recvs):
         if not (self.dist.is_available() and self.dist.is_initialized()):
-            return
+            return []
         ops = [self.dist.P2POp(self.dist.isend, t, peer) for t, peer in sends]
         ops += [self.dist.P2POp(self.dist.irecv, t, peer) for t, peer in recvs]
-        if ops:
-            for req in self.dist.batch_isend_irecv(ops):
-                req.wait()
+        return self.dist.batch_isend_irecv(ops) if ops else []
 
-    def update_ghosts(self, v):
-        """v's top plane (ghosts) := the owner's bottom plane."""
+    def _exchange(self, sends, recvs):
+        for req in self._post(sends, recvs):
+            req.wait()
+
+    def _ghost_ops(self, v):
         nb, r = self.nb, self.part.rank
         sends = [(v[:nb.n_bottom], r - 1)] if self.part.has_below else []
         recvs = [(v[nb.top_begin:], r + 1)] if self.part.has_above else []
-        self._exchange(sends, recvs)
+        return sends, recvs
+
+    def update_ghosts(self, v):
+        """v's top plane (ghosts) := the owner's bottom plane."""
+        self._exchange(*self._ghost_ops(v))
 
     def zero_ghosts(self, v):
         if self.nb.n_top:
@@ -275,8 +298,21 @@ class DistributedOperator:
             self.be.axpy(v[:nb.free_bottom], 1.0, buf)
 
     def vmult(self, dst, src):
-        self.update_ghosts(src)
-        self.be.vmult(dst, src)
+        """dst = A src.  With a backend that applies cell ranges (`vmult_cells`, `split`), the
+        cells that read no ghost DoFs are computed while the ghost update is in flight and the
+        top layer after it (the reference's colour loop, bk3.h:187-227); the sends read only
+        owned entries and the receives write only ghost entries, which the inner cells do not
+        read."""
+        split = getattr(self.be, "split", None)
+        if split is None:
+            self.update_ghosts(src)
+            self.be.vmult(dst, src)
+        else:
+            reqs = self._post(*self._ghost_ops(src))
+            self.be.vmult_cells(dst, src, 0, split, True)
+            for req in reqs:
+                req.wait()
+            self.be.vmult_cells(dst, src, split, self.be.n_cells, False)
         self.compress(dst)
 
     def allreduce(self, values):

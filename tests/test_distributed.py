@@ -1,8 +1,9 @@
 """The z-slab partitioned operator and CG (pmg.distributed) on CPU ranks over gloo.
 
 Each rank computes its cells with the oracle (the CPU restatement, standing in for the GPU
-kernels); the partition, the local renumbering, the ghost update and compress, the global
-dot products and the distributed CG are the library's.  The partitioned vmult must equal the
+kernels); the partition, the local renumbering, the ghost update and compress (with the inner
+cells computed while the ghost update is in flight), the global dot products and the
+distributed CG are the library's.  The partitioned vmult must equal the
 single-domain oracle vmult to 1e-13, every global DoF must be owned by exactly one rank, and
 the distributed Jacobi-CG must take the single-domain Jacobi-CG's iterations and give its
 solution to 1e-10."""
@@ -82,6 +83,13 @@ class OracleBackend:
         self.G = O.geometry_G(ob, p)
         self.cons = np.zeros(nb.n, np.uint8)
         self.cons[nb.constrained] = 1
+        # the cell order of the library backend (inner cells first) and its split at a multiple
+        # of the cells per warp group, so that DistributedOperator.vmult takes the overlapped
+        # path (inner cells during the ghost update, the top layer after it)
+        self.n_cells = nb.cell_order.shape[0]
+        cpw = 32 // (p + 1)
+        self.split = (nb.n_inner_cells // cpw) * cpw
+        self.calls = []
 
     def from_host(self, a):
         return torch.tensor(np.asarray(a, np.float64))
@@ -110,6 +118,21 @@ class OracleBackend:
 
     def vmult(self, dst, src):
         dst.copy_(torch.from_numpy(self.O.vmult(self.p, self.numbering.dof_indices, self.G, self.cons, src.numpy())))
+
+    def vmult_cells(self, dst, src, begin, end, init):
+        """dst += A_K src over the cells [begin, end) of the cell order (init: dst = that with
+        the identity rows), as pmg_operator_vmult_cells."""
+        self.calls.append((begin, end, init))
+        cells = self.numbering.cell_order[begin:end]
+        idx = self.numbering.dof_indices.reshape(self.n_cells, -1)[cells]
+        G = self.G.reshape(self.n_cells, -1)[cells]
+        s = src.numpy()
+        y = self.O.vmult(self.p, idx, G, self.cons, s)
+        if init:
+            dst.copy_(torch.from_numpy(y))
+        else:
+            y[self.cons == 1] -= s[self.cons == 1]  # the identity rows only once
+            dst.add_(torch.from_numpy(y))
 
     def inverse_diagonal(self):
         d = self.O.diagonal(self.p, self.numbering.dof_indices, self.G, self.cons)
@@ -162,6 +185,15 @@ def _worker(rank, world, port, q, case):
         b_g = O.rhs(_obox(O, gbox), p, p + 1, 0, plain_g, cons_g)
         x = be.zeros(nb.n)
         info = cg_solve(A, x, torch.from_numpy(b_g[gid].copy()), reduce=1e-10, max_iterations=500)
+        # the overlapped path: an inner pass with init, then the boundary pass; with ghosts the
+        # top layer is a proper part of the cells
+        assert be.calls[:2] == [(0, be.split, True), (be.split, be.n_cells, False)]
+        if part.has_above:
+            assert 0 < be.split < be.n_cells
+            top = set(be.numbering.cell_order[nb.n_inner_cells:].tolist())
+            di = nb.dof_indices.reshape(be.n_cells, -1)
+            reads_ghost = ((di != 0xFFFFFFFF) & (di >= nb.top_begin)).any(axis=1)
+            assert top == set(np.nonzero(reads_ghost)[0].tolist())
         q.put((rank, gid[:nb.n_owned], dst[:nb.n_owned].numpy(), x[:nb.n_owned].numpy(), info,
                (nb.n_bottom, nb.n_top, nb.free_bottom, nb.free_top)))
         dist.barrier()

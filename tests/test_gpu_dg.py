@@ -35,9 +35,10 @@ BOXES = {
 
 def tile_form(box, p, dtype):
     """True where the face kernel takes the tile form: the box refined at least twice and
-    the tile (64 cells' values plus four face-point arrays of 240 faces) within 200 KiB."""
+    its shared memory (two face-point arrays of 240 faces, then the larger of the 64 cells'
+    values and two more face-point arrays) within 200 KiB."""
     n = p + 1
-    size = (8 if dtype == pmg.F64 else 4) * (64 * n ** 3 + 4 * 240 * n * n)
+    size = (8 if dtype == pmg.F64 else 4) * (2 * 240 * n * n + max(64 * n ** 3, 2 * 240 * n * n))
     return box.refine >= 2 and size <= 200 * 1024
 
 

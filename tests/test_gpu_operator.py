@@ -348,3 +348,62 @@ def test_tensor_core_mode_rejected_where_not_built():
     op64 = pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(refine=1)), 2, pmg.F64, pmg.GEOMETRY_AFFINE)
     with pytest.raises(pmg.PmgError):
         op64.set_tensor_cores(3)
+
+
+# cell ranges (pmg_operator_vmult_cells): the split of a sharded vmult into the cells computed
+# while the ghost update is in flight and the rest; the sum of the passes equals vmult up to
+# the order of the additions, and the oracle on the same cells
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+@pytest.mark.parametrize("degree,geometry,coeff", [(3, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
+                                                   (4, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
+                                                   (2, pmg.GEOMETRY_AFFINE, pmg.COEFF_KAPPA),
+                                                   (5, pmg.GEOMETRY_INVJAC, pmg.COEFF_NONE)])
+def test_vmult_cells_passes_sum_to_vmult(oracle, dtype, degree, geometry, coeff):
+    box = pmg.Box.make(coarse=(3, 2, 2), refine=2, hi=(3.0, 2.0, 2.0),
+                       deform=0 if geometry == pmg.GEOMETRY_AFFINE else 1)
+    ob = obox(oracle, box)
+    op = pmg.LaplaceOperator(pmg.Mesh(box), degree, dtype, geometry, coeff)
+    cpw = op.cells_per_group()
+    assert cpw == 32 // (degree + 1)
+    n_cells = op.n_cells()
+    td = torch.float64 if dtype == pmg.F64 else torch.float32
+    src = torch.tensor(random_src(op.m(), 3), dtype=td, device="cuda")
+    full = op.initialize_dof_vector()
+    op.vmult(full, src)
+    cut1 = (n_cells // 3 // cpw) * cpw
+    cut2 = (2 * n_cells // 3 // cpw) * cpw
+    for cuts in ([0, n_cells], [0, cut1, n_cells], [0, cut1, cut2, n_cells], [0, 0, n_cells]):
+        d = torch.full_like(full, 7.0)  # overwritten by the first (init) pass
+        for k, (a, b) in enumerate(zip(cuts, cuts[1:])):
+            op.vmult_cells(d, src, a, b, k == 0)
+        torch.cuda.synchronize()
+        assert rel_err(d.double().cpu().numpy(), full.double().cpu().numpy()) < (1e-14 if dtype == pmg.F64 else 1e-6)
+    # one pass over a range alone against the oracle on those cells (plus the identity rows)
+    plain, cons, idx = oracle.dofs(ob, degree)
+    if geometry == pmg.GEOMETRY_INVJAC:
+        iJ, jxw = oracle.invjac(ob, degree, coeff)
+        ref = oracle.vmult_invjac(degree, idx[cut1:], np.ascontiguousarray(iJ.reshape(n_cells, -1)[cut1:]).reshape(-1),
+                                  np.ascontiguousarray(jxw.reshape(n_cells, -1)[cut1:]).reshape(-1), cons,
+                                  src.double().cpu().numpy())
+    else:
+        G = oracle.geometry_G(ob, degree, coeff_kind=coeff).reshape(n_cells, -1)
+        ref = oracle.vmult(degree, idx[cut1:], G[cut1:], cons, src.double().cpu().numpy())
+    d = op.initialize_dof_vector()
+    op.vmult_cells(d, src, cut1, n_cells, True)
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype]
+
+
+def test_vmult_cells_rejects_bad_ranges():
+    op = pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(refine=2, deform=1)), 4, pmg.F64)
+    cpw = op.cells_per_group()
+    src = torch.zeros(op.m(), dtype=torch.float64, device="cuda")
+    dst = torch.zeros_like(src)
+    for a, b in ((1, cpw * 2), (0, cpw + 1), (cpw * 2, cpw), (-cpw, 0), (0, 65)):
+        with pytest.raises(pmg.PmgError):
+            op.vmult_cells(dst, src, a, b, True)
+    op.vmult_cells(dst, src, 0, 64, True)  # the cell count ends a range anywhere
+    dg = pmg.DGLaplaceOperator(pmg.Mesh(pmg.Box.make(refine=1)), 2, pmg.F64)
+    v = torch.zeros(dg.m(), dtype=torch.float64, device="cuda")
+    with pytest.raises(pmg.PmgError):
+        dg.vmult_cells(v, v.clone(), 0, 8, True)
