@@ -355,7 +355,6 @@ template <typename T> __global__ void add_kernel(T *__restrict__ dst, const doub
 // adds that to dst in one coalesced pass.  The faces of the tile surface are still met from
 // both sides.
 constexpr int kTileFaces = 240; // 3 x 48 inside, 6 x 16 on the surface
-constexpr int kTileThreads = 256;
 // shared memory of the tile kernel: the face-point arrays F1, F2, then one region that holds
 // the tile's values in phase 1 and the face-point arrays G1, G2 from phase 2 on
 template <int N, typename T> constexpr size_t dg_tile_region() {
@@ -400,8 +399,8 @@ __device__ __forceinline__ void tile_face(int fi, int &d, int &lo, int &up, int 
   }
 }
 
-template <int N, typename T>
-__global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid_constant__ DGTab<N, T> tab,
+template <int N, typename T, int TT>
+__global__ void __launch_bounds__(TT) dg_face_tile_kernel(const __grid_constant__ DGTab<N, T> tab,
                                                                     const __grid_constant__ DGGeo geo,
                                                                     const T *__restrict__ src, T *__restrict__ dst,
                                                                     const int32_t *__restrict__ nbr, int64_t n_tiles) {
@@ -413,10 +412,10 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
     const T *ts = src + base * N3;
-    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) U[e] = ts[e];
+    for (int e = threadIdx.x; e < 64 * N3; e += TT) U[e] = ts[e];
     __syncthreads();
     // 1. fluxes f1 = sigma [u] - {d_n u}, f2 = -[u]/2 at every face point, times the face area
-    for (int t = threadIdx.x; t < NP; t += kTileThreads) {
+    for (int t = threadIdx.x; t < NP; t += TT) {
       const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
       int d, lo, up, F, in;
       tile_face(fi, d, lo, up, F, in);
@@ -466,7 +465,7 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
     }
     __syncthreads();
     // 2. face mass along a
-    for (int t = threadIdx.x; t < NP; t += kTileThreads) {
+    for (int t = threadIdx.x; t < NP; t += TT) {
       const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
       const T *f1 = F1 + fi * N2 + bb * N, *f2 = F2 + fi * N2 + bb * N;
       T g1 = T(0), g2 = T(0);
@@ -481,7 +480,7 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
     __syncthreads();
     // 3. face mass along b: the value-test coefficient (F1) and the normal-derivative-test
     //    coefficient (F2, divided by h; on the tile surface times the outward normal's sign)
-    for (int t = threadIdx.x; t < NP; t += kTileThreads) {
+    for (int t = threadIdx.x; t < NP; t += TT) {
       const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
       const T *g1 = G1 + fi * N2 + a, *g2 = G2 + fi * N2 + a;
       T tv = T(0), tn = T(0);
@@ -508,7 +507,7 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
     //    outward normal is opposite to the one the face was evaluated with) and the
     //    normal-derivative test on every layer, then adds the sum to dst
     T *td = dst + base * N3;
-    for (int e = threadIdx.x; e < 64 * N3; e += kTileThreads) {
+    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
       const int ct = e / N3, l = e - ct * N3;
       const int cx = (ct & 1) | (((ct >> 3) & 1) << 1), cy = ((ct >> 1) & 1) | (((ct >> 4) & 1) << 1),
                 cz = ((ct >> 2) & 1) | (((ct >> 5) & 1) << 1);
@@ -540,14 +539,47 @@ __global__ void __launch_bounds__(kTileThreads) dg_face_tile_kernel(const __grid
   }
 }
 
-// the face form: 2 (default) the tile kernel where the mesh allows it, else 1; PMG_DG_FACE=1 the
-// cell-batch kernel everywhere, 0 the face-by-face kernel (comparison switches)
+// the face form: PMG_DG_FACE=0 the face-by-face kernel, 1 the cell-batch kernel, 2 the tile
+// kernel wherever the mesh allows it (comparison switches, read at every launch); unset: the
+// tile kernel where the mesh allows it and the tiles fill the device at least twice, else the
+// cell-batch kernel
 int face_form() {
-  static const int v = [] {
-    const char *e = std::getenv("PMG_DG_FACE");
-    return (e && e[0] == '0') ? 0 : ((e && e[0] == '1') ? 1 : 2);
-  }();
-  return v;
+  const char *e = std::getenv("PMG_DG_FACE");
+  if (e && (e[0] == '0' || e[0] == '1' || e[0] == '2') && e[1] == 0) return e[0] - '0';
+  return -1;
+}
+
+// block size of the tile kernel on the current device: 256, 512 or 1024 threads, whichever
+// keeps the most threads per SM resident (its shared memory allows few blocks per SM)
+struct TileShape {
+  int threads = 256, blocks_per_sm = 1;
+};
+template <int N, typename T> TileShape tile_shape() {
+  static std::mutex mu;
+  static std::map<int, TileShape> cache; // device -> shape
+  int dev = 0;
+  PMG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  constexpr size_t smem = dg_tile_smem<N, T>();
+  TileShape best;
+  int best_threads = 0;
+  auto probe = [&](auto k, int tt) {
+    PMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nb = 0;
+    PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, tt, smem));
+    if (nb * tt > best_threads) {
+      best_threads = nb * tt;
+      best.threads = tt;
+      best.blocks_per_sm = std::max(1, nb);
+    }
+  };
+  probe(dg_face_tile_kernel<N, T, 256>, 256);
+  probe(dg_face_tile_kernel<N, T, 512>, 512);
+  probe(dg_face_tile_kernel<N, T, 1024>, 1024);
+  cache.emplace(dev, best);
+  return best;
 }
 
 template <int N, typename T> DGTab<N, T> make_dg_tab(const DGHost &h) {
@@ -577,30 +609,30 @@ void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, i
                                                                   static_cast<T *>(dst), h.nbr.as<int32_t>(), n_cells);
   } else {
     constexpr size_t tile_smem = dg_tile_smem<N, T>();
-    if (face_form() == 2 && h.tiles64 && n_cells % 64 == 0 && tile_smem <= 200 * 1024) {
-      auto k = dg_face_tile_kernel<N, T>;
-      static std::mutex mu;
-      static std::map<int, int> per_sm; // device -> resident blocks per SM
-      int dev = 0, resident = 1;
-      PMG_CUDA(cudaGetDevice(&dev));
-      {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = per_sm.find(dev);
-        if (it == per_sm.end()) {
-          PMG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
-          int nb = 0;
-          PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kTileThreads, tile_smem));
-          it = per_sm.emplace(dev, std::max(1, nb)).first;
-        }
-        resident = it->second;
-      }
-      const int64_t n_tiles = n_cells / 64;
-      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, (int64_t)resident * sms));
+    const int form = face_form();
+    const int64_t n_tiles = n_cells / 64;
+    bool tiles = (form == 2 || form < 0) && h.tiles64 && n_cells % 64 == 0 && tile_smem <= 200 * 1024;
+    TileShape sh;
+    if (tiles) {
+      sh = tile_shape<N, T>();
+      if (form < 0 && n_tiles < 2 * (int64_t)sh.blocks_per_sm * sms) tiles = false;
+    }
+    if (tiles) {
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, (int64_t)sh.blocks_per_sm * sms));
       if (units) *units = n_tiles;
       if (blocks) *blocks = grid;
-      k<<<grid, kTileThreads, tile_smem, s>>>(make_dg_tab<N, T>(h), make_geo(h), static_cast<const T *>(src),
-                                              static_cast<T *>(dst), h.nbr.as<int32_t>(), n_tiles);
-    } else if (face_form() == 0) {
+      const auto tab = make_dg_tab<N, T>(h);
+      const auto geo = make_geo(h);
+      const T *sp = static_cast<const T *>(src);
+      T *dp = static_cast<T *>(dst);
+      const int32_t *nb = h.nbr.as<int32_t>();
+      if (sh.threads == 1024)
+        dg_face_tile_kernel<N, T, 1024><<<grid, 1024, tile_smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
+      else if (sh.threads == 512)
+        dg_face_tile_kernel<N, T, 512><<<grid, 512, tile_smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
+      else
+        dg_face_tile_kernel<N, T, 256><<<grid, 256, tile_smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
+    } else if (form == 0) {
       constexpr int B = dg_batch_seq<N>();
       const int grid = (int)std::min<int64_t>((n_cells + B - 1) / B, (int64_t)sms * 16);
       if (units) *units = (n_cells + B - 1) / B;

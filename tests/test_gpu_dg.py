@@ -34,7 +34,7 @@ BOXES = {
 
 
 def tile_form(box, p, dtype):
-    """True where the face kernel takes the tile form: the box refined at least twice and
+    """True where the face kernel can take the tile form: the box refined at least twice and
     its shared memory (two face-point arrays of 240 faces, then the larger of the 64 cells'
     values and two more face-point arrays) within 200 KiB."""
     n = p + 1
@@ -58,9 +58,42 @@ def test_dg_vmult_matches_oracle(oracle, p, dtype, boxname):
         op.vmult(d, torch.tensor(src, dtype=td, device="cuda"))
         torch.cuda.synchronize()
         assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype], c_pen
-        units, _ = op.last_launch(pmg.KERNEL_DG_FACES)
-        n_cells = op.m() // (p + 1) ** 3
-        assert units == (n_cells // 64 if tile_form(box, p, dtype) else -(-n_cells // max(1, 384 // (6 * (p + 1) ** 2))))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 6])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+@pytest.mark.parametrize("boxname", ["cube_r2", "ragged_r2", "neumann_r2"])
+def test_dg_tile_form_matches_oracle(oracle, monkeypatch, p, dtype, boxname):
+    """The tile form of the face kernel (forced with PMG_DG_FACE=2, which the library reads at
+    every launch; by default it takes it only where the tiles fill the device twice) on
+    meshes of 1 to 12 tiles, with Dirichlet and Neumann faces on the tile surfaces."""
+    monkeypatch.setenv("PMG_DG_FACE", "2")
+    box = pmg.Box.make(**BOXES[boxname])
+    ob = obox(oracle, box)
+    c_pen = 2.0 * (p + 1) ** 2
+    op = pmg.DGLaplaceOperator(pmg.Mesh(box), p, dtype, c_pen)
+    src = np.random.default_rng(p).uniform(-1, 1, op.m())
+    ref = oracle.dg_vmult(ob, p, c_pen, src)
+    td = torch.float64 if dtype == pmg.F64 else torch.float32
+    s = torch.tensor(src, dtype=td, device="cuda")
+    d = op.initialize_dof_vector()
+    op.vmult(d, s)
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), ref) < TOL[dtype]
+    units, _ = op.last_launch(pmg.KERNEL_DG_FACES)
+    n_cells = op.m() // (p + 1) ** 3
+    if tile_form(box, p, dtype):
+        assert units == n_cells // 64
+        # the tile form sums each node's faces in a fixed order: a second application, from
+        # a source that is not 16-byte aligned, gives the same bits
+        buf = torch.zeros(op.m() + 1, dtype=td, device="cuda")
+        buf[1:] = s
+        d2 = torch.empty_like(d)
+        op.vmult(d2, buf[1:])
+        torch.cuda.synchronize()
+        assert torch.equal(d, d2)
+    else:
+        assert units == -(-n_cells // max(1, 384 // (6 * (p + 1) ** 2)))
 
 
 @pytest.mark.parametrize("p", [1, 3, 5])
