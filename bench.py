@@ -714,6 +714,13 @@ def gpu_arm(args):
 #   adjoint_q4 the mass-matrix vmult and the per-point form of the adjoint gradient, Q4 FP64
 #              on 2^R cells per axis (default 6)
 #   vmult_q4   one Q4 FP64 vmult on the deformed cube with 2^R cells per axis (default 5)
+#   vmult_q6 / vmult_q6_tc
+#              one FP32 Q6 affine + kappa vmult (the config-3 fine operator) on 3^3 coarse
+#              cells refined R times (default 3 = 24^3), on CUDA cores / on the tensor cores
+#              (TF32 mma, one product)
+#   dg_vmult_q3 / dg_vmult_q3_f32
+#              one FP64 / FP32 DG-SIPG Q3 vmult (cell and face kernels) on 2^R cells per axis
+#              (default 6)
 # ----------------------------------------------------------------------------------------
 def _prof_range(torch, fn):
     torch.cuda.synchronize()
@@ -777,8 +784,34 @@ def _case_vmult_q4(torch, pmg, refine):
     _prof_range(torch, lambda: op.vmult(dst, src))
 
 
+def _vmult_case(torch, op):
+    src = torch.from_numpy(np.random.default_rng(1234).uniform(-1.0, 1.0, op.m())).to(op.torch_dtype).cuda()
+    dst = torch.empty_like(src)
+    for _ in range(3):
+        op.vmult(dst, src)
+    _prof_range(torch, lambda: op.vmult(dst, src))
+
+
+def _case_vmult_q6(torch, pmg, refine, tensor_cores=0):
+    op = pmg.LaplaceOperator(pmg.Mesh(pmg.Box.make(coarse=(3, 3, 3), refine=refine)), 6, pmg.F32,
+                             pmg.GEOMETRY_AFFINE, pmg.COEFF_KAPPA)
+    if tensor_cores:
+        op.set_tensor_cores(tensor_cores)
+    _vmult_case(torch, op)
+
+
+def _case_dg_vmult_q3(torch, pmg, refine, dtype=None):
+    p = 3
+    _vmult_case(torch, pmg.DGLaplaceOperator(pmg.Mesh(pmg.Box.make(refine=refine)), p,
+                                             pmg.F64 if dtype is None else dtype, 2.0 * (p + 1) ** 2))
+
+
 PROFILE_CASES = {"q6_kappa": (_case_q6_kappa, 4), "dg_q3": (_case_dg_q3, 6),
-                 "adjoint_q4": (_case_adjoint_q4, 6), "vmult_q4": (_case_vmult_q4, 5)}
+                 "adjoint_q4": (_case_adjoint_q4, 6), "vmult_q4": (_case_vmult_q4, 5),
+                 "vmult_q6": (_case_vmult_q6, 3),
+                 "vmult_q6_tc": (lambda torch, pmg, r: _case_vmult_q6(torch, pmg, r, 1), 3),
+                 "dg_vmult_q3": (_case_dg_vmult_q3, 6),
+                 "dg_vmult_q3_f32": (lambda torch, pmg, r: _case_dg_vmult_q3(torch, pmg, r, pmg.F32), 6)}
 
 
 def profile_case(args):
