@@ -352,9 +352,12 @@ def time_to_solution(torch, pmg, dev, refine=4, repeats=3):
     cells refined 4 times, 24,137,569 DoFs), f = 1, homogeneous Dirichlet; ph-multigrid with
     p 6 -> 3 -> 2 -> 1 and Q1 h-levels 48^3 .. 3^3, Chebyshev degree 4; FP64 CG to a relative
     residual of 1e-10.  The V-cycle runs in FP32 (mixed) or FP64 (all-FP64 method); each
-    number is the median of `repeats` solves from x = 0 after one warm-up solve."""
+    number is the median of `repeats` solves from x = 0 after one warm-up solve.  Each
+    variant's solution is compared with the FP64 ph-multigrid CG run to 1e-12
+    (`error_vs_fp64_1e-12`: max-norm difference relative to the max norm of that solution)."""
     box = pmg.Box.make(coarse=(3, 3, 3), refine=refine)
     res = {}
+    solutions, x_ref = {}, None
     # fp32_mg / fp64_mg: the ph-multigrid with an FP32 / FP64 V-cycle; fp64_plain_hmg: the
     # all-FP64 plain method (geometric multigrid at degree 6 on every level 48^3 .. 3^3,
     # GeometricTransfer<dim, fe_degree> as in source/geometric_multigrid/program.cc:245-249)
@@ -384,9 +387,17 @@ def time_to_solution(torch, pmg, dev, refine=4, repeats=3):
         rel = float(torch.linalg.norm(r - b) / torch.linalg.norm(b))
         res[name] = {"seconds": float(np.median(times)), "iterations": info["iterations"],
                      "relative_residual": rel, "reduction_per_step": info["reduction_per_step"]}
+        solutions[name] = x
+        if name == "fp64_mg":
+            x_ref, _ = h.solve(b, x=h.fine64.initialize_dof_vector(), reduce=1e-12, max_iterations=100)
         n = h.fine64.m()
-        del h, b, x, r
+        del h, b, r
         torch.cuda.empty_cache()
+    scale = float(x_ref.abs().max())
+    for name, x in solutions.items():
+        res[name]["error_vs_fp64_1e-12"] = float((x - x_ref).abs().max()) / scale
+    del solutions, x_ref
+    torch.cuda.empty_cache()
     res["n_dofs"] = n
     res["speedup_fp32_mg_over_fp64"] = res["fp64_mg"]["seconds"] / res["fp32_mg"]["seconds"]
     res["speedup_fp32_mg_over_fp64_plain"] = res["fp64_plain_hmg"]["seconds"] / res["fp32_mg"]["seconds"]
