@@ -122,6 +122,11 @@ public:
     check(pmg_operator_vmult_cells(op_.get(), dst.get_values(), src.get_values(), cell_begin, cell_end, init,
                                    stream_));
   }
+  int64_t n_cells() const {
+    int64_t v = 0;
+    check(pmg_operator_n_cells(op_.get(), &v));
+    return v;
+  }
   int cells_per_group() const {
     int32_t v = 0;
     check(pmg_operator_cells_per_group(op_.get(), &v));

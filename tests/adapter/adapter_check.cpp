@@ -2,7 +2,8 @@
 // maintainer of the reference would use it, with a stand-in for deal.II's device vector
 // (get_values(), size()), and checks on the GPU:
 //  1. an operator built from the caller's maps (here the box operator's own maps with the
-//     DoF numbers reversed and the cells listed backwards) gives the box operator's vmult;
+//     DoF numbers reversed and the cells listed backwards) gives the box operator's vmult,
+//     also when applied in two cell passes (vmult_cells, the split of a sharded vmult);
 //  2. a mixed-precision ph-multigrid CG solve through LaplaceOperator / Transfer / Chebyshev /
 //     VCycle / solve_cg converges.
 // Prints "adapter ok" and exits 0 on success.  Without a GPU it exits 2 after linking.
@@ -100,6 +101,21 @@ int main() {
     if (!(err <= 1e-12 * ref)) {
       std::printf("adapter: caller-map vmult differs: %.3e of %.3e\n", err, ref);
       return 1;
+    }
+    // 1b. the same product in two cell passes, as a sharded vmult splits it around the ghost
+    //     update: the first cells with init, the rest added
+    {
+      const int64_t split = (A_maps.n_cells() / 2 / A_maps.cells_per_group()) * A_maps.cells_per_group();
+      DeviceVector<double> dsplit(N);
+      A_maps.vmult_cells(dsplit, srcp, 0, split, true);
+      A_maps.vmult_cells(dsplit, srcp, split, A_maps.n_cells(), false);
+      const auto ys = dsplit.download();
+      double e2 = 0;
+      for (int64_t i = 0; i < N; ++i) e2 = std::fmax(e2, std::fabs(ys[i] - yp[i]));
+      if (!(e2 <= 1e-13 * ref)) {
+        std::printf("adapter: split vmult differs: %.3e of %.3e\n", e2, ref);
+        return 1;
+      }
     }
     // 2. ph-multigrid: Q1 on 1^3, 2^3, 4^3 cells, then Q2, Q3 on 4^3; FP32 levels, FP64 CG
     std::vector<std::unique_ptr<pmg::LaplaceOperator<float>>> lv;
