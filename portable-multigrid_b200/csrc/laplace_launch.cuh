@@ -171,18 +171,20 @@ template <typename T, int GEOM, bool SG, int PIPE> VmultShape vmult_shape() {
 
 // L2 policies of vmult_slab_kernel's first read of each index block and of its L2 prefetch
 // of the next group's geometry (0 evict-first, 1 evict-last, 2 evict-normal; packed two bits
-// each).  Both evict-last by default: the scatter reads the index block again and the ring
-// or the direct loads read the prefetched geometry (deformed cube 128^3 on B200: FP32 Q4
-// 2342 -> 2247 us, FP64 Q4 3936 -> 3904 us, FP64 Q3 1777 -> 1762 us against evict-first).
-// PMG_VMULT_IDX_POLICY and PMG_VMULT_PREFETCH_POLICY override.
+// each).  Defaults: evict-normal for the index block, whose scatter reads it again (deformed
+// cube 128^3 on B200: FP32 Q4 2342 -> 2245 us, FP64 Q4 3936 -> 3915 us against evict-first),
+// evict-first for the prefetch.  Evict-last measured as fast on one kernel alone but made the
+// config-3 FP32 V-cycle solve 48 -> 65 ms: evict-last lines outlive the launch and crowd the
+// vectors of every multigrid level out of L2.  PMG_VMULT_IDX_POLICY and
+// PMG_VMULT_PREFETCH_POLICY override.
 inline int idx_policy() {
   static const int v = [] {
-    auto get = [](const char *name) {
+    auto get = [](const char *name, int dflt) {
       const char *e = std::getenv(name);
       const int o = e ? std::atoi(e) : -1;
-      return (o >= 0 && o <= 2) ? o : 1;
+      return (o >= 0 && o <= 2) ? o : dflt;
     };
-    return get("PMG_VMULT_IDX_POLICY") | (get("PMG_VMULT_PREFETCH_POLICY") << 2);
+    return get("PMG_VMULT_IDX_POLICY", 2) | (get("PMG_VMULT_PREFETCH_POLICY", 0) << 2);
   }();
   return v;
 }
