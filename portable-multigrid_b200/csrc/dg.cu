@@ -354,154 +354,206 @@ template <typename T> __global__ void add_kernel(T *__restrict__ dst, const doub
 // give it, in a fixed order (no atomics, so the result does not depend on scheduling), and
 // adds that to dst in one coalesced pass.  The faces of the tile surface are still met from
 // both sides.
-constexpr int kTileFaces = 240; // 3 x 48 inside, 6 x 16 on the surface
-// shared memory of the tile kernel: the face-point arrays F1, F2, then one region that holds
-// the tile's values in phase 1 and the face-point arrays G1, G2 from phase 2 on
+//
+// Faces are numbered by direction d: 80 d + f, f < 48 inside the tile (f = 16 x along + the
+// tangential position), 48 <= f < 64 on the lower and 64 <= f < 80 on the upper surface.  A
+// face point is (a, b), a along the first and b along the second tangential axis; the flux
+// of face point t = (80 d + f) N^2 + b N + a is evaluated with d known at compile time.
+// Where a face's N^2 points divide a warp (N = 2, 4) they lie in one warp, and the face mass
+// M1 x M1 is applied with shuffles, without shared memory or block barriers.
+constexpr int kTileFaces = 240;
+constexpr int kDirFaces = 80;
+template <int N> constexpr int tile_cell_stride() { return N * N * N + 1; } // padded: fewer bank conflicts
+template <int N> constexpr bool tile_shuffles() { return 32 % (N * N) == 0; }
 template <int N, typename T> constexpr size_t dg_tile_region() {
-  return size_t(64) * N * N * N > size_t(2) * kTileFaces * N * N ? size_t(64) * N * N * N
-                                                                  : size_t(2) * kTileFaces * N * N;
+  // the tile's values; without shuffles also the face-mass arrays G1, G2 over them
+  return tile_shuffles<N>() || size_t(64) * tile_cell_stride<N>() > size_t(2) * kTileFaces * N * N
+             ? size_t(64) * tile_cell_stride<N>()
+             : size_t(2) * kTileFaces * N * N;
 }
+// shared memory of the tile kernel: the node-face table (64 x 6 ints), the face-point arrays
+// F1, F2, then the tile region
 template <int N, typename T> constexpr size_t dg_tile_smem() {
-  return sizeof(T) * (size_t(2) * kTileFaces * N * N + dg_tile_region<N, T>());
+  return sizeof(int) * 384 + sizeof(T) * (size_t(2) * kTileFaces * N * N + dg_tile_region<N, T>());
 }
 
 __device__ __forceinline__ int tile_index(int x, int y, int z) {
   return (x & 1) | ((y & 1) << 1) | ((z & 1) << 2) | ((x >> 1) << 3) | ((y >> 1) << 4) | ((z >> 1) << 5);
 }
 
-// face fi of a tile: direction d, the tile cell on the face's lower side (lo) and upper side
-// (up, -1 outside the tile), the face of the inside cell that lies on the tile surface (F,
-// -1 for a face inside the tile)
-__device__ __forceinline__ void tile_face(int fi, int &d, int &lo, int &up, int &F, int &in) {
+// flux values (times the face area) of face f of direction D at face point (a, bb): f1 =
+// sigma [u] - {d_n u}, f2 = -[u]/2 with the normal +D inside the tile, the inside cell's
+// outward normal on the surface (Dirichlet: mirror u+ = -u-, d_n u+ = d_n u-)
+template <int N, typename T, int D>
+__device__ __forceinline__ void tile_flux(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ U,
+                                          const T *__restrict__ src, const int32_t *__restrict__ nbr,
+                                          int64_t base, int f, int a, int bb, T &f1, T &f2) {
+  constexpr int N3 = N * N * N, CS = tile_cell_stride<N>();
+  constexpr int ta = D == 0 ? 1 : 0, tb = D == 2 ? 1 : 2;
+  const T h = (T)geo.h[D], area = (T)(geo.h[ta] * geo.h[tb]), sigma = (T)(geo.c_pen / geo.h[D]);
   int c[3];
-  if (fi < 144) {
-    d = fi / 48;
-    const int w = fi - 48 * d, along = w >> 4, tan = w & 15;
-    const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
-    c[d] = along;
+  f1 = T(0);
+  f2 = T(0);
+  if (f < 48) {
+    const int along = f >> 4, tan = f & 15;
+    c[D] = along;
     c[ta] = tan & 3;
     c[tb] = tan >> 2;
-    lo = tile_index(c[0], c[1], c[2]);
-    c[d] = along + 1;
-    up = tile_index(c[0], c[1], c[2]);
-    F = -1;
-    in = lo;
+    const T *ul = U + tile_index(c[0], c[1], c[2]) * CS;
+    c[D] = along + 1;
+    const T *uu = U + tile_index(c[0], c[1], c[2]) * CS;
+    T dn = T(0), dnn = T(0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const int l = face_node<N>(D, i, a, bb);
+      dn += tab.dphi1[i] * ul[l];
+      dnn += tab.dphi0[i] * uu[l];
+    }
+    const T jump = ul[face_node<N>(D, N - 1, a, bb)] - uu[face_node<N>(D, 0, a, bb)];
+    f1 = sigma * jump - T(0.5) * (dn + dnn) / h;
+    f2 = T(-0.5) * jump;
   } else {
-    const int e = fi - 144;
-    F = e >> 4;
-    d = F >> 1;
-    const int tan = e & 15, ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
-    c[d] = (F & 1) ? 3 : 0;
+    const int sd = (f - 48) >> 4, tan = (f - 48) & 15, F = 2 * D + sd;
+    c[D] = sd ? 3 : 0;
     c[ta] = tan & 3;
     c[tb] = tan >> 2;
-    in = tile_index(c[0], c[1], c[2]);
-    lo = up = -1;
+    const int in = tile_index(c[0], c[1], c[2]);
+    const T *uo = U + in * CS;
+    const T sgn_h = (sd ? T(1) : T(-1)) / h;
+    T dn = T(0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) dn += (sd ? tab.dphi1[i] : tab.dphi0[i]) * uo[face_node<N>(D, i, a, bb)];
+    dn *= sgn_h;
+    const T vo = sd ? uo[face_node<N>(D, N - 1, a, bb)] : uo[face_node<N>(D, 0, a, bb)];
+    const int32_t nb = __ldg(nbr + (base + in) * 6 + F);
+    if (nb >= 0) {
+      const T *un = src + int64_t(nb) * N3;
+      T dnn = T(0);
+#pragma unroll
+      for (int i = 0; i < N; ++i) dnn += (sd ? tab.dphi0[i] : tab.dphi1[i]) * __ldg(un + face_node<N>(D, i, a, bb));
+      dnn *= sgn_h;
+      const T vn = sd ? __ldg(un + face_node<N>(D, 0, a, bb)) : __ldg(un + face_node<N>(D, N - 1, a, bb));
+      const T jump = vo - vn;
+      f1 = sigma * jump - T(0.5) * (dn + dnn);
+      f2 = T(-0.5) * jump;
+    } else if ((geo.dirichlet >> F) & 1) {
+      f1 = sigma * T(2) * vo - dn;
+      f2 = -vo;
+    }
   }
+  f1 *= area;
+  f2 *= area;
 }
 
 template <int N, typename T, int TT>
-__global__ void __launch_bounds__(TT) dg_face_tile_kernel(const __grid_constant__ DGTab<N, T> tab,
+__global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __grid_constant__ DGTab<N, T> tab,
                                                                     const __grid_constant__ DGGeo geo,
                                                                     const T *__restrict__ src, T *__restrict__ dst,
                                                                     const int32_t *__restrict__ nbr, int64_t n_tiles) {
-  constexpr int N2 = N * N, N3 = N2 * N, NP = kTileFaces * N2;
+  constexpr int N2 = N * N, N3 = N2 * N, CS = tile_cell_stride<N>(), NP = kTileFaces * N2, DP = kDirFaces * N2;
+  constexpr bool SHFL = tile_shuffles<N>();
   extern __shared__ __align__(16) unsigned char dg_tile_raw[];
-  T *F1 = reinterpret_cast<T *>(dg_tile_raw), *F2 = F1 + NP;
-  T *U = F2 + NP;                  // the tile's values (phase 1)
-  T *G1 = U, *G2 = G1 + NP;        // over them from phase 2 on
+  int *NF = reinterpret_cast<int *>(dg_tile_raw); // [tile cell][face]: 2 x first face point + upper
+  T *F1 = reinterpret_cast<T *>(dg_tile_raw + sizeof(int) * 384), *F2 = F1 + NP;
+  T *U = F2 + NP;                  // the tile's values, cell stride CS
+  T *G1 = U, *G2 = G1 + NP;        // over them from phase 2 on (without shuffles)
+  // node-face table: face f of direction d seen from tile cell ct as its upper (+d) face
+  // (ct the lower cell of an inside face), lower face (ct the upper cell) or a surface face
+  for (int e = threadIdx.x; e < 384; e += TT) {
+    const int ct = e / 6, F = e - ct * 6, d = F >> 1, sd = F & 1;
+    const int cc[3] = {(ct & 1) | (((ct >> 3) & 1) << 1), ((ct >> 1) & 1) | (((ct >> 4) & 1) << 1),
+                       ((ct >> 2) & 1) | (((ct >> 5) & 1) << 1)};
+    const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+    const int tan = cc[ta] + 4 * cc[tb];
+    int f, up = 0;
+    if (sd && cc[d] < 3) {
+      f = 16 * cc[d] + tan;
+    } else if (!sd && cc[d] > 0) {
+      f = 16 * (cc[d] - 1) + tan;
+      up = 1;
+    } else {
+      f = 48 + 16 * sd + tan;
+    }
+    NF[e] = 2 * ((kDirFaces * d + f) * N2) + up;
+  }
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
     const T *ts = src + base * N3;
-    for (int e = threadIdx.x; e < 64 * N3; e += TT) U[e] = ts[e];
-    __syncthreads();
-    // 1. fluxes f1 = sigma [u] - {d_n u}, f2 = -[u]/2 at every face point, times the face area
-    for (int t = threadIdx.x; t < NP; t += TT) {
-      const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
-      int d, lo, up, F, in;
-      tile_face(fi, d, lo, up, F, in);
-      const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
-      const T h = (T)geo.h[d], area = (T)(geo.h[ta] * geo.h[tb]), sigma = (T)(geo.c_pen / geo.h[d]);
-      T f1 = T(0), f2 = T(0);
-      if (F < 0) { // inside: the lower cell's view, outward normal +d
-        T vo = T(0), vn = T(0), dn = T(0), dnn = T(0);
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-          const int l = face_node<N>(d, i, a, bb);
-          dn += tab.dphi1[i] * U[lo * N3 + l];
-          dnn += tab.dphi0[i] * U[up * N3 + l];
-        }
-        vo = U[lo * N3 + face_node<N>(d, N - 1, a, bb)];
-        vn = U[up * N3 + face_node<N>(d, 0, a, bb)];
-        const T jump = vo - vn;
-        f1 = sigma * jump - T(0.5) * (dn + dnn) / h;
-        f2 = T(-0.5) * jump;
-      } else { // on the tile surface: the inside cell's view
-        const int sd = F & 1;
-        const T sgn_h = (sd ? T(1) : T(-1)) / h;
-        const T *dphi_own = sd ? tab.dphi1 : tab.dphi0;
-        const T *dphi_nb = sd ? tab.dphi0 : tab.dphi1;
-        T dn = T(0);
-#pragma unroll
-        for (int i = 0; i < N; ++i) dn += dphi_own[i] * U[in * N3 + face_node<N>(d, i, a, bb)];
-        dn *= sgn_h;
-        const T vo = U[in * N3 + face_node<N>(d, sd ? N - 1 : 0, a, bb)];
-        const int32_t nb = __ldg(nbr + (base + in) * 6 + F);
-        if (nb >= 0) {
-          const T *un = src + int64_t(nb) * N3;
-          T dnn = T(0);
-#pragma unroll
-          for (int i = 0; i < N; ++i) dnn += dphi_nb[i] * __ldg(un + face_node<N>(d, i, a, bb));
-          dnn *= sgn_h;
-          const T jump = vo - __ldg(un + face_node<N>(d, sd ? 0 : N - 1, a, bb));
-          f1 = sigma * jump - T(0.5) * (dn + dnn);
-          f2 = T(-0.5) * jump;
-        } else if ((geo.dirichlet >> F) & 1) { // mirror: u+ = -u-, d_n u+ = d_n u-
-          f1 = sigma * T(2) * vo - dn;
-          f2 = -vo;
-        }
-      }
-      F1[t] = f1 * area;
-      F2[t] = f2 * area;
+    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
+      const int ct = e / N3;
+      U[ct * CS + (e - ct * N3)] = ts[e];
     }
     __syncthreads();
-    // 2. face mass along a
+    // 1. fluxes at every face point; with shuffles also the face mass (2., 3.): a face's N^2
+    //    points are N^2 consecutive lanes of one warp (NP is a multiple of 32, so every lane
+    //    of a warp takes part)
     for (int t = threadIdx.x; t < NP; t += TT) {
-      const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
-      const T *f1 = F1 + fi * N2 + bb * N, *f2 = F2 + fi * N2 + bb * N;
-      T g1 = T(0), g2 = T(0);
+      const int d = t / DP, r = t - d * DP, f = r / N2, ab = r - f * N2, a = ab % N, bb = ab / N;
+      T f1, f2;
+      if (d == 0) tile_flux<N, T, 0>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+      else if (d == 1) tile_flux<N, T, 1>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+      else tile_flux<N, T, 2>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+      if constexpr (SHFL) {
+        const int lane0 = (threadIdx.x & 31) - ab; // the face's first lane
+        T g1 = T(0), g2 = T(0);
 #pragma unroll
-      for (int k = 0; k < N; ++k) {
-        g1 += tab.M1[a * N + k] * f1[k];
-        g2 += tab.M1[a * N + k] * f2[k];
-      }
-      G1[t] = g1;
-      G2[t] = g2;
-    }
-    __syncthreads();
-    // 3. face mass along b: the value-test coefficient (F1) and the normal-derivative-test
-    //    coefficient (F2, divided by h; on the tile surface times the outward normal's sign)
-    for (int t = threadIdx.x; t < NP; t += TT) {
-      const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
-      const T *g1 = G1 + fi * N2 + a, *g2 = G2 + fi * N2 + a;
-      T tv = T(0), tn = T(0);
+        for (int k = 0; k < N; ++k) {
+          const T x1 = __shfl_sync(0xffffffffu, f1, lane0 + bb * N + k);
+          const T x2 = __shfl_sync(0xffffffffu, f2, lane0 + bb * N + k);
+          g1 += tab.M1[a * N + k] * x1;
+          g2 += tab.M1[a * N + k] * x2;
+        }
+        T tv = T(0), tn = T(0);
 #pragma unroll
-      for (int k = 0; k < N; ++k) {
-        tv += tab.M1[bb * N + k] * g1[k * N];
-        tn += tab.M1[bb * N + k] * g2[k * N];
-      }
-      int d;
-      T sg = T(1);
-      if (fi < 144) {
-        d = fi / 48;
+        for (int k = 0; k < N; ++k) {
+          const T y1 = __shfl_sync(0xffffffffu, g1, lane0 + k * N + a);
+          const T y2 = __shfl_sync(0xffffffffu, g2, lane0 + k * N + a);
+          tv += tab.M1[bb * N + k] * y1;
+          tn += tab.M1[bb * N + k] * y2;
+        }
+        // the normal-derivative coefficient divided by h; on the lower surface times -1
+        const T sg = (f >= 48 && f < 64) ? T(-1) : T(1);
+        F1[t] = tv;
+        F2[t] = tn * sg / (T)geo.h[d];
       } else {
-        const int F = (fi - 144) >> 4;
-        d = F >> 1;
-        sg = (F & 1) ? T(1) : T(-1);
+        F1[t] = f1;
+        F2[t] = f2;
       }
-      F1[t] = tv;
-      F2[t] = tn * sg / (T)geo.h[d];
     }
     __syncthreads();
+    if constexpr (!SHFL) {
+      // 2. face mass along a
+      for (int t = threadIdx.x; t < NP; t += TT) {
+        const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
+        const T *f1 = F1 + fi * N2 + bb * N, *f2 = F2 + fi * N2 + bb * N;
+        T g1 = T(0), g2 = T(0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          g1 += tab.M1[a * N + k] * f1[k];
+          g2 += tab.M1[a * N + k] * f2[k];
+        }
+        G1[t] = g1;
+        G2[t] = g2;
+      }
+      __syncthreads();
+      // 3. face mass along b: the value-test coefficient (F1) and the normal-derivative-test
+      //    coefficient (F2, divided by h; on the lower surface times -1)
+      for (int t = threadIdx.x; t < NP; t += TT) {
+        const int fi = t / N2, ab = t - fi * N2, a = ab % N, bb = ab / N;
+        const T *g1 = G1 + fi * N2 + a, *g2 = G2 + fi * N2 + a;
+        T tv = T(0), tn = T(0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          tv += tab.M1[bb * N + k] * g1[k * N];
+          tn += tab.M1[bb * N + k] * g2[k * N];
+        }
+        const int d = fi / kDirFaces, f = fi - d * kDirFaces;
+        const T sg = (f >= 48 && f < 64) ? T(-1) : T(1);
+        F1[t] = tv;
+        F2[t] = tn * sg / (T)geo.h[d];
+      }
+      __syncthreads();
+    }
     // 4. one thread per tile node sums its six faces in a fixed order (deterministic): the
     //    value test on the face layer (minus for the upper cell of an inside face, whose
     //    outward normal is opposite to the one the face was evaluated with) and the
@@ -509,29 +561,17 @@ __global__ void __launch_bounds__(TT) dg_face_tile_kernel(const __grid_constant_
     T *td = dst + base * N3;
     for (int e = threadIdx.x; e < 64 * N3; e += TT) {
       const int ct = e / N3, l = e - ct * N3;
-      const int cx = (ct & 1) | (((ct >> 3) & 1) << 1), cy = ((ct >> 1) & 1) | (((ct >> 4) & 1) << 1),
-                cz = ((ct >> 2) & 1) | (((ct >> 5) & 1) << 1);
-      const int cc[3] = {cx, cy, cz};
       const int idx[3] = {l % N, (l / N) % N, l / N2};
+      const int *nf = NF + ct * 6;
       T v = T(0);
 #pragma unroll
       for (int F = 0; F < 6; ++F) {
         const int d = F >> 1, sd = F & 1;
         const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
-        const int tan = cc[ta] + 4 * cc[tb];
-        int fi;
-        T sv = T(1);
-        if (sd && cc[d] < 3) {
-          fi = 48 * d + 16 * cc[d] + tan; // lower cell of an inside face
-        } else if (!sd && cc[d] > 0) {
-          fi = 48 * d + 16 * (cc[d] - 1) + tan; // upper cell of an inside face
-          sv = T(-1);
-        } else {
-          fi = 144 + 16 * F + tan; // on the tile surface
-        }
-        const int pab = fi * N2 + idx[tb] * N + idx[ta];
+        const int x = nf[F];
+        const int pab = (x >> 1) + idx[tb] * N + idx[ta];
         v += F2[pab] * (sd ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]]);
-        if (idx[d] == (sd ? N - 1 : 0)) v += sv * F1[pab];
+        if (idx[d] == (sd ? N - 1 : 0)) v += (x & 1) ? -F1[pab] : F1[pab];
       }
       td[e] += v;
     }

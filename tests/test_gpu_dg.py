@@ -35,10 +35,13 @@ BOXES = {
 
 def tile_form(box, p, dtype):
     """True where the face kernel can take the tile form: the box refined at least twice and
-    its shared memory (two face-point arrays of 240 faces, then the larger of the 64 cells'
-    values and two more face-point arrays) within 200 KiB."""
+    its shared memory (a 64 x 6 int table, two face-point arrays of 240 faces, then the 64
+    cells' values at a padded stride, or two more face-point arrays where those are larger
+    and the face mass does not run on shuffles) within 200 KiB."""
     n = p + 1
-    size = (8 if dtype == pmg.F64 else 4) * (2 * 240 * n * n + max(64 * n ** 3, 2 * 240 * n * n))
+    fp, cells = 2 * 240 * n * n, 64 * (n ** 3 + 1)
+    region = cells if (32 % (n * n) == 0 or cells > fp) else fp
+    size = 4 * 384 + (8 if dtype == pmg.F64 else 4) * (fp + region)
     return box.refine >= 2 and size <= 200 * 1024
 
 
