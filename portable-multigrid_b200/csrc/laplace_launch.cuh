@@ -171,12 +171,12 @@ template <typename T, int GEOM, bool SG, int PIPE> VmultShape vmult_shape() {
 
 // L2 policies of vmult_slab_kernel's first read of each index block and of its L2 prefetch
 // of the next group's geometry (0 evict-first, 1 evict-last, 2 evict-normal; packed two bits
-// each).  Defaults: evict-normal for the index block, whose scatter reads it again (deformed
-// cube 128^3 on B200: FP32 Q4 2342 -> 2245 us, FP64 Q4 3936 -> 3915 us against evict-first),
-// evict-first for the prefetch.  Evict-last measured as fast on one kernel alone but made the
-// config-3 FP32 V-cycle solve 48 -> 65 ms: evict-last lines outlive the launch and crowd the
-// vectors of every multigrid level out of L2.  PMG_VMULT_IDX_POLICY and
-// PMG_VMULT_PREFETCH_POLICY override.
+// each).  Both evict-first by default.  On one kernel alone evict-normal for the index block
+// measured faster where the vectors are far larger than L2 (deformed cube 128^3 on B200: FP32
+// Q4 2342 -> 2245 us), but where the source vector almost fits L2 it displaces the vector the
+// gathers read: the FP32 Q6 affine + kappa kernel at 48^3 (vectors of 96 MB, an index map of
+// 152 MB) went from 357 to 680 us with it, and the config-3 FP32 V-cycle solve from 48 to 65 ms.
+// PMG_VMULT_IDX_POLICY and PMG_VMULT_PREFETCH_POLICY override.
 inline int idx_policy() {
   static const int v = [] {
     auto get = [](const char *name, int dflt) {
@@ -184,7 +184,7 @@ inline int idx_policy() {
       const int o = e ? std::atoi(e) : -1;
       return (o >= 0 && o <= 2) ? o : dflt;
     };
-    return get("PMG_VMULT_IDX_POLICY", 2) | (get("PMG_VMULT_PREFETCH_POLICY", 0) << 2);
+    return get("PMG_VMULT_IDX_POLICY", 0) | (get("PMG_VMULT_PREFETCH_POLICY", 0) << 2);
   }();
   return v;
 }
