@@ -32,6 +32,7 @@ namespace {
 
 template <int N, typename T> struct DGTab {
   T M1[N * N];  // 1D mass matrix of the GLL Lagrange basis
+  T K1[N * N];  // 1D stiffness matrix (reference interval), for the fused cell term
   T dphi0[N];   // phi_i'(0)
   T dphi1[N];   // phi_i'(1)
 };
@@ -445,20 +446,11 @@ __device__ __forceinline__ void tile_flux(const DGTab<N, T> &tab, const DGGeo &g
   f2 *= area;
 }
 
-template <int N, typename T, int TT>
-__global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __grid_constant__ DGTab<N, T> tab,
-                                                                    const __grid_constant__ DGGeo geo,
-                                                                    const T *__restrict__ src, T *__restrict__ dst,
-                                                                    const int32_t *__restrict__ nbr, int64_t n_tiles) {
-  constexpr int N2 = N * N, N3 = N2 * N, CS = tile_cell_stride<N>(), NP = kTileFaces * N2, DP = kDirFaces * N2;
-  constexpr bool SHFL = tile_shuffles<N>();
-  extern __shared__ __align__(16) unsigned char dg_tile_raw[];
-  int *NF = reinterpret_cast<int *>(dg_tile_raw); // [tile cell][face]: 2 x first face point + upper
-  T *F1 = reinterpret_cast<T *>(dg_tile_raw + sizeof(int) * 384), *F2 = F1 + NP;
-  T *U = F2 + NP;                  // the tile's values, cell stride CS
-  T *G1 = U, *G2 = G1 + NP;        // over them from phase 2 on (without shuffles)
-  // node-face table: face f of direction d seen from tile cell ct as its upper (+d) face
-  // (ct the lower cell of an inside face), lower face (ct the upper cell) or a surface face
+// node-face table: face f of direction d seen from tile cell ct as its upper (+d) face (ct
+// the lower cell of an inside face), its lower face (ct the upper cell) or a surface face;
+// entry 2 x (first face point) + 1 for the upper cell of an inside face
+template <int N, int TT> __device__ __forceinline__ void fill_node_faces(int *NF) {
+  constexpr int N2 = N * N;
   for (int e = threadIdx.x; e < 384; e += TT) {
     const int ct = e / 6, F = e - ct * 6, d = F >> 1, sd = F & 1;
     const int cc[3] = {(ct & 1) | (((ct >> 3) & 1) << 1), ((ct >> 1) & 1) | (((ct >> 4) & 1) << 1),
@@ -476,6 +468,78 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
     }
     NF[e] = 2 * ((kDirFaces * d + f) * N2) + up;
   }
+}
+
+// phase 1 of the tile kernels with the face mass on shuffles (N^2 divides 32): the fluxes of
+// face point t, then M1 x M1 over the face's N^2 lanes; F1 = the value-test coefficient, F2 =
+// the normal-derivative-test coefficient divided by h (on the lower surface times -1)
+template <int N, typename T>
+__device__ __forceinline__ void tile_face_point_shfl(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ U,
+                                                     const T *__restrict__ src, const int32_t *__restrict__ nbr,
+                                                     int64_t base, int t, T *F1, T *F2) {
+  constexpr int N2 = N * N, DP = kDirFaces * N2;
+  const int d = t / DP, r = t - d * DP, f = r / N2, ab = r - f * N2, a = ab % N, bb = ab / N;
+  T f1, f2;
+  if (d == 0) tile_flux<N, T, 0>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+  else if (d == 1) tile_flux<N, T, 1>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+  else tile_flux<N, T, 2>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+  const int lane0 = (threadIdx.x & 31) - ab; // the face's first lane
+  T g1 = T(0), g2 = T(0);
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const T x1 = __shfl_sync(0xffffffffu, f1, lane0 + bb * N + k);
+    const T x2 = __shfl_sync(0xffffffffu, f2, lane0 + bb * N + k);
+    g1 += tab.M1[a * N + k] * x1;
+    g2 += tab.M1[a * N + k] * x2;
+  }
+  T tv = T(0), tn = T(0);
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const T y1 = __shfl_sync(0xffffffffu, g1, lane0 + k * N + a);
+    const T y2 = __shfl_sync(0xffffffffu, g2, lane0 + k * N + a);
+    tv += tab.M1[bb * N + k] * y1;
+    tn += tab.M1[bb * N + k] * y2;
+  }
+  const T sg = (f >= 48 && f < 64) ? T(-1) : T(1);
+  F1[t] = tv;
+  F2[t] = tn * sg / (T)geo.h[d];
+}
+
+// phase 4 of the tile kernels for node e of the tile: the sum of its six faces' tests in a
+// fixed order (the value test on the face layer, minus for the upper cell of an inside face,
+// and the normal-derivative test on every layer)
+template <int N, typename T>
+__device__ __forceinline__ T tile_node_faces(const DGTab<N, T> &tab, const int *__restrict__ NF, const T *F1,
+                                             const T *F2, int ct, int l) {
+  constexpr int N2 = N * N;
+  const int idx[3] = {l % N, (l / N) % N, l / N2};
+  const int *nf = NF + ct * 6;
+  T v = T(0);
+#pragma unroll
+  for (int F = 0; F < 6; ++F) {
+    const int d = F >> 1, sd = F & 1;
+    const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+    const int x = nf[F];
+    const int pab = (x >> 1) + idx[tb] * N + idx[ta];
+    v += F2[pab] * (sd ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]]);
+    if (idx[d] == (sd ? N - 1 : 0)) v += (x & 1) ? -F1[pab] : F1[pab];
+  }
+  return v;
+}
+
+template <int N, typename T, int TT>
+__global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __grid_constant__ DGTab<N, T> tab,
+                                                                    const __grid_constant__ DGGeo geo,
+                                                                    const T *__restrict__ src, T *__restrict__ dst,
+                                                                    const int32_t *__restrict__ nbr, int64_t n_tiles) {
+  constexpr int N2 = N * N, N3 = N2 * N, CS = tile_cell_stride<N>(), NP = kTileFaces * N2, DP = kDirFaces * N2;
+  constexpr bool SHFL = tile_shuffles<N>();
+  extern __shared__ __align__(16) unsigned char dg_tile_raw[];
+  int *NF = reinterpret_cast<int *>(dg_tile_raw); // [tile cell][face]: 2 x first face point + upper
+  T *F1 = reinterpret_cast<T *>(dg_tile_raw + sizeof(int) * 384), *F2 = F1 + NP;
+  T *U = F2 + NP;                  // the tile's values, cell stride CS
+  T *G1 = U, *G2 = G1 + NP;        // over them from phase 2 on (without shuffles)
+  fill_node_faces<N, TT>(NF);
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
     const T *ts = src + base * N3;
@@ -488,34 +552,14 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
     //    points are N^2 consecutive lanes of one warp (NP is a multiple of 32, so every lane
     //    of a warp takes part)
     for (int t = threadIdx.x; t < NP; t += TT) {
-      const int d = t / DP, r = t - d * DP, f = r / N2, ab = r - f * N2, a = ab % N, bb = ab / N;
-      T f1, f2;
-      if (d == 0) tile_flux<N, T, 0>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
-      else if (d == 1) tile_flux<N, T, 1>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
-      else tile_flux<N, T, 2>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
       if constexpr (SHFL) {
-        const int lane0 = (threadIdx.x & 31) - ab; // the face's first lane
-        T g1 = T(0), g2 = T(0);
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-          const T x1 = __shfl_sync(0xffffffffu, f1, lane0 + bb * N + k);
-          const T x2 = __shfl_sync(0xffffffffu, f2, lane0 + bb * N + k);
-          g1 += tab.M1[a * N + k] * x1;
-          g2 += tab.M1[a * N + k] * x2;
-        }
-        T tv = T(0), tn = T(0);
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-          const T y1 = __shfl_sync(0xffffffffu, g1, lane0 + k * N + a);
-          const T y2 = __shfl_sync(0xffffffffu, g2, lane0 + k * N + a);
-          tv += tab.M1[bb * N + k] * y1;
-          tn += tab.M1[bb * N + k] * y2;
-        }
-        // the normal-derivative coefficient divided by h; on the lower surface times -1
-        const T sg = (f >= 48 && f < 64) ? T(-1) : T(1);
-        F1[t] = tv;
-        F2[t] = tn * sg / (T)geo.h[d];
+        tile_face_point_shfl<N, T>(tab, geo, U, src, nbr, base, t, F1, F2);
       } else {
+        const int d = t / DP, r = t - d * DP, f = r / N2, ab = r - f * N2, a = ab % N, bb = ab / N;
+        T f1, f2;
+        if (d == 0) tile_flux<N, T, 0>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+        else if (d == 1) tile_flux<N, T, 1>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+        else tile_flux<N, T, 2>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
         F1[t] = f1;
         F2[t] = f2;
       }
@@ -561,19 +605,110 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
     T *td = dst + base * N3;
     for (int e = threadIdx.x; e < 64 * N3; e += TT) {
       const int ct = e / N3, l = e - ct * N3;
-      const int idx[3] = {l % N, (l / N) % N, l / N2};
-      const int *nf = NF + ct * 6;
-      T v = T(0);
-#pragma unroll
-      for (int F = 0; F < 6; ++F) {
-        const int d = F >> 1, sd = F & 1;
-        const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
-        const int x = nf[F];
-        const int pab = (x >> 1) + idx[tb] * N + idx[ta];
-        v += F2[pab] * (sd ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]]);
-        if (idx[d] == (sd ? N - 1 : 0)) v += (x & 1) ? -F1[pab] : F1[pab];
-      }
+      const T v = tile_node_faces<N, T>(tab, NF, F1, F2, ct, l);
       td[e] += v;
+    }
+    __syncthreads();
+  }
+}
+
+// The whole DG vmult on a tile (N = 2, 4: the face mass on shuffles): the cell stiffness term
+// of axis-aligned cells, A_K u = cx (K1 x M1 x M1) u + (M1 x (cy K1 x M1 + cz M1 x K1)) u with
+// cx = hy hz / hx, cy = hx hz / hy, cz = hx hy / hz (K1, M1 the 1D stiffness and mass
+// matrices on the reference interval, x acting on the first index), by three passes over the
+// tile in shared memory (z by lines into A and B, y by lines in place, x by nodes into the tile
+// array once the faces have read it), and the face terms as in dg_face_tile_kernel; phase 4
+// stores cell plus face terms: src is read once, dst written once, no index map, no zeroing.
+template <int N> constexpr int fused_cell_stride() { return tile_cell_stride<N>(); }
+template <int N, typename T> constexpr size_t dg_fused_smem() {
+  return sizeof(int) * 384 + sizeof(T) * (size_t(2) * kTileFaces * N * N + size_t(3) * 64 * tile_cell_stride<N>());
+}
+
+template <int N, typename T, int TT>
+__global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __grid_constant__ DGTab<N, T> tab,
+                                                                     const __grid_constant__ DGGeo geo,
+                                                                     const T *__restrict__ src, T *__restrict__ dst,
+                                                                     const int32_t *__restrict__ nbr, int64_t n_tiles) {
+  static_assert(tile_shuffles<N>(), "the fused tile kernel applies the face mass on shuffles");
+  constexpr int N2 = N * N, N3 = N2 * N, CS = tile_cell_stride<N>(), NP = kTileFaces * N2;
+  extern __shared__ __align__(16) unsigned char dg_tile_raw[];
+  int *NF = reinterpret_cast<int *>(dg_tile_raw);
+  T *F1 = reinterpret_cast<T *>(dg_tile_raw + sizeof(int) * 384), *F2 = F1 + NP;
+  T *U = F2 + NP;       // the tile's values, then the cell term
+  T *A = U + 64 * CS;   // z-pass M1 u, then the y-pass P = M1 M1 u, then (x-pass input)
+  T *B = A + 64 * CS;   // z-pass K1 u, then the y-pass S = cy K1 M1 u + cz M1 K1 u
+  const T cx = (T)(geo.h[1] * geo.h[2] / geo.h[0]), cy = (T)(geo.h[0] * geo.h[2] / geo.h[1]),
+          cz = (T)(geo.h[0] * geo.h[1] / geo.h[2]);
+  fill_node_faces<N, TT>(NF);
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t base = tile * 64;
+    const T *ts = src + base * N3;
+    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
+      const int ct = e / N3;
+      U[ct * CS + (e - ct * N3)] = ts[e];
+    }
+    __syncthreads();
+    // cell term, z pass: one thread per z line (cell, i, j)
+    for (int t = threadIdx.x; t < 64 * N2; t += TT) {
+      const int ct = t / N2, o = ct * CS + (t - ct * N2); // (j N + i) within the cell
+      T v[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) v[k] = U[o + k * N2];
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        T sa = T(0), sb = T(0);
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+          sa += tab.M1[k * N + m] * v[m];
+          sb += tab.K1[k * N + m] * v[m];
+        }
+        A[o + k * N2] = sa;
+        B[o + k * N2] = sb;
+      }
+    }
+    // face fluxes and face mass (phases 1-3 of the tile kernel)
+    for (int t = threadIdx.x; t < NP; t += TT) tile_face_point_shfl<N, T>(tab, geo, U, src, nbr, base, t, F1, F2);
+    __syncthreads();
+    // cell term, y pass in place: one thread per y line (cell, i, k)
+    for (int t = threadIdx.x; t < 64 * N2; t += TT) {
+      const int ct = t / N2, r = t - ct * N2, i = r % N, k = r / N, o = ct * CS + k * N2 + i;
+      T a[N], b[N];
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        a[j] = A[o + j * N];
+        b[j] = B[o + j * N];
+      }
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        T pp = T(0), qa = T(0), qb = T(0);
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+          pp += tab.M1[j * N + m] * a[m];
+          qa += tab.K1[j * N + m] * a[m];
+          qb += tab.M1[j * N + m] * b[m];
+        }
+        A[o + j * N] = pp;
+        B[o + j * N] = cy * qa + cz * qb;
+      }
+    }
+    __syncthreads();
+    // cell term, x pass: one thread per node, into the tile array (its values are read)
+    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
+      const int ct = e / N3, l = e - ct * N3, i = l % N, row = ct * CS + (l - i);
+      T c = T(0), d = T(0);
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        c += tab.K1[i * N + m] * A[row + m];
+        d += tab.M1[i * N + m] * B[row + m];
+      }
+      U[ct * CS + l] = cx * c + d;
+    }
+    __syncthreads();
+    // cell plus face terms into dst
+    T *td = dst + base * N3;
+    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
+      const int ct = e / N3, l = e - ct * N3;
+      td[e] = U[ct * CS + l] + tile_node_faces<N, T>(tab, NF, F1, F2, ct, l);
     }
     __syncthreads();
   }
@@ -589,12 +724,12 @@ int face_form() {
   return -1;
 }
 
-// block size of the tile kernel on the current device: 256, 512 or 1024 threads, whichever
-// keeps the most threads per SM resident (its shared memory allows few blocks per SM)
+// block size of a tile kernel on the current device: 256, 512 or 1024 threads, whichever keeps
+// the most threads per SM resident (their shared memory allows few blocks per SM)
 struct TileShape {
   int threads = 256, blocks_per_sm = 1;
 };
-template <int N, typename T> TileShape tile_shape() {
+template <int N, typename T, bool FUSED> TileShape tile_shape() {
   static std::mutex mu;
   static std::map<int, TileShape> cache; // device -> shape
   int dev = 0;
@@ -602,7 +737,7 @@ template <int N, typename T> TileShape tile_shape() {
   std::lock_guard<std::mutex> lock(mu);
   auto it = cache.find(dev);
   if (it != cache.end()) return it->second;
-  constexpr size_t smem = dg_tile_smem<N, T>();
+  constexpr size_t smem = FUSED ? dg_fused_smem<N, T>() : dg_tile_smem<N, T>();
   TileShape best;
   int best_threads = 0;
   auto probe = [&](auto k, int tt) {
@@ -615,16 +750,27 @@ template <int N, typename T> TileShape tile_shape() {
       best.blocks_per_sm = std::max(1, nb);
     }
   };
-  probe(dg_face_tile_kernel<N, T, 256>, 256);
-  probe(dg_face_tile_kernel<N, T, 512>, 512);
-  probe(dg_face_tile_kernel<N, T, 1024>, 1024);
+  if constexpr (FUSED) {
+    if constexpr (tile_shuffles<N>()) {
+      probe(dg_tile_fused_kernel<N, T, 256>, 256);
+      probe(dg_tile_fused_kernel<N, T, 512>, 512);
+      probe(dg_tile_fused_kernel<N, T, 1024>, 1024);
+    }
+  } else {
+    probe(dg_face_tile_kernel<N, T, 256>, 256);
+    probe(dg_face_tile_kernel<N, T, 512>, 512);
+    probe(dg_face_tile_kernel<N, T, 1024>, 1024);
+  }
   cache.emplace(dev, best);
   return best;
 }
 
 template <int N, typename T> DGTab<N, T> make_dg_tab(const DGHost &h) {
   DGTab<N, T> t;
-  for (int a = 0; a < N * N; ++a) t.M1[a] = (T)h.M1[a];
+  for (int a = 0; a < N * N; ++a) {
+    t.M1[a] = (T)h.M1[a];
+    t.K1[a] = (T)h.K1[a];
+  }
   for (int a = 0; a < N; ++a) {
     t.dphi0[a] = (T)h.dphi0[a];
     t.dphi1[a] = (T)h.dphi1[a];
@@ -654,7 +800,7 @@ void face_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, i
     bool tiles = (form == 2 || form < 0) && h.tiles64 && n_cells % 64 == 0 && tile_smem <= 200 * 1024;
     TileShape sh;
     if (tiles) {
-      sh = tile_shape<N, T>();
+      sh = tile_shape<N, T, false>();
       if (form < 0 && n_tiles < 2 * (int64_t)sh.blocks_per_sm * sms) tiles = false;
     }
     if (tiles) {
@@ -714,17 +860,76 @@ void face_dispatch(int degree, const DGHost &h, const void *src, void *dst, int6
   }
 }
 
+// PMG_DG_FUSE=0 turns the fused tile kernel off (a comparison switch, read at every launch)
+bool fuse_allowed() {
+  const char *e = std::getenv("PMG_DG_FUSE");
+  return !(e && e[0] == '0' && e[1] == 0);
+}
+
+template <int N, typename T>
+bool fused_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms, cudaStream_t s,
+                  int64_t *units, int64_t *blocks) {
+  if constexpr (!tile_shuffles<N>()) {
+    return false;
+  } else {
+    constexpr size_t smem = dg_fused_smem<N, T>();
+    const int form = face_form();
+    if (!fuse_allowed() || !(form == 2 || form < 0) || !h.tiles64 || n_cells % 64 != 0 || smem > 200 * 1024)
+      return false;
+    const TileShape sh = tile_shape<N, T, true>();
+    const int64_t n_tiles = n_cells / 64;
+    if (form < 0 && n_tiles < 2 * (int64_t)sh.blocks_per_sm * sms) return false;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, (int64_t)sh.blocks_per_sm * sms));
+    if (units) *units = n_tiles;
+    if (blocks) *blocks = grid;
+    const auto tab = make_dg_tab<N, T>(h);
+    const auto geo = make_geo(h);
+    const T *sp = static_cast<const T *>(src);
+    T *dp = static_cast<T *>(dst);
+    const int32_t *nb = h.nbr.as<int32_t>();
+    if (sh.threads == 1024)
+      dg_tile_fused_kernel<N, T, 1024><<<grid, 1024, smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
+    else if (sh.threads == 512)
+      dg_tile_fused_kernel<N, T, 512><<<grid, 512, smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
+    else
+      dg_tile_fused_kernel<N, T, 256><<<grid, 256, smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
+    PMG_LAUNCH_CHECK();
+    return true;
+  }
+}
+
+template <typename T>
+bool fused_dispatch(int degree, const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms, cudaStream_t s,
+                    int64_t *units, int64_t *blocks) {
+  switch (degree) {
+  case 1: return fused_launch<2, T>(h, src, dst, n_cells, sms, s, units, blocks);
+  case 3: return fused_launch<4, T>(h, src, dst, n_cells, sms, s, units, blocks);
+  default: return false;
+  }
+}
+
 } // namespace
+
+bool dg_apply_fused(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells, int sms,
+                    cudaStream_t s, int64_t *units, int64_t *blocks) {
+  return dtype == PMG_F64 ? fused_dispatch<double>(degree, h, src, dst, n_cells, sms, s, units, blocks)
+                          : fused_dispatch<float>(degree, h, src, dst, n_cells, sms, s, units, blocks);
+}
 
 void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen) {
   const int N = degree + 1;
   const Tables1D t = make_tables(degree, N);
   h.M1.assign(N * N, 0.0);
+  h.K1.assign(N * N, 0.0);
   for (int i = 0; i < N; ++i)
     for (int j = 0; j < N; ++j) {
-      double s = 0;
-      for (int q = 0; q < N; ++q) s += t.S[i * N + q] * t.S[j * N + q] * t.W[q];
+      double s = 0, k = 0;
+      for (int q = 0; q < N; ++q) {
+        s += t.S[i * N + q] * t.S[j * N + q] * t.W[q];
+        k += t.SD[i * N + q] * t.SD[j * N + q] * t.W[q];
+      }
       h.M1[i * N + j] = s;
+      h.K1[i * N + j] = k;
     }
   h.dphi0 = lagrange_derivative_at(degree, 0.0);
   h.dphi1 = lagrange_derivative_at(degree, 1.0);

@@ -8,7 +8,7 @@
 namespace pmg {
 
 struct DGHost {
-  std::vector<double> M1, dphi0, dphi1; // 1D GLL mass matrix, basis derivatives at 0 and 1
+  std::vector<double> M1, K1, dphi0, dphi1; // 1D GLL mass and stiffness matrices, basis derivatives at 0 and 1
   double h[3] = {0, 0, 0};
   double c_pen = 0;  // sigma = c_pen / h on every face (uniform boxes)
   int dirichlet = 0; // face mask
@@ -20,6 +20,12 @@ void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen);
 // units / blocks (if set) receive the cell batches and the blocks of the face-kernel launch
 void dg_apply_faces(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells,
                     int sms, cudaStream_t s, int64_t *units = nullptr, int64_t *blocks = nullptr);
+// The whole DG vmult (cell stiffness and face terms) in one tile kernel where it applies
+// (degrees 1 and 3, the box refined at least twice, the tiles filling the device twice or
+// PMG_DG_FACE=2; PMG_DG_FUSE=0 turns it off): dst = A src, written once.  Returns false, with
+// nothing launched, where it does not apply.
+bool dg_apply_fused(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells, int sms,
+                    cudaStream_t s, int64_t *units = nullptr, int64_t *blocks = nullptr);
 void dg_add_face_diagonal(const DGHost &h, int degree, int dtype, void *diag, int64_t n_cells, int sms,
                           cudaStream_t s);
 void dg_add_boundary_rhs(const DGHost &h, const BoxMesh &mesh, int degree, int nq, int dtype, void *b,

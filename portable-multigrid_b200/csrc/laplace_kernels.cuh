@@ -137,11 +137,6 @@ __device__ __forceinline__ uint64_t policy_evict_last() {
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
-__device__ __forceinline__ uint64_t policy_evict_normal() {
-  uint64_t p;
-  asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
 
 __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes, uint64_t pol) {
   asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(p), "r"(bytes),
@@ -405,7 +400,7 @@ template <int N, typename T, int GEOM, bool SMEM_G, int PIPE = 0>
 __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N, T, GEOM>::value))
     vmult_slab_kernel(const __grid_constant__ Tab<N, T> tab, const T *__restrict__ src, T *__restrict__ dst,
                       const uint32_t *__restrict__ idx, const T *__restrict__ geo,
-                      const T *__restrict__ coef, int64_t n_groups, unsigned int *err, int idx_pol) {
+                      const T *__restrict__ coef, int64_t n_groups, unsigned int *err) {
   using Lo = Layout<N>;
   constexpr int CPW = Lo::CPW, LANES = Lo::LANES, N2 = Lo::N2;
   constexpr int CS = Stride<N>::CELL;
@@ -460,12 +455,6 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   const int64_t warp0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   const uint64_t pol_first = policy_evict_first(), pol_last = policy_evict_last();
-  // L2 policies (idx_pol, two bits each: 0 evict-first, 1 evict-last, 2 evict-normal) of the
-  // first read of a group's index block (bits 0-1; the scatter reads it once more,
-  // evict-first) and of the L2 prefetch of the next group's geometry (bits 2-3; the ring or
-  // the direct loads then read it evict-first)
-  auto pick = [&](int m) { return m == 1 ? pol_last : (m == 2 ? policy_evict_normal() : pol_first); };
-  const uint64_t pol_idx = pick(idx_pol & 3), pol_pf = pick((idx_pol >> 2) & 3);
   if (SMEM_G && GEOM == 0) {
     if (lane == 0) {
       mbar_init(&bars[0], 1);
@@ -486,7 +475,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
     if (gg < n_groups) {
       const uint32_t *ip = idx + gg * (N2 * LANES) + lane;
 #pragma unroll
-      for (int a = 0; a < N2; ++a) cp_async(ibuf + (slot * N2 + a) * LANES, ip + a * LANES, 4, 4, pol_idx);
+      for (int a = 0; a < N2; ++a) cp_async(ibuf + (slot * N2 + a) * LANES, ip + a * LANES, 4, 4, pol_first);
     }
     cp_async_commit();
   };
@@ -512,7 +501,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
 #pragma unroll
       for (int k = 0; k < RP; ++k)
 #pragma unroll
-        for (int i = 0; i < RP; ++i) nidx[k][i] = ld_stream_early(ip + (k * N + i) * LANES, pol_idx);
+        for (int i = 0; i < RP; ++i) nidx[k][i] = ld_stream_early(ip + (k * N + i) * LANES, pol_first);
     }
   };
   auto load_next_src = [&](int64_t gg) {
@@ -538,7 +527,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
 
   for (int64_t g = warp0; g < n_groups; g += nwarps, ++it) {
     if ((GEOM == 0 || GEOM == 3) && lane == 0 && g + nwarps < n_groups)
-      prefetch_l2(geo + (g + nwarps) * (N2 * NCOMP * LANES), N2 * NCOMP * LANES * sizeof(T), pol_pf);
+      prefetch_l2(geo + (g + nwarps) * (N2 * NCOMP * LANES), N2 * NCOMP * LANES * sizeof(T), pol_first);
     const uint32_t *ig = idx + g * (N2 * LANES) + lane;
     const int slot = it & 1;
 
@@ -570,7 +559,7 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
         for (int k = 0; k < N; ++k)
 #pragma unroll
           for (int i = 0; i < N; ++i) {
-            const uint32_t id = ld_stream(ig + (k * N + i) * LANES, pol_idx);
+            const uint32_t id = ld_stream(ig + (k * N + i) * LANES, pol_first);
             u[k][i] = (id != kInvalidIdx) ? ld_keep(src + id, pol_last) : T(0);
           }
       }

@@ -169,26 +169,6 @@ template <typename T, int GEOM, bool SG, int PIPE> VmultShape vmult_shape() {
   return best;
 }
 
-// L2 policies of vmult_slab_kernel's first read of each index block and of its L2 prefetch
-// of the next group's geometry (0 evict-first, 1 evict-last, 2 evict-normal; packed two bits
-// each).  Both evict-first by default.  On one kernel alone evict-normal for the index block
-// measured faster where the vectors are far larger than L2 (deformed cube 128^3 on B200: FP32
-// Q4 2342 -> 2245 us), but where the source vector almost fits L2 it displaces the vector the
-// gathers read: the FP32 Q6 affine + kappa kernel at 48^3 (vectors of 96 MB, an index map of
-// 152 MB) went from 357 to 680 us with it, and the config-3 FP32 V-cycle solve from 48 to 65 ms.
-// PMG_VMULT_IDX_POLICY and PMG_VMULT_PREFETCH_POLICY override.
-inline int idx_policy() {
-  static const int v = [] {
-    auto get = [](const char *name, int dflt) {
-      const char *e = std::getenv(name);
-      const int o = e ? std::atoi(e) : -1;
-      return (o >= 0 && o <= 2) ? o : dflt;
-    };
-    return get("PMG_VMULT_IDX_POLICY", 0) | (get("PMG_VMULT_PREFETCH_POLICY", 0) << 2);
-  }();
-  return v;
-}
-
 template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabLaunch &L) {
   auto k = kern::vmult_slab_kernel<kN, T, GEOM, SG, PIPE>;
   const VmultShape sh = vmult_shape<T, GEOM, SG, PIPE>();
@@ -201,7 +181,7 @@ template <typename T, int GEOM, bool SG, int PIPE> void vmult_launch(const SlabL
   const size_t smem = (size_t)sh.wpb * kern::SlabSmem<kN, T, SG, PIPE>::PER_WARP;
   k<<<grid, 32 * sh.wpb, smem, L.stream>>>(
       make_tab<T>(L), static_cast<const T *>(L.src), static_cast<T *>(L.dst), L.idx,
-      static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err, idx_policy());
+      static_cast<const T *>(L.geo), static_cast<const T *>(L.coef), L.n_groups, L.err);
   PMG_LAUNCH_CHECK();
   if (L.launched) *L.launched = (int64_t)grid * sh.wpb;
 }

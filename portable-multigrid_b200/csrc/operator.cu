@@ -648,6 +648,17 @@ void vmult_init(const pmg_operator &op, void *dst, const void *src, cudaStream_t
 void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s, bool compute) {
   PMG_REQUIRE(dst && src, "null vector");
   PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");
+  if (compute && op.dg && op.n_cells > 0 && op.n_constrained == 0 && !op.tensor_cores) {
+    // DG on 4x4x4 tiles: cell and face terms in one kernel that writes dst once; both launch
+    // records describe it
+    prof::Scope scope("vmult_dg_tile", s);
+    if (dg_apply_fused(*op.dg, op.degree, op.dtype, src, dst, op.n_cells, op.sms, s,
+                       &op.launch_units[PMG_KERNEL_DG_FACES], &op.launch_par[PMG_KERNEL_DG_FACES])) {
+      op.launch_units[PMG_KERNEL_VMULT_CELL] = op.launch_units[PMG_KERNEL_DG_FACES];
+      op.launch_par[PMG_KERNEL_VMULT_CELL] = op.launch_par[PMG_KERNEL_DG_FACES];
+      return;
+    }
+  }
   vmult_init(op, dst, src, s);
   if (compute && op.n_cells > 0 && op.kind == PMG_OP_MASS) {
     prof::Scope scope("vmult_mass", s);

@@ -66,11 +66,14 @@ def test_dg_vmult_matches_oracle(oracle, p, dtype, boxname):
 @pytest.mark.parametrize("p", [1, 2, 3, 4, 6])
 @pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
 @pytest.mark.parametrize("boxname", ["cube_r2", "ragged_r2", "neumann_r2"])
-def test_dg_tile_form_matches_oracle(oracle, monkeypatch, p, dtype, boxname):
+@pytest.mark.parametrize("fuse", ["1", "0"])
+def test_dg_tile_form_matches_oracle(oracle, monkeypatch, p, dtype, boxname, fuse):
     """The tile form of the face kernel (forced with PMG_DG_FACE=2, which the library reads at
     every launch; by default it takes it only where the tiles fill the device twice) on
-    meshes of 1 to 12 tiles, with Dirichlet and Neumann faces on the tile surfaces."""
+    meshes of 1 to 12 tiles, with Dirichlet and Neumann faces on the tile surfaces; at p = 1, 3
+    the cell term runs in the same tile kernel unless PMG_DG_FUSE=0."""
     monkeypatch.setenv("PMG_DG_FACE", "2")
+    monkeypatch.setenv("PMG_DG_FUSE", fuse)
     box = pmg.Box.make(**BOXES[boxname])
     ob = obox(oracle, box)
     c_pen = 2.0 * (p + 1) ** 2
@@ -87,6 +90,8 @@ def test_dg_tile_form_matches_oracle(oracle, monkeypatch, p, dtype, boxname):
     n_cells = op.m() // (p + 1) ** 3
     if tile_form(box, p, dtype):
         assert units == n_cells // 64
+        # with the fused kernel the cell record describes the same tile launch
+        assert (op.last_launch(pmg.KERNEL_VMULT_CELL)[0] == n_cells // 64) == (fuse == "1" and p in (1, 3))
         # the tile form sums each node's faces in a fixed order: a second application, from
         # a source that is not 16-byte aligned, gives the same bits
         buf = torch.zeros(op.m() + 1, dtype=td, device="cuda")
