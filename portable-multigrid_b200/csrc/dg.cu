@@ -37,6 +37,15 @@ template <int N, typename T> struct DGTab {
   T dphi1[N];   // phi_i'(1)
 };
 
+// copy of the 1D tables in shared memory, for the accesses whose index differs between the
+// lanes of a warp (a constant-bank load with divergent addresses is replayed per address)
+template <int N, typename T> __device__ __forceinline__ void load_tab_shared(DGTab<N, T> &st, const DGTab<N, T> &tab) {
+  constexpr int n = (int)(sizeof(DGTab<N, T>) / sizeof(T));
+  const T *from = reinterpret_cast<const T *>(&tab);
+  T *to = reinterpret_cast<T *>(&st);
+  for (int e = threadIdx.x; e < n; e += blockDim.x) to[e] = from[e];
+}
+
 struct DGGeo {
   double h[3];   // cell extents
   double c_pen;  // sigma = c_pen / h_normal
@@ -132,6 +141,9 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
                                                                   int64_t n_cells) {
   constexpr int N2 = N * N, N3 = N2 * N, B = dg_batch<N>(), FP = 6 * B * N2;
   __shared__ T F1[6][B][N2], F2[6][B][N2], G1[6][B][N2], G2[6][B][N2];
+  __shared__ DGTab<N, T> st;
+  load_tab_shared(st, tab);
+  __syncthreads();
   const int t = threadIdx.x;
   // this thread's face point (phases 2-4)
   const int f = t / (B * N2), rem = t - f * (B * N2), b = rem / N2, ab = rem - b * N2, a = ab % N, bb = ab / N;
@@ -169,8 +181,8 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
       T g1 = T(0), g2 = T(0);
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        g1 += tab.M1[a * N + k] * F1[f][b][bb * N + k];
-        g2 += tab.M1[a * N + k] * F2[f][b][bb * N + k];
+        g1 += st.M1[a * N + k] * F1[f][b][bb * N + k];
+        g2 += st.M1[a * N + k] * F2[f][b][bb * N + k];
       }
       G1[f][b][ab] = g1;
       G2[f][b][ab] = g2;
@@ -180,8 +192,8 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
       T tv = T(0), tn = T(0);
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        tv += tab.M1[bb * N + k] * G1[f][b][k * N + a];
-        tn += tab.M1[bb * N + k] * G2[f][b][k * N + a];
+        tv += st.M1[bb * N + k] * G1[f][b][k * N + a];
+        tn += st.M1[bb * N + k] * G2[f][b][k * N + a];
       }
       F1[f][b][ab] = tv;
       F2[f][b][ab] = tn * sgn_h;
@@ -198,7 +210,7 @@ __global__ void __launch_bounds__(dg_threads<N>(), 4) dg_face_kernel(const __gri
         const int dd = ff >> 1, ss = ff & 1;
         const int pa = dd == 0 ? idx[1] : idx[0], pb = dd == 2 ? idx[1] : idx[2];
         const int pab = pb * N + pa;
-        const T *dphi = ss ? tab.dphi1 : tab.dphi0;
+        const T *dphi = ss ? st.dphi1 : st.dphi0;
         v += F2[ff][cb][pab] * dphi[idx[dd]];
         if (idx[dd] == (ss ? N - 1 : 0)) v += F1[ff][cb][pab];
       }
@@ -474,9 +486,10 @@ template <int N, int TT> __device__ __forceinline__ void fill_node_faces(int *NF
 // face point t, then M1 x M1 over the face's N^2 lanes; F1 = the value-test coefficient, F2 =
 // the normal-derivative-test coefficient divided by h (on the lower surface times -1)
 template <int N, typename T>
-__device__ __forceinline__ void tile_face_point_shfl(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ U,
-                                                     const T *__restrict__ src, const int32_t *__restrict__ nbr,
-                                                     int64_t base, int t, T *F1, T *F2) {
+__device__ __forceinline__ void tile_face_point_shfl(const DGTab<N, T> &tab, const DGTab<N, T> &st, const DGGeo &geo,
+                                                     const T *__restrict__ U, const T *__restrict__ src,
+                                                     const int32_t *__restrict__ nbr, int64_t base, int t, T *F1,
+                                                     T *F2) {
   constexpr int N2 = N * N, DP = kDirFaces * N2;
   const int d = t / DP, r = t - d * DP, f = r / N2, ab = r - f * N2, a = ab % N, bb = ab / N;
   T f1, f2;
@@ -489,16 +502,16 @@ __device__ __forceinline__ void tile_face_point_shfl(const DGTab<N, T> &tab, con
   for (int k = 0; k < N; ++k) {
     const T x1 = __shfl_sync(0xffffffffu, f1, lane0 + bb * N + k);
     const T x2 = __shfl_sync(0xffffffffu, f2, lane0 + bb * N + k);
-    g1 += tab.M1[a * N + k] * x1;
-    g2 += tab.M1[a * N + k] * x2;
+    g1 += st.M1[a * N + k] * x1;
+    g2 += st.M1[a * N + k] * x2;
   }
   T tv = T(0), tn = T(0);
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     const T y1 = __shfl_sync(0xffffffffu, g1, lane0 + k * N + a);
     const T y2 = __shfl_sync(0xffffffffu, g2, lane0 + k * N + a);
-    tv += tab.M1[bb * N + k] * y1;
-    tn += tab.M1[bb * N + k] * y2;
+    tv += st.M1[bb * N + k] * y1;
+    tn += st.M1[bb * N + k] * y2;
   }
   const T sg = (f >= 48 && f < 64) ? T(-1) : T(1);
   F1[t] = tv;
@@ -509,7 +522,7 @@ __device__ __forceinline__ void tile_face_point_shfl(const DGTab<N, T> &tab, con
 // fixed order (the value test on the face layer, minus for the upper cell of an inside face,
 // and the normal-derivative test on every layer)
 template <int N, typename T>
-__device__ __forceinline__ T tile_node_faces(const DGTab<N, T> &tab, const int *__restrict__ NF, const T *F1,
+__device__ __forceinline__ T tile_node_faces(const DGTab<N, T> &st, const int *__restrict__ NF, const T *F1,
                                              const T *F2, int ct, int l) {
   constexpr int N2 = N * N;
   const int idx[3] = {l % N, (l / N) % N, l / N2};
@@ -521,7 +534,7 @@ __device__ __forceinline__ T tile_node_faces(const DGTab<N, T> &tab, const int *
     const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
     const int x = nf[F];
     const int pab = (x >> 1) + idx[tb] * N + idx[ta];
-    v += F2[pab] * (sd ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]]);
+    v += F2[pab] * (sd ? st.dphi1[idx[d]] : st.dphi0[idx[d]]);
     if (idx[d] == (sd ? N - 1 : 0)) v += (x & 1) ? -F1[pab] : F1[pab];
   }
   return v;
@@ -539,6 +552,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
   T *F1 = reinterpret_cast<T *>(dg_tile_raw + sizeof(int) * 384), *F2 = F1 + NP;
   T *U = F2 + NP;                  // the tile's values, cell stride CS
   T *G1 = U, *G2 = G1 + NP;        // over them from phase 2 on (without shuffles)
+  __shared__ DGTab<N, T> st;
+  load_tab_shared(st, tab);
   fill_node_faces<N, TT>(NF);
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
@@ -553,7 +568,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
     //    of a warp takes part)
     for (int t = threadIdx.x; t < NP; t += TT) {
       if constexpr (SHFL) {
-        tile_face_point_shfl<N, T>(tab, geo, U, src, nbr, base, t, F1, F2);
+        tile_face_point_shfl<N, T>(tab, st, geo, U, src, nbr, base, t, F1, F2);
       } else {
         const int d = t / DP, r = t - d * DP, f = r / N2, ab = r - f * N2, a = ab % N, bb = ab / N;
         T f1, f2;
@@ -573,8 +588,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
         T g1 = T(0), g2 = T(0);
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-          g1 += tab.M1[a * N + k] * f1[k];
-          g2 += tab.M1[a * N + k] * f2[k];
+          g1 += st.M1[a * N + k] * f1[k];
+          g2 += st.M1[a * N + k] * f2[k];
         }
         G1[t] = g1;
         G2[t] = g2;
@@ -588,8 +603,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
         T tv = T(0), tn = T(0);
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-          tv += tab.M1[bb * N + k] * g1[k * N];
-          tn += tab.M1[bb * N + k] * g2[k * N];
+          tv += st.M1[bb * N + k] * g1[k * N];
+          tn += st.M1[bb * N + k] * g2[k * N];
         }
         const int d = fi / kDirFaces, f = fi - d * kDirFaces;
         const T sg = (f >= 48 && f < 64) ? T(-1) : T(1);
@@ -605,7 +620,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
     T *td = dst + base * N3;
     for (int e = threadIdx.x; e < 64 * N3; e += TT) {
       const int ct = e / N3, l = e - ct * N3;
-      const T v = tile_node_faces<N, T>(tab, NF, F1, F2, ct, l);
+      const T v = tile_node_faces<N, T>(st, NF, F1, F2, ct, l);
       td[e] += v;
     }
     __syncthreads();
@@ -639,6 +654,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
   T *B = A + 64 * CS;   // z-pass K1 u, then the y-pass S = cy K1 M1 u + cz M1 K1 u
   const T cx = (T)(geo.h[1] * geo.h[2] / geo.h[0]), cy = (T)(geo.h[0] * geo.h[2] / geo.h[1]),
           cz = (T)(geo.h[0] * geo.h[1] / geo.h[2]);
+  __shared__ DGTab<N, T> st;
+  load_tab_shared(st, tab);
   fill_node_faces<N, TT>(NF);
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
@@ -667,7 +684,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
       }
     }
     // face fluxes and face mass (phases 1-3 of the tile kernel)
-    for (int t = threadIdx.x; t < NP; t += TT) tile_face_point_shfl<N, T>(tab, geo, U, src, nbr, base, t, F1, F2);
+    for (int t = threadIdx.x; t < NP; t += TT) tile_face_point_shfl<N, T>(tab, st, geo, U, src, nbr, base, t, F1, F2);
     __syncthreads();
     // cell term, y pass in place: one thread per y line (cell, i, k)
     for (int t = threadIdx.x; t < 64 * N2; t += TT) {
@@ -698,8 +715,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
       T c = T(0), d = T(0);
 #pragma unroll
       for (int m = 0; m < N; ++m) {
-        c += tab.K1[i * N + m] * A[row + m];
-        d += tab.M1[i * N + m] * B[row + m];
+        c += st.K1[i * N + m] * A[row + m];
+        d += st.M1[i * N + m] * B[row + m];
       }
       U[ct * CS + l] = cx * c + d;
     }
@@ -708,7 +725,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
     T *td = dst + base * N3;
     for (int e = threadIdx.x; e < 64 * N3; e += TT) {
       const int ct = e / N3, l = e - ct * N3;
-      td[e] = U[ct * CS + l] + tile_node_faces<N, T>(tab, NF, F1, F2, ct, l);
+      td[e] = U[ct * CS + l] + tile_node_faces<N, T>(st, NF, F1, F2, ct, l);
     }
     __syncthreads();
   }
