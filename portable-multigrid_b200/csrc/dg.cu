@@ -646,28 +646,59 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
                                                                      const int32_t *__restrict__ nbr, int64_t n_tiles) {
   static_assert(tile_shuffles<N>(), "the fused tile kernel applies the face mass on shuffles");
   constexpr int N2 = N * N, N3 = N2 * N, CS = tile_cell_stride<N>(), NP = kTileFaces * N2;
+  // the block size is a multiple of N^3: every thread keeps one node position (l) in the node
+  // passes and one line position (r) in the line passes, for cells ct0 + k * (TT / N^3) and
+  // ct1 + k * (TT / N^2), so the index arithmetic and the table rows of its position are
+  // computed once
+  static_assert(TT % N3 == 0, "block size");
+  constexpr int CN = TT / N3, CL = TT / N2;                  // cells per sweep of a pass
+  constexpr int QN = (64 + CN - 1) / CN, QL = (64 + CL - 1) / CL; // sweeps (the last may be partial)
   extern __shared__ __align__(16) unsigned char dg_tile_raw[];
   int *NF = reinterpret_cast<int *>(dg_tile_raw);
   T *F1 = reinterpret_cast<T *>(dg_tile_raw + sizeof(int) * 384), *F2 = F1 + NP;
   T *U = F2 + NP;       // the tile's values, then the cell term
-  T *A = U + 64 * CS;   // z-pass M1 u, then the y-pass P = M1 M1 u, then (x-pass input)
-  T *B = A + 64 * CS;   // z-pass K1 u, then the y-pass S = cy K1 M1 u + cz M1 K1 u
-  const T cx = (T)(geo.h[1] * geo.h[2] / geo.h[0]), cy = (T)(geo.h[0] * geo.h[2] / geo.h[1]),
-          cz = (T)(geo.h[0] * geo.h[1] / geo.h[2]);
+  T *A = U + 64 * CS;   // z pass M1 u, then the y pass P = M1 M1 u
+  T *B = A + 64 * CS;   // z pass K1 u, then the y pass S = cy K1 M1 u + cz M1 K1 u
   __shared__ DGTab<N, T> st;
   load_tab_shared(st, tab);
   fill_node_faces<N, TT>(NF);
+  const T cx = (T)(geo.h[1] * geo.h[2] / geo.h[0]), cy = (T)(geo.h[0] * geo.h[2] / geo.h[1]),
+          cz = (T)(geo.h[0] * geo.h[1] / geo.h[2]);
+  // this thread's node position l = (iz N + iy) N + ix and line position r
+  const int l = threadIdx.x % N3, ct0 = threadIdx.x / N3;
+  const int r = threadIdx.x % N2, ct1 = threadIdx.x / N2;
+  const int idx[3] = {l % N, (l / N) % N, l / N2};
+  T kx[N], mx[N]; // rows ix of K1 and M1 (x pass)
+#pragma unroll
+  for (int m = 0; m < N; ++m) {
+    kx[m] = tab.K1[idx[0] * N + m];
+    mx[m] = tab.M1[idx[0] * N + m];
+  }
+  int off[6];      // the node's face point within each of its six faces
+  T dph[6];        // the normal-derivative test of the node for each face
+  bool lay[6];     // the node lies on the face layer
+#pragma unroll
+  for (int F = 0; F < 6; ++F) {
+    const int d = F >> 1, sd = F & 1;
+    const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+    off[F] = idx[tb] * N + idx[ta];
+    dph[F] = sd ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]];
+    lay[F] = idx[d] == (sd ? N - 1 : 0);
+  }
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
     const T *ts = src + base * N3;
-    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
-      const int ct = e / N3;
-      U[ct * CS + (e - ct * N3)] = ts[e];
+#pragma unroll
+    for (int k = 0; k < QN; ++k) {
+      const int ct = ct0 + k * CN;
+      if (ct < 64) U[ct * CS + l] = ts[ct * N3 + l];
     }
     __syncthreads();
-    // cell term, z pass: one thread per z line (cell, i, j)
-    for (int t = threadIdx.x; t < 64 * N2; t += TT) {
-      const int ct = t / N2, o = ct * CS + (t - ct * N2); // (j N + i) within the cell
+    // cell term, z pass: line r = j N + i of each cell
+#pragma unroll
+    for (int q = 0; q < QL; ++q) {
+      if (ct1 + q * CL >= 64) break;
+      const int o = (ct1 + q * CL) * CS + r;
       T v[N];
 #pragma unroll
       for (int k = 0; k < N; ++k) v[k] = U[o + k * N2];
@@ -686,46 +717,61 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
     // face fluxes and face mass (phases 1-3 of the tile kernel)
     for (int t = threadIdx.x; t < NP; t += TT) tile_face_point_shfl<N, T>(tab, st, geo, U, src, nbr, base, t, F1, F2);
     __syncthreads();
-    // cell term, y pass in place: one thread per y line (cell, i, k)
-    for (int t = threadIdx.x; t < 64 * N2; t += TT) {
-      const int ct = t / N2, r = t - ct * N2, i = r % N, k = r / N, o = ct * CS + k * N2 + i;
-      T a[N], b[N];
+    // cell term, y pass in place: line r = k N + i of each cell
+#pragma unroll
+    for (int q = 0; q < QL; ++q) {
+      if (ct1 + q * CL >= 64) break;
+      const int o = (ct1 + q * CL) * CS + (r / N) * N2 + (r % N);
+      T av[N], bv[N];
 #pragma unroll
       for (int j = 0; j < N; ++j) {
-        a[j] = A[o + j * N];
-        b[j] = B[o + j * N];
+        av[j] = A[o + j * N];
+        bv[j] = B[o + j * N];
       }
 #pragma unroll
       for (int j = 0; j < N; ++j) {
         T pp = T(0), qa = T(0), qb = T(0);
 #pragma unroll
         for (int m = 0; m < N; ++m) {
-          pp += tab.M1[j * N + m] * a[m];
-          qa += tab.K1[j * N + m] * a[m];
-          qb += tab.M1[j * N + m] * b[m];
+          pp += tab.M1[j * N + m] * av[m];
+          qa += tab.K1[j * N + m] * av[m];
+          qb += tab.M1[j * N + m] * bv[m];
         }
         A[o + j * N] = pp;
         B[o + j * N] = cy * qa + cz * qb;
       }
     }
     __syncthreads();
-    // cell term, x pass: one thread per node, into the tile array (its values are read)
-    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
-      const int ct = e / N3, l = e - ct * N3, i = l % N, row = ct * CS + (l - i);
+    // cell term, x pass: this thread's node of each cell, into the tile array (read by now)
+#pragma unroll
+    for (int k = 0; k < QN; ++k) {
+      if (ct0 + k * CN >= 64) break;
+      const int row = (ct0 + k * CN) * CS + (l - idx[0]);
       T c = T(0), d = T(0);
 #pragma unroll
       for (int m = 0; m < N; ++m) {
-        c += st.K1[i * N + m] * A[row + m];
-        d += st.M1[i * N + m] * B[row + m];
+        c += kx[m] * A[row + m];
+        d += mx[m] * B[row + m];
       }
-      U[ct * CS + l] = cx * c + d;
+      U[row + idx[0]] = cx * c + d;
     }
     __syncthreads();
-    // cell plus face terms into dst
+    // cell plus face terms into dst, the six faces in a fixed order
     T *td = dst + base * N3;
-    for (int e = threadIdx.x; e < 64 * N3; e += TT) {
-      const int ct = e / N3, l = e - ct * N3;
-      td[e] = U[ct * CS + l] + tile_node_faces<N, T>(st, NF, F1, F2, ct, l);
+#pragma unroll
+    for (int k = 0; k < QN; ++k) {
+      const int ct = ct0 + k * CN;
+      if (ct >= 64) break;
+      const int *nf = NF + ct * 6;
+      T v = U[ct * CS + l];
+#pragma unroll
+      for (int F = 0; F < 6; ++F) {
+        const int x = nf[F];
+        const int pab = (x >> 1) + off[F];
+        v += F2[pab] * dph[F];
+        if (lay[F]) v += (x & 1) ? -F1[pab] : F1[pab];
+      }
+      td[ct * N3 + l] = v;
     }
     __syncthreads();
   }
