@@ -639,6 +639,68 @@ template <int N, typename T> constexpr size_t dg_fused_smem() {
   return sizeof(int) * 384 + sizeof(T) * (size_t(2) * kTileFaces * N * N + size_t(3) * 64 * tile_cell_stride<N>());
 }
 
+// the fluxes of face f of direction D at this thread's face point, whose node offsets within
+// a cell are fb + i * stride(D) (fb = the point's node on layer 0); as tile_flux
+template <int N, typename T, int D>
+__device__ __forceinline__ void tile_flux_at(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ U,
+                                             const T *__restrict__ src, const int32_t *__restrict__ nbr, int64_t base,
+                                             int f, int tan_f, int fb, T &f1, T &f2) {
+  constexpr int N3 = N * N * N, CS = tile_cell_stride<N>(), SD = D == 0 ? 1 : (D == 1 ? N : N * N);
+  // tile cell (x, y, z) -> index: bit interleaving (tile_index); `tan_f` is the face's
+  // tangential cell position (c_ta + 4 c_tb) and f its along position / surface side
+  constexpr int ta = D == 0 ? 1 : 0, tb = D == 2 ? 1 : 2;
+  const T h = (T)geo.h[D], area = (T)(geo.h[ta] * geo.h[tb]), sigma = (T)(geo.c_pen / geo.h[D]);
+  int c[3];
+  c[ta] = tan_f & 3;
+  c[tb] = tan_f >> 2;
+  f1 = T(0);
+  f2 = T(0);
+  if (f < 48) {
+    c[D] = f >> 4;
+    const T *ul = U + tile_index(c[0], c[1], c[2]) * CS + fb;
+    c[D] += 1;
+    const T *uu = U + tile_index(c[0], c[1], c[2]) * CS + fb;
+    T dn = T(0), dnn = T(0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      dn += tab.dphi1[i] * ul[i * SD];
+      dnn += tab.dphi0[i] * uu[i * SD];
+    }
+    const T jump = ul[(N - 1) * SD] - uu[0];
+    f1 = sigma * jump - T(0.5) * (dn + dnn) / h;
+    f2 = T(-0.5) * jump;
+  } else {
+    const int sd = f >= 64, F = 2 * D + sd;
+    c[D] = sd ? 3 : 0;
+    const int in = tile_index(c[0], c[1], c[2]);
+    const T *uo = U + in * CS + fb;
+    const T sgn_h = (sd ? T(1) : T(-1)) / h;
+    T dn = T(0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) dn += (sd ? tab.dphi1[i] : tab.dphi0[i]) * uo[i * SD];
+    dn *= sgn_h;
+    const T vo = sd ? uo[(N - 1) * SD] : uo[0];
+    const int32_t nb = __ldg(nbr + (base + in) * 6 + F);
+    if (nb >= 0) {
+      const T *un = src + int64_t(nb) * N3 + fb;
+      T dnn = T(0), line[N];
+#pragma unroll
+      for (int i = 0; i < N; ++i) line[i] = __ldg(un + i * SD);
+#pragma unroll
+      for (int i = 0; i < N; ++i) dnn += (sd ? tab.dphi0[i] : tab.dphi1[i]) * line[i];
+      dnn *= sgn_h;
+      const T jump = vo - (sd ? line[0] : line[N - 1]);
+      f1 = sigma * jump - T(0.5) * (dn + dnn);
+      f2 = T(-0.5) * jump;
+    } else if ((geo.dirichlet >> F) & 1) {
+      f1 = sigma * T(2) * vo - dn;
+      f2 = -vo;
+    }
+  }
+  f1 *= area;
+  f2 *= area;
+}
+
 template <int N, typename T, int TT>
 __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __grid_constant__ DGTab<N, T> tab,
                                                                      const __grid_constant__ DGGeo geo,
@@ -653,6 +715,10 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
   static_assert(TT % N3 == 0, "block size");
   constexpr int CN = TT / N3, CL = TT / N2;                  // cells per sweep of a pass
   constexpr int QN = (64 + CN - 1) / CN, QL = (64 + CL - 1) / CL; // sweeps (the last may be partial)
+  // a warp's lanes take 32 / N^2 consecutive faces, and 240 is a multiple of that: the bound
+  // of the face loop is the same for every lane of a warp, so its shuffles see full warps
+  static_assert(kTileFaces % (32 / N2) == 0, "warp-uniform face loop");
+  constexpr int QF = (kTileFaces + CL - 1) / CL;
   extern __shared__ __align__(16) unsigned char dg_tile_raw[];
   int *NF = reinterpret_cast<int *>(dg_tile_raw);
   T *F1 = reinterpret_cast<T *>(dg_tile_raw + sizeof(int) * 384), *F2 = F1 + NP;
@@ -668,23 +734,47 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
   const int l = threadIdx.x % N3, ct0 = threadIdx.x / N3;
   const int r = threadIdx.x % N2, ct1 = threadIdx.x / N2;
   const int idx[3] = {l % N, (l / N) % N, l / N2};
-  T kx[N], mx[N]; // rows ix of K1 and M1 (x pass)
-#pragma unroll
-  for (int m = 0; m < N; ++m) {
-    kx[m] = tab.K1[idx[0] * N + m];
-    mx[m] = tab.M1[idx[0] * N + m];
-  }
+  // this thread's face point (a, b) = (r mod N, r / N) in every face it evaluates: the
+  // face's first lane and the layer-0 node of the point per direction
+  const int fa = r % N, fbb = r / N, lane0 = (threadIdx.x & 31) - r;
+  const int fb0 = face_node<N>(0, 0, fa, fbb), fb1 = face_node<N>(1, 0, fa, fbb), fb2 = face_node<N>(2, 0, fa, fbb);
+  // the table rows of its positions (x-pass rows of K1 and M1, face-mass rows of a and b, the
+  // node's normal-derivative tests) held in registers in FP32; in FP64 they would exceed
+  // the 64 registers a thread has and are read from shared memory instead
+  constexpr bool HOLD = sizeof(T) == 4;
+  constexpr int HN = HOLD ? N : 1, H6 = HOLD ? 6 : 1;
+  T kx[HN], mx[HN], ma[HN], mb[HN], dph[H6];
   int off[6];      // the node's face point within each of its six faces
-  T dph[6];        // the normal-derivative test of the node for each face
   bool lay[6];     // the node lies on the face layer
 #pragma unroll
   for (int F = 0; F < 6; ++F) {
     const int d = F >> 1, sd = F & 1;
     const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
     off[F] = idx[tb] * N + idx[ta];
-    dph[F] = sd ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]];
     lay[F] = idx[d] == (sd ? N - 1 : 0);
   }
+  if constexpr (HOLD) {
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      kx[m] = tab.K1[idx[0] * N + m];
+      mx[m] = tab.M1[idx[0] * N + m];
+      ma[m] = tab.M1[fa * N + m];
+      mb[m] = tab.M1[fbb * N + m];
+    }
+#pragma unroll
+    for (int F = 0; F < 6; ++F) {
+      const int d = F >> 1;
+      dph[F] = (F & 1) ? tab.dphi1[idx[d]] : tab.dphi0[idx[d]];
+    }
+  }
+  auto KX = [&](int m) { if constexpr (HOLD) return kx[m]; else return st.K1[idx[0] * N + m]; };
+  auto MX = [&](int m) { if constexpr (HOLD) return mx[m]; else return st.M1[idx[0] * N + m]; };
+  auto MA = [&](int m) { if constexpr (HOLD) return ma[m]; else return st.M1[fa * N + m]; };
+  auto MB = [&](int m) { if constexpr (HOLD) return mb[m]; else return st.M1[fbb * N + m]; };
+  auto DPH = [&](int F) {
+    if constexpr (HOLD) return dph[F];
+    else return (F & 1) ? st.dphi1[idx[F >> 1]] : st.dphi0[idx[F >> 1]];
+  };
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * 64;
     const T *ts = src + base * N3;
@@ -714,8 +804,43 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
         B[o + k * N2] = sb;
       }
     }
-    // face fluxes and face mass (phases 1-3 of the tile kernel)
-    for (int t = threadIdx.x; t < NP; t += TT) tile_face_point_shfl<N, T>(tab, st, geo, U, src, nbr, base, t, F1, F2);
+    // face fluxes and face mass (phases 1-3 of the tile kernel): faces ct1 + q * CL, each on
+    // N^2 consecutive lanes of one warp; FP64 takes the generic loop (the unrolled one
+    // exceeds its registers)
+    if constexpr (!HOLD) {
+      for (int t = threadIdx.x; t < NP; t += TT) tile_face_point_shfl<N, T>(tab, st, geo, U, src, nbr, base, t, F1, F2);
+    } else
+#pragma unroll
+    for (int q = 0; q < QF; ++q) {
+      const int fi = ct1 + q * CL; // face 80 d + f
+      if (fi >= kTileFaces) break; // warp-uniform
+      T f1, f2;
+      if (fi < kDirFaces) {
+        tile_flux_at<N, T, 0>(tab, geo, U, src, nbr, base, fi, fi < 48 ? fi & 15 : (fi - 48) & 15, fb0, f1, f2);
+      } else if (fi < 2 * kDirFaces) {
+        const int f = fi - kDirFaces;
+        tile_flux_at<N, T, 1>(tab, geo, U, src, nbr, base, f, f < 48 ? f & 15 : (f - 48) & 15, fb1, f1, f2);
+      } else {
+        const int f = fi - 2 * kDirFaces;
+        tile_flux_at<N, T, 2>(tab, geo, U, src, nbr, base, f, f < 48 ? f & 15 : (f - 48) & 15, fb2, f1, f2);
+      }
+      T g1 = T(0), g2 = T(0);
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        g1 += MA(k) * __shfl_sync(0xffffffffu, f1, lane0 + fbb * N + k);
+        g2 += MA(k) * __shfl_sync(0xffffffffu, f2, lane0 + fbb * N + k);
+      }
+      T tv = T(0), tn = T(0);
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        tv += MB(k) * __shfl_sync(0xffffffffu, g1, lane0 + k * N + fa);
+        tn += MB(k) * __shfl_sync(0xffffffffu, g2, lane0 + k * N + fa);
+      }
+      const int d = fi / kDirFaces, f = fi - d * kDirFaces;
+      const T sg = (f >= 48 && f < 64) ? T(-1) : T(1);
+      F1[fi * N2 + r] = tv;
+      F2[fi * N2 + r] = tn * sg / (T)geo.h[d];
+    }
     __syncthreads();
     // cell term, y pass in place: line r = k N + i of each cell
 #pragma unroll
@@ -750,8 +875,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
       T c = T(0), d = T(0);
 #pragma unroll
       for (int m = 0; m < N; ++m) {
-        c += kx[m] * A[row + m];
-        d += mx[m] * B[row + m];
+        c += KX(m) * A[row + m];
+        d += MX(m) * B[row + m];
       }
       U[row + idx[0]] = cx * c + d;
     }
@@ -768,7 +893,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
       for (int F = 0; F < 6; ++F) {
         const int x = nf[F];
         const int pab = (x >> 1) + off[F];
-        v += F2[pab] * dph[F];
+        v += F2[pab] * DPH(F);
         if (lay[F]) v += (x & 1) ? -F1[pab] : F1[pab];
       }
       td[ct * N3 + l] = v;
