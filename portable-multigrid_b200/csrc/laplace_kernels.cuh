@@ -20,9 +20,10 @@
 //    No block-wide barrier is used; warps are independent.
 //  * The index map and G are stored lane-contiguous per group ([group][point][lane]), so
 //    every load of them is a fully coalesced warp access; G is column-major per group (one
-//    contiguous chunk per x point), each warp bulk-prefetches the next group's G into L2
-//    (cp.async.bulk.prefetch.L2) and streams the columns of the current group through a
-//    two-slot shared-memory ring filled by TMA bulk copies one column ahead.
+//    contiguous chunk per x point). The ring variant streams the columns of the current
+//    group through a two-slot shared-memory ring filled by TMA bulk copies one column ahead;
+//    the direct-load variant bulk-prefetches the next group's G into L2
+//    (cp.async.bulk.prefetch.L2) instead.
 //  * Scatter with native FP64/FP32 atomic adds (red.global.add) into L2.
 //  * The 1D tables are kernel parameters (constant bank), indexed at compile time.
 #pragma once
@@ -135,6 +136,12 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
 __device__ __forceinline__ uint64_t policy_evict_last() {
   uint64_t p;
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint64_t policy_evict_normal() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
 
@@ -281,6 +288,15 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
 #endif
 #ifndef PMG_VMULT_EO_PHASE1X
 #define PMG_VMULT_EO_PHASE1X -1
+#endif
+// L2 prefetch of the next group's geometry (full and inverse-Jacobian layouts): -1 the tuned
+// default, 1 evict-first, 0 none, 2 evict-normal.  The default prefetches (evict-first) for the
+// direct-load variants only: the ring variant streams each column through its TMA ring
+// already, and the extra prefetch only added L2 traffic (deformed cube on B200, FP64 128^3:
+// Q4 3914-3968 -> 3721-3737 us, Q5 at 64^3 1188 -> 1157 us, Q3 unchanged without it; FP32 Q4
+// with direct loads 2156 -> 2430-2497 us without it)
+#ifndef PMG_VMULT_PREFETCH
+#define PMG_VMULT_PREFETCH -1
 #endif
 template <int N> struct Stride {
   // per-cell stride of the exchange buffers, padded where that lowers bank conflicts of
@@ -526,8 +542,10 @@ __global__ void __launch_bounds__(SMEM_G ? 256 : 128, (SMEM_G ? 1 : MinBlocks<N,
   }
 
   for (int64_t g = warp0; g < n_groups; g += nwarps, ++it) {
-    if ((GEOM == 0 || GEOM == 3) && lane == 0 && g + nwarps < n_groups)
-      prefetch_l2(geo + (g + nwarps) * (N2 * NCOMP * LANES), N2 * NCOMP * LANES * sizeof(T), pol_first);
+    constexpr bool PREFETCH = PMG_VMULT_PREFETCH == -1 ? !SMEM_G : PMG_VMULT_PREFETCH != 0;
+    if ((GEOM == 0 || GEOM == 3) && PREFETCH && lane == 0 && g + nwarps < n_groups)
+      prefetch_l2(geo + (g + nwarps) * (N2 * NCOMP * LANES), N2 * NCOMP * LANES * sizeof(T),
+                  PMG_VMULT_PREFETCH == 2 ? policy_evict_normal() : pol_first);
     const uint32_t *ig = idx + g * (N2 * LANES) + lane;
     const int slot = it & 1;
 
