@@ -99,17 +99,19 @@ inline int pipe_override() {
   }();
   return v;
 }
-// Defaults from B200 sweeps (cell kernel time, 48^3..128^3 meshes): the register pipeline
-// (3) for the FP64 ring variant at N = 4, 5 (deformed cube 128^3: Q4 4255 -> 4042 us, Q3
-// 1918 -> 1797 us); the shared-memory index pipeline (1) for the FP64 ring variant at N >= 6
-// (Q5 +18 %; the register pipeline there: 1186 -> 1428 us) and for the FP32 Q6 affine kernel
-// (+9 %; register pipeline 356 -> 435 us); none elsewhere (FP32 full geometry Q4 with the
-// register pipeline 2160 -> 2307 us, with the index pipeline 2415 us; Q4/Q5 affine and FP64
-// Q6 affine lose 15-35 % with the index pipeline).
+// Defaults from B200 sweeps (cell kernel time, 48^3..128^3 meshes), for the FP64 ring variant
+// without the L2 prefetch: the register pipeline (3) at N = 4 (deformed cube 128^3: Q3 1895 ->
+// 1758-1798 us); none at N = 5 (Q4: 3734-3764 us against 3803-3837 us with the register
+// pipeline, which was ahead, 4255 -> 4042 us, while the ring variant still prefetched); the
+// shared-memory index pipeline (1) at N = 3 (Q2 677 -> 657 us) and N >= 6 (Q5 +18 %; the
+// register pipeline there: 1186 -> 1428 us); and the index pipeline for the FP32 Q6 affine
+// kernel (+9 %; register pipeline 356 -> 435 us); none elsewhere (FP32 full geometry Q4 with
+// the register pipeline 2160 -> 2307 us, with the index pipeline 2415 us; Q4/Q5 affine and
+// FP64 Q6 affine lose 15-35 % with the index pipeline).
 template <typename T, int GEOM, bool SG> int use_pipe() {
   const int o = pipe_override();
   if (o >= 0 && o <= 3) return o;
-  if (SG) return sizeof(T) == 8 ? (kN >= 6 ? 1 : (kN >= 4 ? 3 : 0)) : 0;
+  if (SG) return sizeof(T) == 8 ? ((kN >= 6 || kN == 3) ? 1 : (kN == 4 ? 3 : 0)) : 0;
   if ((GEOM == 1 || GEOM == 2) && kN == 7 && sizeof(T) == 4) return 1;
   return 0;
 }
