@@ -54,10 +54,10 @@ CASES = [
     ("q5_deformed_24", dict(coarse=(3, 3, 3), refine=3, deform=1), 5, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
     ("q6_affine_kappa_24", dict(coarse=(3, 3, 3), refine=3), 6, pmg.GEOMETRY_AFFINE, pmg.COEFF_KAPPA),
     ("q4_invjac_32", dict(refine=5, deform=1), 4, pmg.GEOMETRY_INVJAC, pmg.COEFF_NONE),
-    # Q2 on the deformed 64^3 cube (FP64: ring with the index pipeline) and Q3 on 32^3 (FP64:
+    # Q2 on the deformed 64^3 cube (FP64: ring with the index pipeline) and Q3 on 64^3 (FP64:
     # ring with the register pipeline)
     ("q2_deformed_64", dict(refine=6, deform=1), 2, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
-    ("q3_deformed_32", dict(refine=5, deform=1), 3, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
+    ("q3_deformed_64", dict(refine=6, deform=1), 3, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
 ]
 
 
