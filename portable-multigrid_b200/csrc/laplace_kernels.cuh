@@ -293,8 +293,9 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
 // default, 1 evict-first, 0 none, 2 evict-normal.  The default prefetches (evict-first) for the
 // direct-load variants only: the ring variant streams each column through its TMA ring
 // already, and the extra prefetch only added L2 traffic (deformed cube on B200, FP64 128^3:
-// Q4 3914-3968 -> 3721-3737 us, Q5 at 64^3 1188 -> 1157 us, Q3 unchanged without it; FP32 Q4
-// with direct loads 2156 -> 2430-2497 us without it)
+// Q4 3914-3968 -> 3721-3737 us, Q5 at 64^3 1188 -> 1157 us, Q3 unchanged without it; FP32
+// ring variants Q3 972 -> 914 us, Q2 398 -> 381 us; FP32 Q4 with direct loads 2156 ->
+// 2430-2497 us without it)
 #ifndef PMG_VMULT_PREFETCH
 #define PMG_VMULT_PREFETCH -1
 #endif
