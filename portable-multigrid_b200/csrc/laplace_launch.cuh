@@ -75,9 +75,10 @@ template <typename K> void allow_smem(K kernel, size_t bytes) {
 }
 
 // Full geometry streams through the shared-memory column ring (TMA) where that measured faster
-// on B200 (deformed-cube sweeps at 64^3/128^3): FP64 degrees 1-5 and FP32 degrees 2-3; FP32
-// degrees 1, 4, 5, 6 (whose register-heavy unrolled forms hide the latency at 8 warps/SM) and
-// FP64 degree 6 load it directly.
+// on B200 (deformed-cube sweeps at 64^3/128^3): FP64 degrees 1-5 and FP32 degrees 2, 3, 5, 6
+// (FP32 Q5 64^3 621 -> 563 us, Q6 1236 -> 1135 us once the ring no longer prefetched into L2);
+// FP32 degrees 1 and 4 (whose unrolled forms hide the latency at 8 warps/SM: Q4 128^3 2158
+// against 2427 us with the ring) and FP64 degree 6 (2372 against 2488 us) load it directly.
 // PMG_VMULT_STAGE=0 / 1 forces direct loads / the ring (a tuning switch; both are compiled).
 inline int stage_override() {
   static const int v = [] {
@@ -89,7 +90,7 @@ inline int stage_override() {
 template <typename T> bool use_ring() {
   const int o = stage_override();
   if (o == 0 || o == 1) return o == 1;
-  return sizeof(T) == 8 ? kN != 7 : (kN == 3 || kN == 4);
+  return sizeof(T) == 8 ? kN != 7 : (kN != 2 && kN != 5);
 }
 // gather pipeline (PIPE template parameter); PMG_VMULT_PIPE=0/1/2/3 overrides
 inline int pipe_override() {
