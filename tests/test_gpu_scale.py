@@ -58,6 +58,9 @@ CASES = [
     # ring with the register pipeline)
     ("q2_deformed_64", dict(refine=6, deform=1), 2, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
     ("q3_deformed_64", dict(refine=6, deform=1), 3, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
+    # Q6 full geometry on the deformed 24^3 cube (FP32: ring; FP64: direct loads with the L2
+    # prefetch of the next group)
+    ("q6_deformed_24", dict(coarse=(3, 3, 3), refine=3, deform=1), 6, pmg.GEOMETRY_FULL, pmg.COEFF_NONE),
 ]
 
 
