@@ -634,18 +634,28 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
 // tile in shared memory (z by lines into A and B, y by lines in place, x by nodes into the tile
 // array once the faces have read it), and the face terms as in dg_face_tile_kernel; phase 4
 // stores cell plus face terms: src is read once, dst written once, no index map, no zeroing.
-template <int N> constexpr int fused_cell_stride() { return tile_cell_stride<N>(); }
+// Shared-memory layout of a cell in the fused kernel: node (i, j, k) at k PZ + j N + i, cell
+// stride CS.  FP32 at N = 4 pads each z plane to 20 entries and the cell to 80: the two cells
+// a warp covers in a line pass then fall on the two halves of the 32 banks, and the 16 lines
+// of a y pass (planes 20 apart) on distinct banks.  Elsewhere planes of N^2 and a cell stride
+// of N^3 + 1.
+template <int N, typename T> struct FusedLayout {
+  static constexpr bool PAD = sizeof(T) == 4 && N == 4;
+  static constexpr int PZ = PAD ? N * N + 4 : N * N;
+  static constexpr int CS = PAD ? N * PZ : N * N * N + 1;
+};
 template <int N, typename T> constexpr size_t dg_fused_smem() {
-  return sizeof(int) * 384 + sizeof(T) * (size_t(2) * kTileFaces * N * N + size_t(3) * 64 * tile_cell_stride<N>());
+  return sizeof(int) * 384 + sizeof(T) * (size_t(2) * kTileFaces * N * N + size_t(3) * 64 * FusedLayout<N, T>::CS);
 }
 
 // the fluxes of face f of direction D at this thread's face point, whose node offsets within
-// a cell are fb + i * stride(D) (fb = the point's node on layer 0); as tile_flux
-template <int N, typename T, int D>
+// a cell are fb + i * stride(D) in the tile's layout (cell stride CS, z planes PZ apart) and
+// fbg + i * stride(D) in memory (fb, fbg = the point's node on layer 0); as tile_flux
+template <int N, typename T, int D, int CS, int PZ>
 __device__ __forceinline__ void tile_flux_at(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ U,
                                              const T *__restrict__ src, const int32_t *__restrict__ nbr, int64_t base,
-                                             int f, int tan_f, int fb, T &f1, T &f2) {
-  constexpr int N3 = N * N * N, CS = tile_cell_stride<N>(), SD = D == 0 ? 1 : (D == 1 ? N : N * N);
+                                             int f, int tan_f, int fb, int fbg, T &f1, T &f2) {
+  constexpr int N3 = N * N * N, SD = D == 0 ? 1 : (D == 1 ? N : PZ), SG = D == 0 ? 1 : (D == 1 ? N : N * N);
   // tile cell (x, y, z) -> index: bit interleaving (tile_index); `tan_f` is the face's
   // tangential cell position (c_ta + 4 c_tb) and f its along position / surface side
   constexpr int ta = D == 0 ? 1 : 0, tb = D == 2 ? 1 : 2;
@@ -682,10 +692,10 @@ __device__ __forceinline__ void tile_flux_at(const DGTab<N, T> &tab, const DGGeo
     const T vo = sd ? uo[(N - 1) * SD] : uo[0];
     const int32_t nb = __ldg(nbr + (base + in) * 6 + F);
     if (nb >= 0) {
-      const T *un = src + int64_t(nb) * N3 + fb;
+      const T *un = src + int64_t(nb) * N3 + fbg;
       T dnn = T(0), line[N];
 #pragma unroll
-      for (int i = 0; i < N; ++i) line[i] = __ldg(un + i * SD);
+      for (int i = 0; i < N; ++i) line[i] = __ldg(un + i * SG);
 #pragma unroll
       for (int i = 0; i < N; ++i) dnn += (sd ? tab.dphi0[i] : tab.dphi1[i]) * line[i];
       dnn *= sgn_h;
@@ -707,7 +717,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
                                                                      const T *__restrict__ src, T *__restrict__ dst,
                                                                      const int32_t *__restrict__ nbr, int64_t n_tiles) {
   static_assert(tile_shuffles<N>(), "the fused tile kernel applies the face mass on shuffles");
-  constexpr int N2 = N * N, N3 = N2 * N, CS = tile_cell_stride<N>(), NP = kTileFaces * N2;
+  constexpr int N2 = N * N, N3 = N2 * N, NP = kTileFaces * N2;
+  constexpr int CS = FusedLayout<N, T>::CS, PZ = FusedLayout<N, T>::PZ; // cell stride, z-plane stride
   // the block size is a multiple of N^3: every thread keeps one node position (l) in the node
   // passes and one line position (r) in the line passes, for cells ct0 + k * (TT / N^3) and
   // ct1 + k * (TT / N^2), so the index arithmetic and the table rows of its position are
@@ -734,15 +745,21 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
   const int l = threadIdx.x % N3, ct0 = threadIdx.x / N3;
   const int r = threadIdx.x % N2, ct1 = threadIdx.x / N2;
   const int idx[3] = {l % N, (l / N) % N, l / N2};
+  const int sl = idx[2] * PZ + idx[1] * N + idx[0]; // the node's place in the tile layout
   // this thread's face point (a, b) = (r mod N, r / N) in every face it evaluates: the
   // face's first lane and the layer-0 node of the point per direction
   const int fa = r % N, fbb = r / N, lane0 = (threadIdx.x & 31) - r;
-  const int fb0 = face_node<N>(0, 0, fa, fbb), fb1 = face_node<N>(1, 0, fa, fbb), fb2 = face_node<N>(2, 0, fa, fbb);
+  // layer-0 node of the face point: in memory (k N^2 + j N + i) and in the tile layout
+  const int fg0 = face_node<N>(0, 0, fa, fbb), fg1 = face_node<N>(1, 0, fa, fbb), fg2 = face_node<N>(2, 0, fa, fbb);
+  auto tile_off = [](int g) { return (g / (N * N)) * PZ + g % (N * N); };
+  const int fb0 = tile_off(fg0), fb1 = tile_off(fg1), fb2 = tile_off(fg2);
   // the table rows of its positions (x-pass rows of K1 and M1, face-mass rows of a and b, the
   // node's normal-derivative tests) held in registers in FP32; in FP64 they would exceed
   // the 64 registers a thread has and are read from shared memory instead
   constexpr bool HOLD = sizeof(T) == 4;
   constexpr int HN = HOLD ? N : 1, H6 = HOLD ? 6 : 1;
+  // the generic face loop (FP64) reads the tile in the plain layout of the tile kernel
+  static_assert(HOLD || (CS == tile_cell_stride<N>() && PZ == N2), "tile layout");
   T kx[HN], mx[HN], ma[HN], mb[HN], dph[H6];
   int off[6];      // the node's face point within each of its six faces
   bool lay[6];     // the node lies on the face layer
@@ -781,7 +798,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
 #pragma unroll
     for (int k = 0; k < QN; ++k) {
       const int ct = ct0 + k * CN;
-      if (ct < 64) U[ct * CS + l] = ts[ct * N3 + l];
+      if (ct < 64) U[ct * CS + sl] = ts[ct * N3 + l];
     }
     __syncthreads();
     // cell term, z pass: line r = j N + i of each cell
@@ -791,7 +808,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
       const int o = (ct1 + q * CL) * CS + r;
       T v[N];
 #pragma unroll
-      for (int k = 0; k < N; ++k) v[k] = U[o + k * N2];
+      for (int k = 0; k < N; ++k) v[k] = U[o + k * PZ];
 #pragma unroll
       for (int k = 0; k < N; ++k) {
         T sa = T(0), sb = T(0);
@@ -800,8 +817,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
           sa += tab.M1[k * N + m] * v[m];
           sb += tab.K1[k * N + m] * v[m];
         }
-        A[o + k * N2] = sa;
-        B[o + k * N2] = sb;
+        A[o + k * PZ] = sa;
+        B[o + k * PZ] = sb;
       }
     }
     // face fluxes and face mass (phases 1-3 of the tile kernel): faces ct1 + q * CL, each on
@@ -816,13 +833,16 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
       if (fi >= kTileFaces) break; // warp-uniform
       T f1, f2;
       if (fi < kDirFaces) {
-        tile_flux_at<N, T, 0>(tab, geo, U, src, nbr, base, fi, fi < 48 ? fi & 15 : (fi - 48) & 15, fb0, f1, f2);
+        tile_flux_at<N, T, 0, CS, PZ>(tab, geo, U, src, nbr, base, fi, fi < 48 ? fi & 15 : (fi - 48) & 15, fb0, fg0,
+                                      f1, f2);
       } else if (fi < 2 * kDirFaces) {
         const int f = fi - kDirFaces;
-        tile_flux_at<N, T, 1>(tab, geo, U, src, nbr, base, f, f < 48 ? f & 15 : (f - 48) & 15, fb1, f1, f2);
+        tile_flux_at<N, T, 1, CS, PZ>(tab, geo, U, src, nbr, base, f, f < 48 ? f & 15 : (f - 48) & 15, fb1, fg1, f1,
+                                      f2);
       } else {
         const int f = fi - 2 * kDirFaces;
-        tile_flux_at<N, T, 2>(tab, geo, U, src, nbr, base, f, f < 48 ? f & 15 : (f - 48) & 15, fb2, f1, f2);
+        tile_flux_at<N, T, 2, CS, PZ>(tab, geo, U, src, nbr, base, f, f < 48 ? f & 15 : (f - 48) & 15, fb2, fg2, f1,
+                                      f2);
       }
       T g1 = T(0), g2 = T(0);
 #pragma unroll
@@ -846,7 +866,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
 #pragma unroll
     for (int q = 0; q < QL; ++q) {
       if (ct1 + q * CL >= 64) break;
-      const int o = (ct1 + q * CL) * CS + (r / N) * N2 + (r % N);
+      const int o = (ct1 + q * CL) * CS + (r / N) * PZ + (r % N);
       T av[N], bv[N];
 #pragma unroll
       for (int j = 0; j < N; ++j) {
@@ -871,7 +891,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
 #pragma unroll
     for (int k = 0; k < QN; ++k) {
       if (ct0 + k * CN >= 64) break;
-      const int row = (ct0 + k * CN) * CS + (l - idx[0]);
+      const int row = (ct0 + k * CN) * CS + (sl - idx[0]);
       T c = T(0), d = T(0);
 #pragma unroll
       for (int m = 0; m < N; ++m) {
@@ -888,7 +908,7 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
       const int ct = ct0 + k * CN;
       if (ct >= 64) break;
       const int *nf = NF + ct * 6;
-      T v = U[ct * CS + l];
+      T v = U[ct * CS + sl];
 #pragma unroll
       for (int F = 0; F < 6; ++F) {
         const int x = nf[F];
