@@ -238,9 +238,11 @@ pmg_status pmg_operator_dof_lattice(const pmg_operator *op, int32_t *ijk);
 
 /* Shape of the last launch of one of the operator's grid-stride kernels (inspection; the
  * reference launches one Kokkos team per cell batch and has no counterpart): *units = the
- * work units (warp groups of cells; cell batches for the DG face kernel) and *parallel =
- * the warps (blocks for the DG face kernel) of the grid that shared them, so a launch with
- * units >= 2 * parallel gave every warp two or more units.  Zero before the first launch. */
+ * work units (warp groups of cells; cell batches or 4x4x4 cell tiles for the DG face
+ * kernels) and *parallel = the warps (blocks for the DG face kernels) of the grid that shared
+ * them, so a launch with units >= 2 * parallel gave every warp two or more units.  Where a DG
+ * vmult runs as one fused tile kernel (cell and face terms), both the VMULT_CELL and the
+ * DG_FACES records describe that launch.  Zero before the first launch. */
 #define PMG_KERNEL_VMULT_CELL 0 /* the cell kernel of vmult                              */
 #define PMG_KERNEL_DG_FACES 1   /* the face kernel of a DG vmult                         */
 #define PMG_KERNEL_MASS 2       /* the cell kernel of a mass-matrix vmult                */
