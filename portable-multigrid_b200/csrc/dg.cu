@@ -397,11 +397,20 @@ __device__ __forceinline__ int tile_index(int x, int y, int z) {
 // flux values (times the face area) of face f of direction D at face point (a, bb): f1 =
 // sigma [u] - {d_n u}, f2 = -[u]/2 with the normal +D inside the tile, the inside cell's
 // outward normal on the surface (Dirichlet: mirror u+ = -u-, d_n u+ = d_n u-)
-template <int N, typename T, int D>
+// face_node in a tile layout whose z planes are PZ entries apart
+template <int N, int PZ> __device__ __forceinline__ int face_node_t(int d, int layer, int a, int b) {
+  const int i = d == 0 ? layer : a;
+  const int j = d == 1 ? layer : (d == 0 ? a : b);
+  const int k = d == 2 ? layer : b;
+  return k * PZ + j * N + i;
+}
+
+// (the tile in shared memory: cell stride CS, z planes PZ apart; src in memory: N^3 per cell)
+template <int N, typename T, int D, int CS = tile_cell_stride<N>(), int PZ = N * N>
 __device__ __forceinline__ void tile_flux(const DGTab<N, T> &tab, const DGGeo &geo, const T *__restrict__ U,
                                           const T *__restrict__ src, const int32_t *__restrict__ nbr,
                                           int64_t base, int f, int a, int bb, T &f1, T &f2) {
-  constexpr int N3 = N * N * N, CS = tile_cell_stride<N>();
+  constexpr int N3 = N * N * N;
   constexpr int ta = D == 0 ? 1 : 0, tb = D == 2 ? 1 : 2;
   const T h = (T)geo.h[D], area = (T)(geo.h[ta] * geo.h[tb]), sigma = (T)(geo.c_pen / geo.h[D]);
   int c[3];
@@ -418,11 +427,11 @@ __device__ __forceinline__ void tile_flux(const DGTab<N, T> &tab, const DGGeo &g
     T dn = T(0), dnn = T(0);
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const int l = face_node<N>(D, i, a, bb);
+      const int l = face_node_t<N, PZ>(D, i, a, bb);
       dn += tab.dphi1[i] * ul[l];
       dnn += tab.dphi0[i] * uu[l];
     }
-    const T jump = ul[face_node<N>(D, N - 1, a, bb)] - uu[face_node<N>(D, 0, a, bb)];
+    const T jump = ul[face_node_t<N, PZ>(D, N - 1, a, bb)] - uu[face_node_t<N, PZ>(D, 0, a, bb)];
     f1 = sigma * jump - T(0.5) * (dn + dnn) / h;
     f2 = T(-0.5) * jump;
   } else {
@@ -435,9 +444,9 @@ __device__ __forceinline__ void tile_flux(const DGTab<N, T> &tab, const DGGeo &g
     const T sgn_h = (sd ? T(1) : T(-1)) / h;
     T dn = T(0);
 #pragma unroll
-    for (int i = 0; i < N; ++i) dn += (sd ? tab.dphi1[i] : tab.dphi0[i]) * uo[face_node<N>(D, i, a, bb)];
+    for (int i = 0; i < N; ++i) dn += (sd ? tab.dphi1[i] : tab.dphi0[i]) * uo[face_node_t<N, PZ>(D, i, a, bb)];
     dn *= sgn_h;
-    const T vo = sd ? uo[face_node<N>(D, N - 1, a, bb)] : uo[face_node<N>(D, 0, a, bb)];
+    const T vo = sd ? uo[face_node_t<N, PZ>(D, N - 1, a, bb)] : uo[face_node_t<N, PZ>(D, 0, a, bb)];
     const int32_t nb = __ldg(nbr + (base + in) * 6 + F);
     if (nb >= 0) {
       const T *un = src + int64_t(nb) * N3;
@@ -485,7 +494,7 @@ template <int N, int TT> __device__ __forceinline__ void fill_node_faces(int *NF
 // phase 1 of the tile kernels with the face mass on shuffles (N^2 divides 32): the fluxes of
 // face point t, then M1 x M1 over the face's N^2 lanes; F1 = the value-test coefficient, F2 =
 // the normal-derivative-test coefficient divided by h (on the lower surface times -1)
-template <int N, typename T>
+template <int N, typename T, int CS = tile_cell_stride<N>(), int PZ = N * N>
 __device__ __forceinline__ void tile_face_point_shfl(const DGTab<N, T> &tab, const DGTab<N, T> &st, const DGGeo &geo,
                                                      const T *__restrict__ U, const T *__restrict__ src,
                                                      const int32_t *__restrict__ nbr, int64_t base, int t, T *F1,
@@ -493,9 +502,9 @@ __device__ __forceinline__ void tile_face_point_shfl(const DGTab<N, T> &tab, con
   constexpr int N2 = N * N, DP = kDirFaces * N2;
   const int d = t / DP, r = t - d * DP, f = r / N2, ab = r - f * N2, a = ab % N, bb = ab / N;
   T f1, f2;
-  if (d == 0) tile_flux<N, T, 0>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
-  else if (d == 1) tile_flux<N, T, 1>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
-  else tile_flux<N, T, 2>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+  if (d == 0) tile_flux<N, T, 0, CS, PZ>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+  else if (d == 1) tile_flux<N, T, 1, CS, PZ>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
+  else tile_flux<N, T, 2, CS, PZ>(tab, geo, U, src, nbr, base, f, a, bb, f1, f2);
   const int lane0 = (threadIdx.x & 31) - ab; // the face's first lane
   T g1 = T(0), g2 = T(0);
 #pragma unroll
@@ -635,12 +644,12 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_face_tile_kernel(const __gri
 // array once the faces have read it), and the face terms as in dg_face_tile_kernel; phase 4
 // stores cell plus face terms: src is read once, dst written once, no index map, no zeroing.
 // Shared-memory layout of a cell in the fused kernel: node (i, j, k) at k PZ + j N + i, cell
-// stride CS.  FP32 at N = 4 pads each z plane to 20 entries and the cell to 80: the two cells
-// a warp covers in a line pass then fall on the two halves of the 32 banks, and the 16 lines
-// of a y pass (planes 20 apart) on distinct banks.  Elsewhere planes of N^2 and a cell stride
-// of N^3 + 1.
+// stride CS.  At N = 4 each z plane is padded to 20 entries and the cell to 80: in FP32 the two
+// cells a warp covers in a line pass then fall on the two halves of the 32 banks, and in both
+// types the 16 lines of a y pass (planes 20 apart) on distinct banks.  At N = 2 planes of
+// N^2 and a cell stride of N^3 + 1.
 template <int N, typename T> struct FusedLayout {
-  static constexpr bool PAD = sizeof(T) == 4 && N == 4;
+  static constexpr bool PAD = N == 4;
   static constexpr int PZ = PAD ? N * N + 4 : N * N;
   static constexpr int CS = PAD ? N * PZ : N * N * N + 1;
 };
@@ -758,8 +767,6 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
   // the 64 registers a thread has and are read from shared memory instead
   constexpr bool HOLD = sizeof(T) == 4;
   constexpr int HN = HOLD ? N : 1, H6 = HOLD ? 6 : 1;
-  // the generic face loop (FP64) reads the tile in the plain layout of the tile kernel
-  static_assert(HOLD || (CS == tile_cell_stride<N>() && PZ == N2), "tile layout");
   T kx[HN], mx[HN], ma[HN], mb[HN], dph[H6];
   int off[6];      // the node's face point within each of its six faces
   bool lay[6];     // the node lies on the face layer
@@ -825,7 +832,8 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
     // N^2 consecutive lanes of one warp; FP64 takes the generic loop (the unrolled one
     // exceeds its registers)
     if constexpr (!HOLD) {
-      for (int t = threadIdx.x; t < NP; t += TT) tile_face_point_shfl<N, T>(tab, st, geo, U, src, nbr, base, t, F1, F2);
+      for (int t = threadIdx.x; t < NP; t += TT)
+        tile_face_point_shfl<N, T, CS, PZ>(tab, st, geo, U, src, nbr, base, t, F1, F2);
     } else
 #pragma unroll
     for (int q = 0; q < QF; ++q) {
