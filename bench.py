@@ -537,7 +537,43 @@ def dg_time_to_solution(torch, pmg, dev, refine=6, repeats=3):
     res["n_dofs"] = n
     res["speedup_fp32_mg_over_fp64"] = res["fp64_mg"]["seconds"] / res["fp32_mg"]["seconds"]
     res["config"] = "DG-SIPG Q3, 64^3 cells, DG Q3 -> CG Q3 -> Q1 -> h-levels, Chebyshev(5)"
+    res["dg_vmult"] = dg_vmult_rates(torch, pmg, dev, refine)
     return res
+
+
+def dg_vmult_rates(torch, pmg, dev, refine=6, launches=20, peak=None):
+    """The DG-SIPG Q3 vmult of config 4 alone (64^3 cells), FP32 and FP64: CUDA-event time per
+    vmult (all its kernels: the fused tile kernel where the mesh allows it), GDoF/s and the
+    algorithmic bytes 2 s N + 6 s C (src read and dst written once, six geometry values per
+    cell; DG indices are implicit) over that time as a fraction of the HBM peak."""
+    p = 3
+    mesh = pmg.Mesh(pmg.Box.make(refine=refine))
+    peak = peak or measured_peaks()[0]
+    out = {}
+    for name, dt, tdt in (("fp32", pmg.F32, torch.float32), ("fp64", pmg.F64, torch.float64)):
+        op = pmg.DGLaplaceOperator(mesh, p, dt, 2.0 * (p + 1) ** 2, device=dev)
+        src = torch.rand(op.m(), dtype=tdt, device=f"cuda:{dev}")
+        dst = torch.empty_like(src)
+        for _ in range(3):
+            op.vmult(dst, src)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(launches):
+            op.vmult(dst, src)
+        e1.record()
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / launches * 1e-3
+        s = 8 if dt == pmg.F64 else 4
+        alg = 2 * s * op.m() + 6 * s * mesh.n_cells()
+        units, par = op.last_launch(pmg.KERNEL_DG_FACES)
+        out[name] = {"vmult_us": t * 1e6, "gdofs": op.m() / t / 1e9, "algorithmic_bytes": alg,
+                     "frac_of_hbm": alg / t / 1e9 / peak, "tiles": units, "blocks": par}
+        del op, src, dst
+    del mesh
+    torch.cuda.empty_cache()
+    out["peak_gbs"] = peak
+    return out
 
 
 def adjoint_check(torch, pmg, dev, refine=5, n_dirs=8, eps=1e-6):
