@@ -207,3 +207,27 @@ def test_dg_vmult_with_unaligned_vectors(p, dtype):
     op.vmult(d1, s_off)
     torch.cuda.synchronize()
     assert torch.equal(d0, d1)
+
+
+@pytest.mark.parametrize("form", ["0", "1"])
+@pytest.mark.parametrize("p", [1, 3, 4])
+@pytest.mark.parametrize("dtype", [pmg.F64, pmg.F32])
+@pytest.mark.parametrize("boxname", ["cube_r2", "ragged_3x2x1", "neumann_r2"])
+def test_dg_face_forms_match_oracle(oracle, monkeypatch, form, p, dtype, boxname):
+    """The comparison forms of the face kernel, selected at every launch: PMG_DG_FACE=0 (the
+    six faces one after another) and 1 (the cell-batch kernel, also where tiles would apply)."""
+    monkeypatch.setenv("PMG_DG_FACE", form)
+    box = pmg.Box.make(**BOXES[boxname])
+    ob = obox(oracle, box)
+    c_pen = 2.0 * (p + 1) ** 2
+    op = pmg.DGLaplaceOperator(pmg.Mesh(box), p, dtype, c_pen)
+    src = np.random.default_rng(p).uniform(-1, 1, op.m())
+    td = torch.float64 if dtype == pmg.F64 else torch.float32
+    d = op.initialize_dof_vector()
+    op.vmult(d, torch.tensor(src, dtype=td, device="cuda"))
+    torch.cuda.synchronize()
+    assert rel_err(d.double().cpu().numpy(), oracle.dg_vmult(ob, p, c_pen, src)) < TOL[dtype]
+    units, _ = op.last_launch(pmg.KERNEL_DG_FACES)
+    n_cells = op.m() // (p + 1) ** 3
+    batch = 128 // (p + 1) ** 2 if form == "0" else max(1, 384 // (6 * (p + 1) ** 2))
+    assert units == -(-n_cells // batch)
