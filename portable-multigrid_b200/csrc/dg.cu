@@ -720,11 +720,19 @@ __device__ __forceinline__ void tile_flux_at(const DGTab<N, T> &tab, const DGGeo
   f2 *= area;
 }
 
-template <int N, typename T, int TT>
+// the Chebyshev step the fused kernel can apply in place of storing A x (CHEB):
+// out = x + f1 (x - x_prev) + f2 D^{-1} (b - A x), x = src; prev null: x_prev = 0
+template <typename T> struct ChebArgs {
+  const T *prev, *b, *invd;
+  T f1, f2;
+};
+
+template <int N, typename T, int TT, bool CHEB = false>
 __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __grid_constant__ DGTab<N, T> tab,
                                                                      const __grid_constant__ DGGeo geo,
                                                                      const T *__restrict__ src, T *__restrict__ dst,
-                                                                     const int32_t *__restrict__ nbr, int64_t n_tiles) {
+                                                                     const int32_t *__restrict__ nbr, int64_t n_tiles,
+                                                                     ChebArgs<T> cheb = ChebArgs<T>{}) {
   static_assert(tile_shuffles<N>(), "the fused tile kernel applies the face mass on shuffles");
   constexpr int N2 = N * N, N3 = N2 * N, NP = kTileFaces * N2;
   constexpr int CS = FusedLayout<N, T>::CS, PZ = FusedLayout<N, T>::PZ; // cell stride, z-plane stride
@@ -924,7 +932,17 @@ __global__ void __launch_bounds__(TT, 1024 / TT) dg_tile_fused_kernel(const __gr
         v += F2[pab] * DPH(F);
         if (lay[F]) v += (x & 1) ? -F1[pab] : F1[pab];
       }
-      td[ct * N3 + l] = v;
+      if constexpr (CHEB) {
+        // the Chebyshev step of vector_ops (cheb_update_into) with A x from registers; out
+        // (dst) may be prev, whose entry only this thread reads, never src, which the
+        // neighbouring tiles read
+        const int64_t gi = (base + ct) * N3 + l;
+        const T xv = ts[ct * N3 + l];
+        const T xo = cheb.prev ? cheb.prev[gi] : T(0);
+        dst[gi] = xv + cheb.f1 * (xv - xo) + cheb.f2 * cheb.invd[gi] * (cheb.b[gi] - v);
+      } else {
+        td[ct * N3 + l] = v;
+      }
     }
     __syncthreads();
   }
@@ -1082,9 +1100,10 @@ bool fuse_allowed() {
   return !(e && e[0] == '0' && e[1] == 0);
 }
 
+// cheb (optional): apply the Chebyshev step (dst = out) instead of storing A src
 template <int N, typename T>
 bool fused_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms, cudaStream_t s,
-                  int64_t *units, int64_t *blocks) {
+                  int64_t *units, int64_t *blocks, const DGChebStep *cheb, bool launch = true) {
   if constexpr (!tile_shuffles<N>()) {
     return false;
   } else {
@@ -1095,6 +1114,7 @@ bool fused_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, 
     const TileShape sh = tile_shape<N, T, true>();
     const int64_t n_tiles = n_cells / 64;
     if (form < 0 && n_tiles < 2 * (int64_t)sh.blocks_per_sm * sms) return false;
+    if (!launch) return true;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, (int64_t)sh.blocks_per_sm * sms));
     if (units) *units = n_tiles;
     if (blocks) *blocks = grid;
@@ -1103,12 +1123,22 @@ bool fused_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, 
     const T *sp = static_cast<const T *>(src);
     T *dp = static_cast<T *>(dst);
     const int32_t *nb = h.nbr.as<int32_t>();
-    if (sh.threads == 1024)
+    if (cheb) {
+      const ChebArgs<T> ca{static_cast<const T *>(cheb->prev), static_cast<const T *>(cheb->b),
+                           static_cast<const T *>(cheb->invd), (T)cheb->f1, (T)cheb->f2};
+      if (sh.threads == 1024)
+        dg_tile_fused_kernel<N, T, 1024, true><<<grid, 1024, smem, s>>>(tab, geo, sp, dp, nb, n_tiles, ca);
+      else if (sh.threads == 512)
+        dg_tile_fused_kernel<N, T, 512, true><<<grid, 512, smem, s>>>(tab, geo, sp, dp, nb, n_tiles, ca);
+      else
+        dg_tile_fused_kernel<N, T, 256, true><<<grid, 256, smem, s>>>(tab, geo, sp, dp, nb, n_tiles, ca);
+    } else if (sh.threads == 1024) {
       dg_tile_fused_kernel<N, T, 1024><<<grid, 1024, smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
-    else if (sh.threads == 512)
+    } else if (sh.threads == 512) {
       dg_tile_fused_kernel<N, T, 512><<<grid, 512, smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
-    else
+    } else {
       dg_tile_fused_kernel<N, T, 256><<<grid, 256, smem, s>>>(tab, geo, sp, dp, nb, n_tiles);
+    }
     PMG_LAUNCH_CHECK();
     return true;
   }
@@ -1116,10 +1146,10 @@ bool fused_launch(const DGHost &h, const void *src, void *dst, int64_t n_cells, 
 
 template <typename T>
 bool fused_dispatch(int degree, const DGHost &h, const void *src, void *dst, int64_t n_cells, int sms, cudaStream_t s,
-                    int64_t *units, int64_t *blocks) {
+                    int64_t *units, int64_t *blocks, const DGChebStep *cheb, bool launch = true) {
   switch (degree) {
-  case 1: return fused_launch<2, T>(h, src, dst, n_cells, sms, s, units, blocks);
-  case 3: return fused_launch<4, T>(h, src, dst, n_cells, sms, s, units, blocks);
+  case 1: return fused_launch<2, T>(h, src, dst, n_cells, sms, s, units, blocks, cheb, launch);
+  case 3: return fused_launch<4, T>(h, src, dst, n_cells, sms, s, units, blocks, cheb, launch);
   default: return false;
   }
 }
@@ -1127,9 +1157,15 @@ bool fused_dispatch(int degree, const DGHost &h, const void *src, void *dst, int
 } // namespace
 
 bool dg_apply_fused(const DGHost &h, int degree, int dtype, const void *src, void *dst, int64_t n_cells, int sms,
-                    cudaStream_t s, int64_t *units, int64_t *blocks) {
-  return dtype == PMG_F64 ? fused_dispatch<double>(degree, h, src, dst, n_cells, sms, s, units, blocks)
-                          : fused_dispatch<float>(degree, h, src, dst, n_cells, sms, s, units, blocks);
+                    cudaStream_t s, int64_t *units, int64_t *blocks, const DGChebStep *cheb) {
+  return dtype == PMG_F64 ? fused_dispatch<double>(degree, h, src, dst, n_cells, sms, s, units, blocks, cheb)
+                          : fused_dispatch<float>(degree, h, src, dst, n_cells, sms, s, units, blocks, cheb);
+}
+
+bool dg_fused_applies(const DGHost &h, int degree, int dtype, int64_t n_cells, int sms) {
+  return dtype == PMG_F64
+             ? fused_dispatch<double>(degree, h, nullptr, nullptr, n_cells, sms, nullptr, nullptr, nullptr, nullptr, false)
+             : fused_dispatch<float>(degree, h, nullptr, nullptr, n_cells, sms, nullptr, nullptr, nullptr, nullptr, false);
 }
 
 void dg_setup(DGHost &h, const BoxMesh &mesh, int degree, double c_pen) {

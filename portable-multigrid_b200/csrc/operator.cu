@@ -645,6 +645,23 @@ void vmult_init(const pmg_operator &op, void *dst, const void *src, cudaStream_t
 }
 } // namespace
 
+// The Chebyshev step out = cur + f1 (cur - prev) + f2 invd (b - A cur) in one launch where the
+// operator is a DG operator on 4x4x4 tiles (the fused tile kernel writes each entry of A cur
+// once, so it applies the step there instead of storing A cur); false, with nothing launched,
+// elsewhere.  out may be prev, not cur.
+bool operator_vmult_chebyshev(const pmg_operator &op, void *out, const void *cur, const void *prev, const void *b,
+                              const void *invd, double f1, double f2, cudaStream_t s) {
+  if (!op.dg || op.n_cells == 0 || op.n_constrained > 0 || op.tensor_cores || out == cur) return false;
+  if (!dg_fused_applies(*op.dg, op.degree, op.dtype, op.n_cells, op.sms)) return false;
+  const DGChebStep c{prev, b, invd, f1, f2};
+  prof::Scope scope("vmult_dg_tile", s);
+  const bool ran = dg_apply_fused(*op.dg, op.degree, op.dtype, cur, out, op.n_cells, op.sms, s,
+                                  &op.launch_units[PMG_KERNEL_DG_FACES], &op.launch_par[PMG_KERNEL_DG_FACES], &c);
+  op.launch_units[PMG_KERNEL_VMULT_CELL] = op.launch_units[PMG_KERNEL_DG_FACES];
+  op.launch_par[PMG_KERNEL_VMULT_CELL] = op.launch_par[PMG_KERNEL_DG_FACES];
+  return ran;
+}
+
 void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStream_t s, bool compute) {
   PMG_REQUIRE(dst && src, "null vector");
   PMG_REQUIRE(dst != src, "vmult needs distinct src and dst");

@@ -235,6 +235,8 @@ void operator_vmult(const pmg_operator &op, void *dst, const void *src, cudaStre
                     bool compute = true);
 void operator_vmult_cells(const pmg_operator &op, void *dst, const void *src, int64_t cell_begin,
                           int64_t cell_end, bool init, cudaStream_t s);
+bool operator_vmult_chebyshev(const pmg_operator &op, void *out, const void *cur, const void *prev, const void *b,
+                              const void *invd, double f1, double f2, cudaStream_t s);
 void operator_compute_inverse_diagonal(pmg_operator &op, cudaStream_t s);
 void operator_assemble_rhs(const pmg_operator &op, int f_kind, int nq, void *b, cudaStream_t s);
 void operator_copy_geometry(const pmg_operator &op, double *host);

@@ -175,12 +175,15 @@ void chebyshev_apply(pmg_chebyshev &c, void *dst, const void *src, bool from_zer
   double rhok = c.delta / c.theta;
   const double sigma = c.theta / c.delta;
   for (int k = 1; k < d; ++k) {
-    operator_vmult(op, c.Ax.get(), cur, s);
     const double rhokp = 1.0 / (2.0 * sigma - rhok);
     const double f1 = rhokp * rhok, f2 = 2.0 * rhokp / c.delta;
     rhok = rhokp;
     void *out = prev ? prev : (cur == A ? B : A);
-    vec::cheb_update_into(out, cur, prev, src, c.Ax.get(), op.inv_diag.get(), f1, f2, dt, N, s);
+    // DG operators on cell tiles apply the step inside their vmult kernel (A cur never stored)
+    if (!operator_vmult_chebyshev(op, out, cur, prev, src, op.inv_diag.get(), f1, f2, s)) {
+      operator_vmult(op, c.Ax.get(), cur, s);
+      vec::cheb_update_into(out, cur, prev, src, c.Ax.get(), op.inv_diag.get(), f1, f2, dt, N, s);
+    }
     prev = cur;
     cur = out;
   }
