@@ -989,6 +989,13 @@ template <int N, typename T, bool FUSED> TileShape tile_shape() {
       probe(dg_tile_fused_kernel<N, T, 256>, 256);
       probe(dg_tile_fused_kernel<N, T, 512>, 512);
       probe(dg_tile_fused_kernel<N, T, 1024>, 1024);
+      // the Chebyshev-step variants take the same shape; they need the same shared memory
+      PMG_CUDA(cudaFuncSetAttribute(dg_tile_fused_kernel<N, T, 256, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PMG_CUDA(cudaFuncSetAttribute(dg_tile_fused_kernel<N, T, 512, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PMG_CUDA(cudaFuncSetAttribute(dg_tile_fused_kernel<N, T, 1024, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
   } else {
     probe(dg_face_tile_kernel<N, T, 256>, 256);
